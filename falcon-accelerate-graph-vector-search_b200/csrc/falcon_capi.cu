@@ -1,0 +1,535 @@
+// C ABI of libfalcon_b200.so: index management, search entry points and the
+// reference-kernel-compatible falcon_vadd.  Host code; all device work is
+// issued on the caller's stream.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/falcon.h"
+#include "falcon_internal.h"
+
+using namespace falcon;
+
+struct falcon_index {
+    int device = 0;
+    int num_sms = 0;
+    int64_t n = 0;
+    int dim = 0, dpad = 0, max_degree = 0, entry = 0, storage = 0;
+    int64_t link_stride = 0;
+    int ids_offset = 0;
+    float *d_f32 = nullptr;        // n x dpad
+    uint16_t *d_bf16 = nullptr;    // n x dpad
+    uint8_t *d_fp8 = nullptr;      // n x dpad
+    float *d_scales = nullptr;     // n
+    int32_t *d_links = nullptr;    // n x link_stride
+    int32_t *d_labels = nullptr;   // n or null
+    int64_t device_bytes = 0;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_error(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+#define FALCON_CUDA(call)                                                                               \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess) {                                                                        \
+            rc = set_error(e_ == cudaErrorMemoryAllocation ? FALCON_ERR_OOM : FALCON_ERR_CUDA, "%s: %s", \
+                           #call, cudaGetErrorString(e_));                                              \
+            goto done;                                                                                  \
+        }                                                                                               \
+    } while (0)
+
+int pad16(int d) { return (d + 15) / 16 * 16; }
+
+void free_index_buffers(falcon_index *ix)
+{
+    cudaFree(ix->d_f32);
+    cudaFree(ix->d_bf16);
+    cudaFree(ix->d_fp8);
+    cudaFree(ix->d_scales);
+    cudaFree(ix->d_links);
+    cudaFree(ix->d_labels);
+    ix->d_f32 = nullptr; ix->d_bf16 = nullptr; ix->d_fp8 = nullptr;
+    ix->d_scales = nullptr; ix->d_links = nullptr; ix->d_labels = nullptr;
+}
+
+// Host-side validation of the adjacency rows: count in [0, max_degree], ids in [0, n).
+int validate_graph(const falcon_index_desc *d)
+{
+    for (int64_t r = 0; r < d->num_vectors; r++) {
+        const int32_t *row = d->links + r * d->link_stride;
+        const int32_t c = row[0];
+        if (c < 0 || c > d->max_degree)
+            return set_error(FALCON_ERR_GRAPH, "row %lld: neighbour count %d outside [0, %d]", (long long)r, c,
+                             d->max_degree);
+        for (int j = 0; j < c; j++) {
+            const int32_t v = row[d->ids_offset + j];
+            if (v < 0 || v >= d->num_vectors)
+                return set_error(FALCON_ERR_GRAPH, "row %lld: neighbour id %d outside [0, %lld)", (long long)r, v,
+                                 (long long)d->num_vectors);
+        }
+    }
+    return FALCON_OK;
+}
+
+int check_params(const falcon_search_params &p, const falcon_index *ix, int64_t qi)
+{
+    int ef = p.ef < p.k ? p.k : p.ef;
+    if (p.k < 1 || ef < 1 || ef > kMaxEf)
+        return set_error(FALCON_ERR_ARG, "query %lld: k=%d ef=%d (need 1 <= k, ef <= %d)", (long long)qi, p.k, p.ef, kMaxEf);
+    if (p.mc < 1 || p.mc > kMaxMc) return set_error(FALCON_ERR_ARG, "query %lld: mc=%d outside [1,%d]", (long long)qi, p.mc, kMaxMc);
+    if (p.mg < 1 || p.mg > kMaxMg) return set_error(FALCON_ERR_ARG, "query %lld: mg=%d outside [1,%d]", (long long)qi, p.mg, kMaxMg);
+    if (p.cand_queue_size < 1 || p.cand_queue_size > kMaxCandQueue)
+        return set_error(FALCON_ERR_ARG, "query %lld: cand_queue_size=%d outside [1,%d]", (long long)qi, p.cand_queue_size, kMaxCandQueue);
+    if (p.bloom_bits < kMinBloomBits || p.bloom_bits > kMaxBloomBits)
+        return set_error(FALCON_ERR_ARG, "query %lld: bloom_bits=%d outside [%d,%d]", (long long)qi, p.bloom_bits, kMinBloomBits, kMaxBloomBits);
+    if (p.max_hops < 0) return set_error(FALCON_ERR_ARG, "query %lld: max_hops < 0", (long long)qi);
+    if (p.mode != FALCON_MODE_INTER && p.mode != FALCON_MODE_INTRA)
+        return set_error(FALCON_ERR_ARG, "query %lld: unknown mode %d", (long long)qi, p.mode);
+    if (p.mode == FALCON_MODE_INTRA &&
+        (p.channels < 1 || p.channels > kMaxChannels || (p.channels & (p.channels - 1))))
+        return set_error(FALCON_ERR_ARG, "query %lld: channels=%d must be a power of two <= %d", (long long)qi, p.channels, kMaxChannels);
+    if (p.precision == FALCON_PREC_BF16 && !(ix->storage & FALCON_STORE_BF16))
+        return set_error(FALCON_ERR_ARG, "BF16 traversal needs FALCON_STORE_BF16 in the index");
+    if (p.precision == FALCON_PREC_FP8 && !(ix->storage & FALCON_STORE_FP8))
+        return set_error(FALCON_ERR_ARG, "FP8 traversal needs FALCON_STORE_FP8 in the index");
+    if (p.precision < 0 || p.precision > 2) return set_error(FALCON_ERR_ARG, "unknown precision %d", p.precision);
+    return FALCON_OK;
+}
+
+QParams to_qparams(const falcon_search_params &p)
+{
+    QParams q;
+    q.k = p.k;
+    q.ef = p.ef < p.k ? p.k : p.ef;
+    q.mc = p.mc;
+    q.mg = p.mg;
+    q.cq = p.cand_queue_size;
+    q.bloom_bits = p.bloom_bits;
+    q.seed = p.hash_seed;
+    q.mode = p.mode;
+    q.channels = p.channels;
+    q.precision = p.precision;
+    q.rerank = p.rerank;
+    q.max_hops = p.max_hops;
+    return q;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *falcon_last_error(void) { return g_last_error.c_str(); }
+
+const char *falcon_build_info(void) { return "libfalcon_b200 sm_100a (inter-query + intra-query DST traversal)"; }
+
+void falcon_default_params(falcon_search_params *p)
+{
+    if (!p) return;
+    p->k = 10;
+    p->ef = 64;
+    p->mc = 1;
+    p->mg = 1;
+    p->cand_queue_size = 32;
+    p->bloom_bits = 16;
+    p->hash_seed = 1;
+    p->mode = FALCON_MODE_INTER;
+    p->channels = 4;
+    p->precision = FALCON_PREC_F32;
+    p->rerank = 0;
+    p->max_hops = 0;
+}
+
+int falcon_index_create(const falcon_index_desc *d, falcon_index **out)
+{
+    if (!d || !out) return set_error(FALCON_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (d->num_vectors < 1 || d->dim < 1 || pad16(d->dim) > kMaxDimPadded || d->max_degree < 1 ||
+        d->max_degree > kMaxDegree || !d->vectors || !d->links || d->vector_stride < d->dim ||
+        d->link_stride < d->ids_offset + d->max_degree || d->ids_offset < 1)
+        return set_error(FALCON_ERR_ARG, "invalid index description (n=%lld dim=%d max_degree=%d)",
+                         (long long)d->num_vectors, d->dim, d->max_degree);
+    if (d->num_vectors > 0x7fffffffLL) return set_error(FALCON_ERR_ARG, "more than 2^31-1 vectors");
+    if (d->entry_point < 0 || d->entry_point >= d->num_vectors)
+        return set_error(FALCON_ERR_GRAPH, "entry point %d outside [0, %lld)", d->entry_point, (long long)d->num_vectors);
+    int rc = validate_graph(d);
+    if (rc != FALCON_OK) return rc;
+
+    DeviceGuard guard(d->device);
+    if (!guard.ok) return set_error(FALCON_ERR_CUDA, "cannot select device %d", d->device);
+    falcon_index *ix = new falcon_index;
+    ix->device = d->device;
+    ix->n = d->num_vectors;
+    ix->dim = d->dim;
+    ix->dpad = pad16(d->dim);
+    ix->max_degree = d->max_degree;
+    ix->entry = d->entry_point;
+    ix->storage = d->storage | FALCON_STORE_F32;
+    ix->link_stride = d->link_stride;
+    ix->ids_offset = d->ids_offset;
+    {
+        rc = FALCON_OK;
+        const size_t nvec = (size_t)ix->n;
+        const size_t f32_bytes = nvec * ix->dpad * sizeof(float);
+        cudaDeviceProp prop;
+        FALCON_CUDA(cudaGetDeviceProperties(&prop, ix->device));
+        ix->num_sms = prop.multiProcessorCount;
+        FALCON_CUDA(cudaMalloc(&ix->d_f32, f32_bytes));
+        FALCON_CUDA(cudaMemset(ix->d_f32, 0, f32_bytes));
+        FALCON_CUDA(cudaMemcpy2D(ix->d_f32, ix->dpad * sizeof(float), d->vectors, d->vector_stride * sizeof(float),
+                                 ix->dim * sizeof(float), nvec, cudaMemcpyHostToDevice));
+        ix->device_bytes += f32_bytes;
+        const size_t link_bytes = nvec * ix->link_stride * sizeof(int32_t);
+        FALCON_CUDA(cudaMalloc(&ix->d_links, link_bytes));
+        FALCON_CUDA(cudaMemcpy(ix->d_links, d->links, link_bytes, cudaMemcpyHostToDevice));
+        ix->device_bytes += link_bytes;
+        if (d->labels) {
+            FALCON_CUDA(cudaMalloc(&ix->d_labels, nvec * sizeof(int32_t)));
+            FALCON_CUDA(cudaMemcpy(ix->d_labels, d->labels, nvec * sizeof(int32_t), cudaMemcpyHostToDevice));
+            ix->device_bytes += nvec * sizeof(int32_t);
+        }
+        if (ix->storage & FALCON_STORE_BF16) {
+            FALCON_CUDA(cudaMalloc(&ix->d_bf16, nvec * ix->dpad * sizeof(uint16_t)));
+            FALCON_CUDA(launch_encode_bf16(ix->d_f32, ix->dpad, ix->n, ix->dim, ix->dpad, ix->d_bf16, 0));
+            ix->device_bytes += nvec * ix->dpad * sizeof(uint16_t);
+        }
+        if (ix->storage & FALCON_STORE_FP8) {
+            FALCON_CUDA(cudaMalloc(&ix->d_fp8, nvec * ix->dpad));
+            FALCON_CUDA(cudaMalloc(&ix->d_scales, nvec * sizeof(float)));
+            FALCON_CUDA(launch_encode_fp8(ix->d_f32, ix->dpad, ix->n, ix->dim, ix->dpad, ix->d_fp8, ix->d_scales, 0));
+            ix->device_bytes += nvec * ix->dpad + nvec * sizeof(float);
+        }
+        FALCON_CUDA(cudaDeviceSynchronize());
+    }
+done:
+    if (rc != FALCON_OK) {
+        free_index_buffers(ix);
+        delete ix;
+        return rc;
+    }
+    *out = ix;
+    return FALCON_OK;
+}
+
+int falcon_index_free(falcon_index *ix)
+{
+    if (!ix) return FALCON_OK;
+    DeviceGuard guard(ix->device);
+    free_index_buffers(ix);
+    delete ix;
+    return FALCON_OK;
+}
+
+int falcon_index_info_get(const falcon_index *ix, falcon_index_info *info)
+{
+    if (!ix || !info) return set_error(FALCON_ERR_ARG, "null argument");
+    info->num_vectors = ix->n;
+    info->dim = ix->dim;
+    info->dim_padded = ix->dpad;
+    info->max_degree = ix->max_degree;
+    info->entry_point = ix->entry;
+    info->storage = ix->storage;
+    info->device = ix->device;
+    info->device_bytes = ix->device_bytes;
+    return FALCON_OK;
+}
+
+static bool read_file(const std::string &path, std::vector<char> &buf)
+{
+    FILE *f = fopen(path.c_str(), "rb");
+    if (!f) return false;
+    fseek(f, 0, SEEK_END);
+    long sz = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    buf.resize(sz > 0 ? (size_t)sz : 0);
+    const bool ok = sz <= 0 || fread(buf.data(), 1, (size_t)sz, f) == (size_t)sz;
+    fclose(f);
+    return ok;
+}
+
+int falcon_index_load_fpga(const char *index_dir, const char *graph_type, int32_t dim, int32_t storage,
+                           int32_t device, falcon_index **out)
+{
+    if (!index_dir || !graph_type || !out || dim < 1) return set_error(FALCON_ERR_ARG, "null argument or dim < 1");
+    const std::string dir(index_dir), gt(graph_type);
+    if (gt != "HNSW" && gt != "NSG") return set_error(FALCON_ERR_ARG, "graph_type must be HNSW or NSG");
+    std::vector<char> meta, links, vecs, labels;
+    if (!read_file(dir + "/meta.bin", meta)) return set_error(FALCON_ERR_IO, "cannot read %s/meta.bin", index_dir);
+    const int32_t *m = reinterpret_cast<const int32_t *>(meta.data());
+    int32_t n, entry, md;
+    if (gt == "HNSW") {   // cur_element_count, maxlevel_, enterpoint_node_, maxM_, maxM0_ (hnsw.py:270-275)
+        if (meta.size() < 20) return set_error(FALCON_ERR_IO, "meta.bin too short for HNSW");
+        n = m[0]; entry = m[2]; md = m[4];
+    } else {              // num_nodes, entry point, width (nsg_to_FPGA.py)
+        if (meta.size() < 12) return set_error(FALCON_ERR_IO, "meta.bin too short for NSG");
+        n = m[0]; entry = m[1]; md = m[2];
+    }
+    if (n < 1 || md < 1 || md > kMaxDegree) return set_error(FALCON_ERR_IO, "meta.bin: n=%d max_degree=%d", n, md);
+    const int64_t lstride = 16LL * (1 + (md + 15) / 16);
+    const int64_t vstride = pad16(dim) + 16;
+    if (!read_file(dir + "/ground_links_1_chan_0.bin", links) || (int64_t)links.size() != (int64_t)n * lstride * 4)
+        return set_error(FALCON_ERR_IO, "ground_links_1_chan_0.bin missing or not %lld bytes", (long long)n * lstride * 4);
+    if (!read_file(dir + "/ground_vectors_1_chan_0.bin", vecs) || (int64_t)vecs.size() != (int64_t)n * vstride * 4)
+        return set_error(FALCON_ERR_IO, "ground_vectors_1_chan_0.bin missing or not %lld bytes for dim %d",
+                         (long long)n * vstride * 4, dim);
+    const bool have_labels = read_file(dir + "/ground_labels.bin", labels) && (int64_t)labels.size() == (int64_t)n * 4;
+    falcon_index_desc d;
+    memset(&d, 0, sizeof(d));
+    d.num_vectors = n;
+    d.dim = dim;
+    d.max_degree = md;
+    d.vectors = reinterpret_cast<const float *>(vecs.data());
+    d.vector_stride = vstride;
+    d.links = reinterpret_cast<const int32_t *>(links.data());
+    d.link_stride = lstride;
+    d.ids_offset = 16;
+    d.entry_point = entry;
+    d.labels = (gt == "HNSW" && have_labels) ? reinterpret_cast<const int32_t *>(labels.data()) : nullptr;
+    d.storage = storage;
+    d.device = device;
+    return falcon_index_create(&d, out);
+}
+
+int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t query_stride,
+                  const int32_t *entry_points, const falcon_search_params *params, int32_t per_query_params,
+                  int32_t *out_ids, float *out_dists, int32_t out_stride, int32_t *out_hops, int32_t *out_visited,
+                  int32_t memory, void *stream_v)
+{
+    if (!ix || !params || !out_ids || !out_dists) return set_error(FALCON_ERR_ARG, "null argument");
+    if (nq < 0 || (nq > 0 && !queries) || query_stride < ix->dim)
+        return set_error(FALCON_ERR_ARG, "bad queries (nq=%lld, stride=%lld, dim=%d)", (long long)nq,
+                         (long long)query_stride, ix->dim);
+    if (memory != FALCON_MEM_HOST && memory != FALCON_MEM_DEVICE) return set_error(FALCON_ERR_ARG, "bad memory flag");
+    if (nq == 0) return FALCON_OK;
+    if (per_query_params && memory == FALCON_MEM_DEVICE)
+        return set_error(FALCON_ERR_ARG, "per-query params must be host memory");
+    const int64_t np = per_query_params ? nq : 1;
+    int ef_max = 0, k_max = 0, mc_max = 1, mg_max = 1, bits_max = kMinBloomBits, prec = -1, mode = -1, ch_max = 1;
+    bool any_rerank = false;
+    std::vector<QParams> qp((size_t)np);
+    for (int64_t i = 0; i < np; i++) {
+        int rc = check_params(params[i], ix, i);
+        if (rc != FALCON_OK) return rc;
+        qp[i] = to_qparams(params[i]);
+        if (prec >= 0 && prec != params[i].precision)
+            return set_error(FALCON_ERR_UNSUPPORTED, "one call must use one precision");
+        if (mode >= 0 && mode != params[i].mode) return set_error(FALCON_ERR_UNSUPPORTED, "one call must use one mode");
+        prec = params[i].precision;
+        mode = params[i].mode;
+        ef_max = qp[i].ef > ef_max ? qp[i].ef : ef_max;
+        k_max = qp[i].k > k_max ? qp[i].k : k_max;
+        mc_max = qp[i].mc > mc_max ? qp[i].mc : mc_max;
+        mg_max = qp[i].mg > mg_max ? qp[i].mg : mg_max;
+        bits_max = qp[i].bloom_bits > bits_max ? qp[i].bloom_bits : bits_max;
+        if (qp[i].mode == FALCON_MODE_INTRA && qp[i].channels > ch_max) ch_max = qp[i].channels;
+        any_rerank |= (qp[i].rerank != 0 && qp[i].precision != FALCON_PREC_F32);
+    }
+    if (out_stride < k_max) return set_error(FALCON_ERR_ARG, "out_stride %d < k %d", out_stride, k_max);
+    if (mode == FALCON_MODE_INTRA) return set_error(FALCON_ERR_UNSUPPORTED, "intra-query mode not built in this library");
+    if (any_rerank)
+        for (int64_t i = 0; i < np; i++)
+            if (!(qp[i].rerank != 0 && qp[i].precision != FALCON_PREC_F32))
+                return set_error(FALCON_ERR_UNSUPPORTED, "rerank must be set for all queries of a call or none");
+    if (entry_points && memory == FALCON_MEM_HOST) {
+        for (int64_t i = 0; i < nq; i++)
+            if (entry_points[i] < 0 || entry_points[i] >= ix->n)
+                return set_error(FALCON_ERR_ARG, "entry point of query %lld out of range", (long long)i);
+    }
+
+    DeviceGuard guard(ix->device);
+    if (!guard.ok) return set_error(FALCON_ERR_CUDA, "cannot select device %d", ix->device);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream_v);
+    int rc = FALCON_OK;
+    const bool host = memory == FALCON_MEM_HOST;
+    float *d_q = nullptr;
+    int32_t *d_entries = nullptr, *d_ids = nullptr, *d_hops = nullptr, *d_vis = nullptr, *d_cand = nullptr;
+    float *d_d = nullptr, *d_cand_d = nullptr;
+    QParams *d_params = nullptr;
+    int32_t *d_scratch = nullptr;   // [0..1] work counter (u64), [2] status
+    int32_t status_h = 0;
+    SearchLaunch a;
+    memset(&a, 0, sizeof(a));
+    {
+        const size_t qbytes = (size_t)nq * query_stride * sizeof(float);
+        if (host) {
+            FALCON_CUDA(cudaMallocAsync((void **)&d_q, qbytes, s));
+            FALCON_CUDA(cudaMemcpyAsync(d_q, queries, qbytes, cudaMemcpyHostToDevice, s));
+            if (entry_points) {
+                FALCON_CUDA(cudaMallocAsync((void **)&d_entries, nq * sizeof(int32_t), s));
+                FALCON_CUDA(cudaMemcpyAsync(d_entries, entry_points, nq * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+            }
+            FALCON_CUDA(cudaMallocAsync((void **)&d_ids, (size_t)nq * out_stride * sizeof(int32_t), s));
+            FALCON_CUDA(cudaMallocAsync((void **)&d_d, (size_t)nq * out_stride * sizeof(float), s));
+            if (out_hops) FALCON_CUDA(cudaMallocAsync((void **)&d_hops, nq * sizeof(int32_t), s));
+            if (out_visited) FALCON_CUDA(cudaMallocAsync((void **)&d_vis, nq * sizeof(int32_t), s));
+        }
+        FALCON_CUDA(cudaMallocAsync((void **)&d_params, np * sizeof(QParams), s));
+        FALCON_CUDA(cudaMemcpyAsync(d_params, qp.data(), np * sizeof(QParams), cudaMemcpyHostToDevice, s));
+        FALCON_CUDA(cudaMallocAsync((void **)&d_scratch, 4 * sizeof(int32_t), s));
+        FALCON_CUDA(cudaMemsetAsync(d_scratch, 0, 4 * sizeof(int32_t), s));
+
+        a.g.vecs = reinterpret_cast<const unsigned char *>(ix->d_f32);
+        a.g.vstride_bytes = (int64_t)ix->dpad * 4;
+        if (prec == FALCON_PREC_BF16) {
+            a.g.vecs = reinterpret_cast<const unsigned char *>(ix->d_bf16);
+            a.g.vstride_bytes = (int64_t)ix->dpad * 2;
+        } else if (prec == FALCON_PREC_FP8) {
+            a.g.vecs = ix->d_fp8;
+            a.g.vstride_bytes = ix->dpad;
+        }
+        a.g.scales = ix->d_scales;
+        a.g.vecs32 = reinterpret_cast<const unsigned char *>(ix->d_f32);
+        a.g.vstride32_bytes = (int64_t)ix->dpad * 4;
+        a.g.links = ix->d_links;
+        a.g.lstride = ix->link_stride;
+        a.g.ids_off = ix->ids_offset;
+        a.g.max_degree = ix->max_degree;
+        a.g.dim = ix->dim;
+        a.g.dpad = ix->dpad;
+        a.g.n = ix->n;
+        a.g.labels = ix->d_labels;
+        a.queries = host ? d_q : queries;
+        a.qstride = query_stride;
+        a.entries = host ? d_entries : entry_points;
+        a.default_entry = ix->entry;
+        a.nq = nq;
+        a.params = d_params;
+        a.per_query = per_query_params ? 1 : 0;
+        a.out_ids = host ? d_ids : out_ids;
+        a.out_d = host ? d_d : out_dists;
+        a.out_stride = out_stride;
+        a.write_all_ef = 0;
+        a.out_hops = host ? d_hops : out_hops;
+        a.out_visited = host ? d_vis : out_visited;
+        a.work_counter = d_scratch;
+        a.status = d_scratch + 2;
+        a.bloom_bits_max = bits_max;
+        a.ef_max = ef_max;
+        a.mc_max = mc_max;
+        a.mg_max = mg_max;
+        int32_t *final_ids = a.out_ids;
+        float *final_d = a.out_d;
+        if (any_rerank) {
+            FALCON_CUDA(cudaMallocAsync((void **)&d_cand, (size_t)nq * ef_max * sizeof(int32_t), s));
+            FALCON_CUDA(cudaMallocAsync((void **)&d_cand_d, (size_t)nq * ef_max * sizeof(float), s));
+            a.out_ids = d_cand;
+            a.out_d = d_cand_d;
+            a.out_stride = ef_max;
+            a.write_all_ef = 1;
+        }
+        const int elem = prec == FALCON_PREC_BF16 ? kBF16 : (prec == FALCON_PREC_FP8 ? kFP8 : kF32);
+        FALCON_CUDA(launch_search(a, elem, ix->num_sms, s));
+        if (any_rerank) {
+            RerankLaunch r;
+            memset(&r, 0, sizeof(r));
+            r.g = a.g;
+            r.queries = a.queries;
+            r.qstride = a.qstride;
+            r.nq = nq;
+            r.params = d_params;
+            r.per_query = a.per_query;
+            r.cand_ids = d_cand;
+            r.cand_stride = ef_max;
+            r.out_ids = final_ids;
+            r.out_d = final_d;
+            r.out_stride = out_stride;
+            FALCON_CUDA(launch_rerank(r, ef_max, ix->num_sms, s));
+        }
+        if (host) {
+            FALCON_CUDA(cudaMemcpyAsync(out_ids, d_ids, (size_t)nq * out_stride * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            FALCON_CUDA(cudaMemcpyAsync(out_dists, d_d, (size_t)nq * out_stride * sizeof(float), cudaMemcpyDeviceToHost, s));
+            if (out_hops) FALCON_CUDA(cudaMemcpyAsync(out_hops, d_hops, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            if (out_visited) FALCON_CUDA(cudaMemcpyAsync(out_visited, d_vis, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            FALCON_CUDA(cudaMemcpyAsync(&status_h, d_scratch + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        }
+    }
+done:
+    for (void *p : {(void *)d_q, (void *)d_entries, (void *)d_ids, (void *)d_d, (void *)d_hops, (void *)d_vis,
+                    (void *)d_params, (void *)d_scratch, (void *)d_cand, (void *)d_cand_d})
+        if (p) cudaFreeAsync(p, s);
+    if (rc == FALCON_OK && host) {
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return set_error(FALCON_ERR_CUDA, "search: %s", cudaGetErrorString(e));
+        if (status_h & 1) return FALCON_WARN_TRUNCATED;
+    }
+    return rc;
+}
+
+int falcon_vadd(int32_t query_num, int32_t query_batch_size, int32_t ef, int32_t candidate_queue_runtime_size,
+                int32_t max_cand_batch_size, int32_t max_async_stage_num, int32_t runtime_n_bucket_addr_bits,
+                uint32_t hash_seed, int32_t max_bloom_out_burst_size, int32_t max_link_num_base, int32_t dim,
+                int64_t num_db_vec, const int32_t *entry_point_ids, const float *query_vectors,
+                const void *db_vectors, const void *links_base, int32_t *out_id, float *out_dist,
+                int32_t *mem_debug, int32_t device)
+{
+    if (query_num < 0 || query_batch_size < 1 || max_bloom_out_burst_size < 1 || !entry_point_ids || !query_vectors ||
+        !db_vectors || !links_base || !out_id || !out_dist || !mem_debug)
+        return set_error(FALCON_ERR_ARG, "falcon_vadd: invalid argument");
+    falcon_index_desc d;
+    memset(&d, 0, sizeof(d));
+    d.num_vectors = num_db_vec;
+    d.dim = dim;
+    d.max_degree = max_link_num_base;
+    d.vectors = reinterpret_cast<const float *>(db_vectors);
+    d.vector_stride = pad16(dim) + 16;
+    d.links = reinterpret_cast<const int32_t *>(links_base);
+    d.link_stride = 16LL * (1 + (max_link_num_base + 15) / 16);
+    d.ids_offset = 16;
+    d.entry_point = query_num > 0 ? entry_point_ids[0] : 0;
+    d.device = device;
+    falcon_index *ix = nullptr;
+    int rc = falcon_index_create(&d, &ix);
+    if (rc != FALCON_OK) return rc;
+    falcon_search_params p;
+    falcon_default_params(&p);
+    p.k = ef;
+    p.ef = ef;
+    p.mc = max_cand_batch_size;
+    p.mg = max_async_stage_num;
+    p.cand_queue_size = candidate_queue_runtime_size;
+    p.bloom_bits = runtime_n_bucket_addr_bits;
+    p.hash_seed = hash_seed;
+    std::vector<int32_t> hops((size_t)query_num), vis((size_t)query_num);
+    rc = falcon_search(ix, query_vectors, query_num, pad16(dim), entry_point_ids, &p, 0, out_id, out_dist, ef,
+                       hops.data(), vis.data(), FALCON_MEM_HOST, nullptr);
+    if (rc >= 0) {
+        for (int32_t i = 0; i < query_num; i++) {
+            mem_debug[2 * i] = hops[i];
+            mem_debug[2 * i + 1] = vis[i];
+        }
+    }
+    falcon_index_free(ix);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,94 @@
+// Internal structures shared by the traversal kernels and the C-ABI layer.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace falcon {
+
+constexpr float kLarge = 1e20f;   // constants.hpp:14 large_float
+
+enum Elem { kF32 = 0, kBF16 = 1, kFP8 = 2 };
+
+// Limits of the built kernels.
+constexpr int kMaxEf = 256;
+constexpr int kMaxCandQueue = 32;
+constexpr int kMaxMc = 8;
+constexpr int kMaxMg = 16;
+constexpr int kMaxDegree = 128;
+constexpr int kMaxBloomBits = 18;
+constexpr int kMinBloomBits = 10;
+constexpr int kMaxDimPadded = 512;
+constexpr int kMaxChannels = 8;
+
+// Device view of one resident graph.
+struct GraphView {
+    const unsigned char *vecs;      // traversal storage (f32 / bf16 / fp8 codes)
+    int64_t vstride_bytes;
+    const float *scales;            // fp8: one scale per vector
+    const unsigned char *vecs32;    // FP32 storage (rerank), may equal vecs
+    int64_t vstride32_bytes;
+    const int32_t *links;           // count at row*lstride, ids at row*lstride+ids_off
+    int64_t lstride;
+    int32_t ids_off;
+    int32_t max_degree;
+    int32_t dim;
+    int32_t dpad;
+    int64_t n;
+    const int32_t *labels;          // may be null
+};
+
+// Per-query search parameters as the kernels read them.
+struct QParams {
+    int32_t k, ef, mc, mg, cq, bloom_bits;
+    uint32_t seed;
+    int32_t mode, channels, precision, rerank, max_hops;
+};
+
+struct SearchLaunch {
+    GraphView g;
+    const float *queries;
+    int64_t qstride;
+    const int32_t *entries;         // may be null
+    int32_t default_entry;
+    int64_t nq;
+    const QParams *params;          // device array (1 or nq)
+    int32_t per_query;
+    // result rows: out_ids[q*out_stride + i] for i < (rerank ? ef : k)
+    int32_t *out_ids;
+    float *out_d;
+    int32_t out_stride;
+    int32_t write_all_ef;           // 1: write ef results (rerank input), physical ids
+    int32_t *out_hops;
+    int32_t *out_visited;
+    int32_t *work_counter;          // zeroed before launch
+    int32_t *status;                // bit 0: some query hit max_hops
+    int32_t bloom_bits_max;         // shared-memory Bloom size per warp/channel
+    int32_t ef_max;
+    int32_t mc_max, mg_max;
+};
+
+struct RerankLaunch {
+    GraphView g;
+    const float *queries;
+    int64_t qstride;
+    int64_t nq;
+    const QParams *params;
+    int32_t per_query;
+    const int32_t *cand_ids;        // nq x cand_stride physical ids (best-first)
+    int32_t cand_stride;
+    int32_t *out_ids;
+    float *out_d;
+    int32_t out_stride;
+};
+
+// Launchers (falcon_kernels.cu).  Return cudaError_t of the launch.
+cudaError_t launch_search(const SearchLaunch &a, int elem, int num_sms, cudaStream_t s);
+cudaError_t launch_rerank(const RerankLaunch &a, int ef_max, int num_sms, cudaStream_t s);
+cudaError_t launch_encode_bf16(const float *src, int64_t src_stride, int64_t n, int dim, int dpad, uint16_t *dst,
+                               cudaStream_t s);
+cudaError_t launch_encode_fp8(const float *src, int64_t src_stride, int64_t n, int dim, int dpad, uint8_t *dst,
+                              float *scales, cudaStream_t s);
+// Number of kernel launches the last launch_search issued (for accounting).
+int search_kernel_count();
+
+}  // namespace falcon

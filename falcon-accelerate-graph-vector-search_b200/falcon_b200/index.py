@@ -1,0 +1,202 @@
+"""Host-side mirror of the reference's search interface over the C ABI.
+
+The reference host (FPGA_multi_DDR/FPGA_inter_query_v1.3_longer_FIFO_alt_PR/
+src/host.cpp:34-96) takes mc (max_cand_per_group), mg
+(max_group_num_in_pipe), ef, the graph and its max degree, then launches the
+kernel once over all queries and reads back ids, distances and per-query
+debug counters (hops, visited).  FalconIndex.search keeps those names and
+outputs; everything runs in libfalcon_b200.so.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .formats import Graph
+
+_PREC = {"f32": _lib.PREC_F32, "bf16": _lib.PREC_BF16, "fp8": _lib.PREC_FP8}
+_MODE = {"inter": _lib.MODE_INTER, "intra": _lib.MODE_INTRA}
+_STORE = {"f32": _lib.STORE_F32, "bf16": _lib.STORE_BF16, "fp8": _lib.STORE_FP8}
+
+
+def storage_mask(storage):
+    if isinstance(storage, int):
+        return storage
+    m = 0
+    for s in storage:
+        m |= _STORE[s]
+    return m
+
+
+def make_params(k=10, ef=64, mc=1, mg=1, cand_queue_size=32, bloom_bits=16, hash_seed=1, mode="inter",
+                channels=4, precision="f32", rerank=False, max_hops=0):
+    p = _lib.SearchParams()
+    p.k, p.ef, p.mc, p.mg = int(k), int(ef), int(mc), int(mg)
+    p.cand_queue_size, p.bloom_bits, p.hash_seed = int(cand_queue_size), int(bloom_bits), int(hash_seed)
+    p.mode = _MODE[mode] if isinstance(mode, str) else int(mode)
+    p.channels = int(channels)
+    p.precision = _PREC[precision] if isinstance(precision, str) else int(precision)
+    p.rerank = 1 if rerank else 0
+    p.max_hops = int(max_hops)
+    return p
+
+
+class SearchResult:
+    def __init__(self, ids, dists, hops, visited, status):
+        self.ids, self.dists, self.hops, self.visited, self.status = ids, dists, hops, visited, status
+
+    def __iter__(self):
+        return iter((self.ids, self.dists, self.hops, self.visited))
+
+
+class FalconIndex:
+    """A device-resident graph index (one GPU)."""
+
+    def __init__(self, graph, storage=("f32",), device=0):
+        lib = _lib.load()
+        self._graph_keepalive = graph
+        d = _lib.IndexDesc()
+        d.num_vectors = graph.n
+        d.dim = graph.dim
+        d.max_degree = graph.max_degree
+        d.vectors = graph.vectors.ctypes.data
+        d.vector_stride = graph.vectors.strides[0] // 4
+        d.links = graph.links.ctypes.data
+        d.link_stride = graph.links.strides[0] // 4
+        d.ids_offset = graph.ids_offset
+        d.entry_point = graph.entry_point
+        d.labels = graph.labels.ctypes.data if graph.labels is not None else None
+        d.storage = storage_mask(storage)
+        d.device = int(device)
+        h = ctypes.c_void_p()
+        _lib.check(lib.falcon_index_create(ctypes.byref(d), ctypes.byref(h)))
+        self._h = h
+        self.device = int(device)
+        self.dim = graph.dim
+        self.n = graph.n
+
+    @classmethod
+    def load_fpga(cls, index_dir, graph_type, dim, storage=("f32",), device=0):
+        lib = _lib.load()
+        obj = cls.__new__(cls)
+        h = ctypes.c_void_p()
+        _lib.check(lib.falcon_index_load_fpga(index_dir.encode(), graph_type.encode(), int(dim),
+                                              storage_mask(storage), int(device), ctypes.byref(h)))
+        obj._h = h
+        obj._graph_keepalive = None
+        obj.device = int(device)
+        info = obj.info()
+        obj.dim, obj.n = info.dim, info.num_vectors
+        return obj
+
+    def info(self):
+        inf = _lib.IndexInfo()
+        _lib.check(_lib.load().falcon_index_info_get(self._h, ctypes.byref(inf)))
+        return inf
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().falcon_index_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def search(self, queries, k=10, ef=64, mc=1, mg=1, cand_queue_size=32, bloom_bits=16, hash_seed=1,
+               mode="inter", channels=4, precision="f32", rerank=False, max_hops=0, entry_points=None,
+               per_query=None, out_stride=None, stream=None):
+        """Search host queries [nq, dim] (numpy) or device queries (torch CUDA tensor).
+
+        per_query: optional list/array of dicts or SearchParams, one per query
+        (mixed k/ef/mc in one launch).  Returns (ids, dists, hops, visited) with
+        ids/dists [nq, out_stride] best-first (out_stride = max k by default).
+        """
+        lib = _lib.load()
+        if per_query is not None:
+            arr = (_lib.SearchParams * len(per_query))()
+            for i, p in enumerate(per_query):
+                arr[i] = p if isinstance(p, _lib.SearchParams) else make_params(**p)
+            params, pq, kmax = arr, 1, max(p.k for p in arr)
+        else:
+            params, pq = make_params(k, ef, mc, mg, cand_queue_size, bloom_bits, hash_seed, mode, channels,
+                                     precision, rerank, max_hops), 0
+            kmax = params.k
+        ostride = int(out_stride or kmax)
+        if _is_torch_cuda(queries):
+            return self._search_device(queries, params, pq, ostride, entry_points, stream)
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        if q.ndim != 2 or q.shape[1] != self.dim:
+            raise ValueError("queries must be [nq, %d]" % self.dim)
+        nq = q.shape[0]
+        ids = np.empty((nq, ostride), dtype=np.int32)
+        dists = np.empty((nq, ostride), dtype=np.float32)
+        hops = np.empty(nq, dtype=np.int32)
+        vis = np.empty(nq, dtype=np.int32)
+        ep = None
+        if entry_points is not None:
+            ep = np.ascontiguousarray(entry_points, dtype=np.int32)
+        pptr = ctypes.cast(params, ctypes.POINTER(_lib.SearchParams)) if pq else ctypes.byref(params)
+        rc = lib.falcon_search(self._h, q.ctypes.data, nq, q.shape[1], ep.ctypes.data if ep is not None else None,
+                               pptr, pq, ids.ctypes.data, dists.ctypes.data, ostride, hops.ctypes.data,
+                               vis.ctypes.data, _lib.MEM_HOST, stream)
+        _lib.check(rc)
+        return SearchResult(ids, dists, hops, vis, rc)
+
+    def _search_device(self, queries, params, pq, ostride, entry_points, stream):
+        import torch
+        lib = _lib.load()
+        if pq:
+            raise ValueError("per-query params with device queries: pass host queries")
+        q = queries.contiguous().float()
+        nq = q.shape[0]
+        dev = q.device
+        ids = torch.empty((nq, ostride), dtype=torch.int32, device=dev)
+        dists = torch.empty((nq, ostride), dtype=torch.float32, device=dev)
+        hops = torch.empty(nq, dtype=torch.int32, device=dev)
+        vis = torch.empty(nq, dtype=torch.int32, device=dev)
+        ep = None
+        if entry_points is not None:
+            ep = entry_points.to(device=dev, dtype=torch.int32).contiguous()
+        s = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+        rc = lib.falcon_search(self._h, q.data_ptr(), nq, q.stride(0), ep.data_ptr() if ep is not None else None,
+                               ctypes.byref(params), 0, ids.data_ptr(), dists.data_ptr(), ostride, hops.data_ptr(),
+                               vis.data_ptr(), _lib.MEM_DEVICE, ctypes.c_void_p(s))
+        _lib.check(rc)
+        return SearchResult(ids, dists, hops, vis, rc)
+
+
+def _is_torch_cuda(x):
+    try:
+        import torch
+    except ImportError:
+        return False
+    return isinstance(x, torch.Tensor) and x.is_cuda
+
+
+def vadd(query_vectors_padded, entry_point_ids, db_vectors_ref, links_ref, num_db_vec, dim, ef=64,
+         candidate_queue_runtime_size=32, max_cand_batch_size=1, max_async_stage_num=1,
+         runtime_n_bucket_addr_bits=16, hash_seed=1, max_bloom_out_burst_size=16, max_link_num_base=64,
+         query_batch_size=None, device=0):
+    """The reference kernel's argument list (vadd.cpp:11-95) on reference-layout host buffers."""
+    lib = _lib.load()
+    qv = np.ascontiguousarray(query_vectors_padded, dtype=np.float32)
+    nq = qv.shape[0]
+    ep = np.ascontiguousarray(entry_point_ids, dtype=np.int32)
+    out_id = np.empty((nq, ef), dtype=np.int32)
+    out_dist = np.empty((nq, ef), dtype=np.float32)
+    mem_debug = np.empty((nq, 2), dtype=np.int32)
+    dv = np.ascontiguousarray(db_vectors_ref)
+    lk = np.ascontiguousarray(links_ref)
+    rc = lib.falcon_vadd(nq, int(query_batch_size or max(nq, 1)), ef, candidate_queue_runtime_size,
+                         max_cand_batch_size, max_async_stage_num, runtime_n_bucket_addr_bits, hash_seed,
+                         max_bloom_out_burst_size, max_link_num_base, dim, num_db_vec, ep.ctypes.data,
+                         qv.ctypes.data, dv.ctypes.data, lk.ctypes.data, out_id.ctypes.data, out_dist.ctypes.data,
+                         mem_debug.ctypes.data, device)
+    _lib.check(rc)
+    return out_id, out_dist, mem_debug
+
+
+__all__ = ["FalconIndex", "Graph", "make_params", "vadd", "storage_mask"]

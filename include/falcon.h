@@ -1,0 +1,182 @@
+/*
+ * falcon.h -- C ABI of the B200 graph vector search library (libfalcon_b200.so).
+ *
+ * The library is a drop-in for the Falcon FPGA search path of
+ * fpgasystems/Falcon-accelerate-graph-vector-search: best-first traversal of
+ * an HNSW base layer or an NSG graph with delayed-synchronization traversal
+ * (mc candidates per group, mg groups in flight), in inter-query mode (one
+ * warp per query) and intra-query mode (one thread block per query, the
+ * neighbour list split over channel warps).  Results, hop counts and visited
+ * counts are bit-identical to the reference kernel's when distances are FP32.
+ *
+ * Conventions: every function returns an int status (FALCON_OK == 0, negative
+ * on error, never aborts); falcon_last_error() gives a thread-local message.
+ * Pointers are plain host or device pointers as flagged; no torch types.
+ */
+#ifndef FALCON_H
+#define FALCON_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define FALCON_OK 0
+#define FALCON_WARN_TRUNCATED 1     /* some query stopped at max_hops */
+#define FALCON_ERR_ARG (-1)         /* invalid argument */
+#define FALCON_ERR_OOM (-2)         /* device or host allocation failed */
+#define FALCON_ERR_CUDA (-3)        /* CUDA runtime error */
+#define FALCON_ERR_IO (-4)          /* index file missing or malformed */
+#define FALCON_ERR_GRAPH (-5)       /* graph invalid: id out of range, degree > max */
+#define FALCON_ERR_UNSUPPORTED (-6) /* parameter combination not built */
+
+/* base-vector storage formats (bit mask in falcon_index_desc.storage) */
+#define FALCON_STORE_F32 1
+#define FALCON_STORE_BF16 2
+#define FALCON_STORE_FP8 4          /* OCP E4M3 codes + one FP32 scale per vector */
+
+/* traversal precision (falcon_search_params.precision) */
+#define FALCON_PREC_F32 0
+#define FALCON_PREC_BF16 1
+#define FALCON_PREC_FP8 2
+
+/* search modes (falcon_search_params.mode) */
+#define FALCON_MODE_INTER 0         /* one warp per query (reference inter-query v1.3) */
+#define FALCON_MODE_INTRA 1         /* one block per query, `channels` warps (intra-query v1.5) */
+
+/* memory flags for falcon_search */
+#define FALCON_MEM_HOST 0
+#define FALCON_MEM_DEVICE 1
+
+typedef struct falcon_index falcon_index;
+
+/*
+ * Index description.  Replaces the buffers the reference host loads and
+ * hands to its kernel (FPGA_multi_DDR/FPGA_inter_query_v1.3_longer_FIFO_alt_PR/
+ * src/host.cpp:201-713 and vadd.cpp:11-95):
+ *   links: adjacency rows; row r holds its neighbour count at
+ *          links[r*link_stride] and the ids at links[r*link_stride+ids_offset+j].
+ *          The reference file layout (64-byte header line, then the ids) is
+ *          link_stride = 16*(1+ceil(max_degree/16)), ids_offset = 16.
+ *   vectors: FP32, row r at vectors[r*vector_stride]; the first `dim` values
+ *          are used (the reference layout has vector_stride = pad16(dim)+16).
+ *   labels: optional physical-id -> label map applied to returned ids
+ *          (host.cpp:1002-1007); NULL returns physical ids.
+ * All pointers are host memory; the index copies what it needs to the device.
+ */
+typedef struct falcon_index_desc {
+    int64_t num_vectors;
+    int32_t dim;
+    int32_t max_degree;
+    const float *vectors;
+    int64_t vector_stride;
+    const int32_t *links;
+    int64_t link_stride;
+    int32_t ids_offset;
+    int32_t entry_point;
+    const int32_t *labels;
+    int32_t storage;                /* FALCON_STORE_* mask; 0 = FP32 only */
+    int32_t device;                 /* CUDA device ordinal */
+} falcon_index_desc;
+
+typedef struct falcon_index_info {
+    int64_t num_vectors;
+    int32_t dim, dim_padded, max_degree, entry_point, storage, device;
+    int64_t device_bytes;           /* HBM held by the index */
+} falcon_index_info;
+
+/*
+ * Search parameters.  Names follow the reference host (host.cpp:34-96):
+ * mc = max_cand_per_group, mg = max_group_num_in_pipe,
+ * cand_queue_size = candidate_queue_runtime_size (32 in the reference),
+ * bloom_bits = runtime_n_bucket_addr_bits (16 for the 4-channel builds),
+ * hash_seed = 1 in the reference.  k <= ef; k > ef raises ef to k.
+ */
+typedef struct falcon_search_params {
+    int32_t k;
+    int32_t ef;                     /* result queue size, 1..256 */
+    int32_t mc;                     /* candidates per group, 1..8 */
+    int32_t mg;                     /* groups in flight, 1..16 */
+    int32_t cand_queue_size;        /* 1..32 */
+    int32_t bloom_bits;             /* 10..18 */
+    uint32_t hash_seed;
+    int32_t mode;                   /* FALCON_MODE_* */
+    int32_t channels;               /* intra mode: 1,2,4,8 */
+    int32_t precision;              /* FALCON_PREC_* (storage must hold it) */
+    int32_t rerank;                 /* reduced precision: exact FP32 rerank of the final ef */
+    int32_t max_hops;               /* 0 = unbounded; else traversal stops, status 1 */
+} falcon_search_params;
+
+/* Reference defaults: k=10, ef=64, mc=1, mg=1, cand_queue_size=32,
+   bloom_bits=16, hash_seed=1, inter mode, FP32. */
+void falcon_default_params(falcon_search_params *p);
+
+/* Build a device-resident index from host arrays.  Replaces the host's file
+   loading + buffer migration (host.cpp:201-713, 927). */
+int falcon_index_create(const falcon_index_desc *desc, falcon_index **out);
+
+/* Load the reference's FPGA index files (meta.bin, ground_links_1_chan_0.bin,
+   ground_vectors_1_chan_0.bin, ground_labels.bin written by
+   vector_search_baselines/scripts_hnsw/hnsw.py:264-377 and
+   scripts_nsg/nsg_to_FPGA.py:56-137; read as host.cpp:201-278 reads them).
+   graph_type is "HNSW" or "NSG". */
+int falcon_index_load_fpga(const char *index_dir, const char *graph_type, int32_t dim, int32_t storage,
+                           int32_t device, falcon_index **out);
+
+int falcon_index_info_get(const falcon_index *ix, falcon_index_info *info);
+int falcon_index_free(falcon_index *ix);
+
+/*
+ * Search nq queries.  Replaces the kernel launch + result migration of the
+ * reference host (host.cpp:852-993, vadd.cpp:11-95).
+ *   queries:      nq rows of `dim` floats, row stride query_stride floats
+ *   entry_points: per-query entry ids, or NULL for the index entry point
+ *                 (the reference sets every query to the global entry,
+ *                 host.cpp:711-713)
+ *   params:       one falcon_search_params, or nq of them when
+ *                 per_query_params != 0 (mixed k/ef/mc in one launch)
+ *   out_ids/out_dists: nq rows of out_stride (>= every k); the first k of a
+ *                 row are the results best-first, the rest -1 / 1e20
+ *   out_hops/out_visited: per query (may be NULL); hops = 1 + popped
+ *                 candidates, visited = Bloom-accepted neighbours
+ *                 (the reference's mem_debug[2q], [2q+1])
+ *   memory:       FALCON_MEM_HOST (pageable or pinned host buffers; copies are
+ *                 made on `stream`) or FALCON_MEM_DEVICE (all buffers on the
+ *                 index's device)
+ *   stream:       cudaStream_t (NULL = the legacy default stream); the call
+ *                 returns after the results are in place for host memory and
+ *                 after enqueueing for device memory.
+ */
+int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t query_stride,
+                  const int32_t *entry_points, const falcon_search_params *params, int32_t per_query_params,
+                  int32_t *out_ids, float *out_dists, int32_t out_stride, int32_t *out_hops,
+                  int32_t *out_visited, int32_t memory, void *stream);
+
+/*
+ * The reference kernel's own argument list (vadd.cpp:11-95, one channel),
+ * on host buffers in the reference layout, for hosts that bind `vadd`
+ * directly: query_vectors nq x pad16(dim) floats, db_vectors and links_base
+ * in the FPGA file layout, out_id/out_dist nq x ef, mem_debug nq x 2
+ * (hops, visited).  query_batch_size and max_bloom_out_burst_size only shape
+ * the FPGA pipeline and do not change results; they are validated and
+ * otherwise ignored.
+ */
+int falcon_vadd(int32_t query_num, int32_t query_batch_size, int32_t ef, int32_t candidate_queue_runtime_size,
+                int32_t max_cand_batch_size, int32_t max_async_stage_num, int32_t runtime_n_bucket_addr_bits,
+                uint32_t hash_seed, int32_t max_bloom_out_burst_size, int32_t max_link_num_base, int32_t dim,
+                int64_t num_db_vec, const int32_t *entry_point_ids, const float *query_vectors,
+                const void *db_vectors, const void *links_base, int32_t *out_id, float *out_dist,
+                int32_t *mem_debug, int32_t device);
+
+/* Thread-local description of the last error on this thread. */
+const char *falcon_last_error(void);
+
+/* Library build information (architecture, version). */
+const char *falcon_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FALCON_H */

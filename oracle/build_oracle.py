@@ -1,0 +1,139 @@
+"""Build recipe for the parity oracle (test infrastructure only).
+
+Outputs:
+  oracle/liboracle.so               the C restatement (falcon_oracle.c)
+  oracle/_ref/libfalcon_ref_d{D}.so the reference's own v1.3 HLS kernel headers
+                                    compiled as plain C++ through the harness
+                                    in oracle/ref_harness/ (one per dimension D)
+  oracle/_ref/libhnswlib_ref.so     the reference's vendored hnswlib (graph
+                                    builder + CPU search baseline)
+  oracle/_ref/murmur_golden,
+  oracle/_ref/bloom_golden          drivers around the reference's software
+                                    Murmur2 / Bloom, used to regenerate the
+                                    golden fixtures in tests/golden/
+
+The reference builds need the reference checkout at REF_ROOT; when it is
+absent (the GPU box) only the prebuilt files are used.  Reference sources are
+compiled where they lie; the only copies are transient ones in a temporary
+directory for the v1.3 kernel headers, which get three build-time edits
+(listed in ref_harness/ref_inter_harness.cpp) before compilation.
+"""
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_ROOT = "/root/reference"
+REF_V13 = os.path.join(REF_ROOT, "FPGA_multi_DDR", "FPGA_inter_query_v1.3_longer_FIFO_alt_PR", "src")
+REF_HNSWLIB = os.path.join(REF_ROOT, "networked_FPGA", "CPU_programs_oldest", "hnswlib")
+REF_MURMUR = os.path.join(REF_ROOT, "unit_tests", "bloom_and_hash", "sw_murmur2", "murmur2.cpp")
+REF_SWBLOOM = os.path.join(REF_ROOT, "unit_tests", "bloom_and_hash", "sw_bloom")
+REF_DIMS = (96, 128, 384)
+REF_OUT = os.path.join(HERE, "_ref")
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("build failed: %s\n%s" % (" ".join(cmd), r.stdout[-4000:]))
+
+
+def _stale(out, srcs):
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(s) > t for s in srcs if os.path.exists(s))
+
+
+def build_oracle(force=False):
+    src = os.path.join(HERE, "falcon_oracle.c")
+    out = os.path.join(HERE, "liboracle.so")
+    if force or _stale(out, [src]):
+        _run(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math",
+              "-pthread", src, "-o", out + ".tmp", "-lm"])
+        os.replace(out + ".tmp", out)
+    return out
+
+
+_EDITS = [
+    # constructor-local arrays the HLS code points members at -> heap storage
+    ("priority_queue.hpp", r"result_t queue_array\[hardware_queue_size\];",
+     "result_t* queue_array = new result_t[hardware_queue_size];"),
+    ("bloom_filter.hpp", r"ap_uint<512> hash_buckets\[num_512b_buckets_int\];",
+     "ap_uint<512>* hash_buckets = new ap_uint<512>[num_512b_buckets_int];"),
+    # result-queue hardware size 64 -> 256 (slots past ef are inert)
+    ("constants.hpp", r"const int hardware_result_queue_size = 64;",
+     "const int hardware_result_queue_size = 256;"),
+]
+
+
+def _patched_v13_copy(dst, dim):
+    names = ["constants.hpp", "types.hpp", "utils.hpp", "priority_queue.hpp", "bloom_filter.hpp",
+             "compute.hpp", "DRAM_utils.hpp", "scheduler.hpp"]
+    for n in names:
+        shutil.copy(os.path.join(REF_V13, n), os.path.join(dst, n))
+    for fname, pat, rep in _EDITS:
+        p = os.path.join(dst, fname)
+        s = open(p).read()
+        s2, k = re.subn(pat, rep, s)
+        if k != 1:
+            raise RuntimeError("reference edit did not apply to %s: %s" % (fname, pat))
+        open(p, "w").write(s2)
+    p = os.path.join(dst, "constants.hpp")
+    s = open(p).read()
+    s2, k = re.subn(r"#define D 128\b", "#define D %d" % dim, s)
+    if k != 1:
+        raise RuntimeError("could not set D in constants.hpp")
+    open(p, "w").write(s2)
+
+
+def build_ref(force=False):
+    """Build the reference-derived checkers.  Returns False if the reference
+    checkout is absent (prebuilt files are then used as they are)."""
+    if not os.path.isdir(REF_ROOT):
+        return False
+    os.makedirs(REF_OUT, exist_ok=True)
+    shim = os.path.join(HERE, "ref_harness", "shim")
+    harness = os.path.join(HERE, "ref_harness", "ref_inter_harness.cpp")
+    for dim in REF_DIMS:
+        out = os.path.join(REF_OUT, "libfalcon_ref_d%d.so" % dim)
+        srcs = [harness] + [os.path.join(shim, f) for f in os.listdir(shim)] + [os.path.abspath(__file__)]
+        if not force and not _stale(out, srcs):
+            continue
+        with tempfile.TemporaryDirectory() as td:
+            _patched_v13_copy(td, dim)
+            _run(["g++", "-O1", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math",
+                  "-Wno-unknown-pragmas", "-pthread", "-I", shim, "-I", td, harness, "-o", out + ".tmp"])
+        os.replace(out + ".tmp", out)
+    out = os.path.join(REF_OUT, "libhnswlib_ref.so")
+    src = os.path.join(HERE, "ref_harness", "hnswlib_ref.cpp")
+    if force or _stale(out, [src]):
+        # -mavx2 (not -march=native): the library travels to other x86 hosts.
+        _run(["g++", "-O3", "-mavx2", "-mfma", "-std=c++17", "-fPIC", "-shared", "-pthread", "-I", REF_HNSWLIB,
+              src, "-o", out + ".tmp"])
+        os.replace(out + ".tmp", out)
+    out = os.path.join(REF_OUT, "murmur_golden")
+    src = os.path.join(HERE, "ref_harness", "murmur_golden.cpp")
+    if force or _stale(out, [src]):
+        with tempfile.TemporaryDirectory() as td:
+            obj = os.path.join(td, "murmur2.o")
+            _run(["g++", "-O1", "-c", "-Dmain=reference_murmur2_demo_main", REF_MURMUR, "-o", obj])
+            _run(["g++", "-O1", src, obj, "-o", out])
+    out = os.path.join(REF_OUT, "bloom_golden")
+    src = os.path.join(HERE, "ref_harness", "bloom_golden.cpp")
+    if force or _stale(out, [src]):
+        _run(["g++", "-O1", "-I", REF_SWBLOOM, src, "-o", out])
+    return True
+
+
+def build_all(force=False):
+    build_oracle(force)
+    return build_ref(force)
+
+
+if __name__ == "__main__":
+    ok = build_all(force="--force" in sys.argv)
+    print("oracle built; reference checkers %s" % ("built" if ok else "skipped (no reference checkout)"))

@@ -1,0 +1,295 @@
+"""TEST INFRASTRUCTURE ONLY: Python access to the parity oracle.
+
+  search(...)          the C restatement (oracle/falcon_oracle.c)
+  ref_inter_search(...) the reference's own v1.3 HLS kernel compiled as C++
+                        (oracle/_ref/libfalcon_ref_d{D}.so)
+  Hnsw                 the reference's vendored hnswlib (oracle/_ref/libhnswlib_ref.so)
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
+arm use this module.  The product library never does.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+F32, BF16, FP8 = 0, 1, 2
+
+
+class FoGraph(ctypes.Structure):
+    _fields_ = [
+        ("vectors", ctypes.c_void_p),
+        ("scales", ctypes.c_void_p),
+        ("elem", ctypes.c_int),
+        ("vec_stride", ctypes.c_int64),
+        ("vectors_f32", ctypes.c_void_p),
+        ("vec_stride_f32", ctypes.c_int64),
+        ("links", ctypes.c_void_p),
+        ("link_stride", ctypes.c_int64),
+        ("ids_offset", ctypes.c_int),
+        ("max_degree", ctypes.c_int),
+        ("dim", ctypes.c_int),
+        ("dpad", ctypes.c_int),
+        ("n", ctypes.c_int64),
+    ]
+
+
+class FoParams(ctypes.Structure):
+    _fields_ = [
+        ("k", ctypes.c_int), ("ef", ctypes.c_int), ("mc", ctypes.c_int), ("mg", ctypes.c_int),
+        ("cand_queue_size", ctypes.c_int), ("bloom_bits", ctypes.c_int), ("hash_seed", ctypes.c_uint32),
+        ("mode", ctypes.c_int), ("channels", ctypes.c_int), ("rerank", ctypes.c_int), ("max_hops", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        p = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(p):
+            import build_oracle   # noqa: F401  (oracle/ on sys.path)
+            build_oracle.build_oracle()
+        _lib = ctypes.CDLL(p)
+        _lib.fo_search.restype = ctypes.c_int
+        _lib.fo_search.argtypes = [ctypes.POINTER(FoGraph), ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                   ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p,
+                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        _lib.fo_murmur2_keylen4.restype = ctypes.c_uint32
+        _lib.fo_murmur2_keylen4.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
+        _lib.fo_fp8e4m3_to_f32.restype = ctypes.c_float
+        _lib.fo_fp8e4m3_to_f32.argtypes = [ctypes.c_uint8]
+        _lib.fo_queue_insert_sort.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                              ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        _lib.fo_bloom_stream.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p]
+        _lib.fo_l2_batch.argtypes = [ctypes.POINTER(FoGraph), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                     ctypes.c_void_p]
+    return _lib
+
+
+def pad16(d):
+    return (d + 15) // 16 * 16
+
+
+class OracleGraph:
+    """Keeps the arrays alive and builds the fo_graph view.
+
+    vectors_f32: [n, dim] float32; links: reference layout rows.
+    elem/stored: the traversal storage (F32, or BF16 uint16 codes [n, dpad],
+    or FP8 uint8 codes [n, dpad] + scales [n])."""
+
+    def __init__(self, vectors_f32, links, max_degree, ids_offset=16, elem=F32, stored=None, scales=None):
+        n, dim = vectors_f32.shape
+        self.dim, self.dpad, self.n = dim, pad16(dim), n
+        v = np.zeros((n, self.dpad), dtype=np.float32)
+        v[:, :dim] = vectors_f32
+        self.v32 = v
+        self.links = np.ascontiguousarray(links, dtype=np.int32)
+        self.stored = v if elem == F32 else np.ascontiguousarray(stored)
+        self.scales = None if scales is None else np.ascontiguousarray(scales, dtype=np.float32)
+        g = FoGraph()
+        g.vectors = self.stored.ctypes.data
+        g.scales = self.scales.ctypes.data if self.scales is not None else None
+        g.elem = elem
+        g.vec_stride = self.stored.shape[1]
+        g.vectors_f32 = v.ctypes.data
+        g.vec_stride_f32 = self.dpad
+        g.links = self.links.ctypes.data
+        g.link_stride = self.links.shape[1]
+        g.ids_offset = ids_offset
+        g.max_degree = max_degree
+        g.dim = dim
+        g.dpad = self.dpad
+        g.n = n
+        self.g = g
+
+
+def make_params(k=10, ef=64, mc=1, mg=1, cand_queue_size=32, bloom_bits=16, hash_seed=1, mode="inter",
+                channels=4, rerank=False, max_hops=0):
+    p = FoParams()
+    p.k, p.ef, p.mc, p.mg = k, ef, mc, mg
+    p.cand_queue_size, p.bloom_bits, p.hash_seed = cand_queue_size, bloom_bits, hash_seed
+    p.mode = 0 if mode == "inter" else 1
+    p.channels, p.rerank, p.max_hops = channels, 1 if rerank else 0, max_hops
+    return p
+
+
+def search(og, queries, entries, params, out_stride=None, threads=None):
+    """params: one FoParams or a list (one per query).  Returns ids, dists, hops, visited, status."""
+    q = np.ascontiguousarray(queries, dtype=np.float32)
+    nq = q.shape[0]
+    e = np.ascontiguousarray(np.broadcast_to(np.asarray(entries, dtype=np.int32), (nq,)))
+    if isinstance(params, FoParams):
+        parr, stride, kmax = params, 0, params.k
+    else:
+        parr = (FoParams * nq)(*params)
+        stride, kmax = 1, max(p.k for p in params)
+    os_ = out_stride or kmax
+    ids = np.empty((nq, os_), dtype=np.int32)
+    d = np.empty((nq, os_), dtype=np.float32)
+    hops = np.empty(nq, dtype=np.int32)
+    vis = np.empty(nq, dtype=np.int32)
+    threads = threads or min(32, os.cpu_count() or 1)
+    rc = lib().fo_search(ctypes.byref(og.g), ctypes.byref(parr) if stride == 0 else parr, stride, q.ctypes.data,
+                         q.shape[1], e.ctypes.data, nq, os_, ids.ctypes.data, d.ctypes.data, hops.ctypes.data,
+                         vis.ctypes.data, threads)
+    if rc < 0:
+        raise ValueError("oracle rejected arguments: %d" % rc)
+    return ids, d, hops, vis, rc
+
+
+def murmur2(key, seed):
+    return int(lib().fo_murmur2_keylen4(key & 0xffffffff, seed & 0xffffffff))
+
+
+def fp8_to_f32(code):
+    return float(lib().fo_fp8e4m3_to_f32(code))
+
+
+def queue_insert_sort(values, ids, n, v15=False):
+    """Insert a stream into an n-slot systolic queue, then sort; returns the
+    queue best-first (ids, dists), like the reference's unit test kernel."""
+    vals = np.ascontiguousarray(values, dtype=np.float32)
+    iv = np.ascontiguousarray(ids, dtype=np.int32)
+    d = np.empty(n, dtype=np.float32)
+    i = np.empty(n, dtype=np.int32)
+    lib().fo_queue_insert_sort(d.ctypes.data, i.ctypes.data, n, vals.ctypes.data, iv.ctypes.data, len(vals),
+                               1 if v15 else 0)
+    return i[::-1].copy(), d[::-1].copy()
+
+
+def bloom_stream(keys, bits=16, seed=1):
+    k = np.ascontiguousarray(keys, dtype=np.uint32)
+    out = np.empty(len(k), dtype=np.uint8)
+    lib().fo_bloom_stream(k.ctypes.data, len(k), bits, seed, out.ctypes.data)
+    return out
+
+
+def l2_batch(og, query, ids):
+    q = np.ascontiguousarray(query, dtype=np.float32)
+    i = np.ascontiguousarray(ids, dtype=np.int32)
+    out = np.empty(len(i), dtype=np.float32)
+    lib().fo_l2_batch(ctypes.byref(og.g), q.ctypes.data, i.ctypes.data, len(i), out.ctypes.data)
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Reference harness (the reference's own HLS kernel code run as C++)
+# ---------------------------------------------------------------------------
+_ref_libs = {}
+
+
+def ref_available(dim):
+    return os.path.exists(os.path.join(REF_DIR, "libfalcon_ref_d%d.so" % dim))
+
+
+def _ref_lib(dim):
+    if dim not in _ref_libs:
+        p = os.path.join(REF_DIR, "libfalcon_ref_d%d.so" % dim)
+        L = ctypes.CDLL(p)
+        L.ref_inter_search.restype = ctypes.c_int
+        L.ref_inter_search.argtypes = [ctypes.c_int] * 6 + [ctypes.c_uint, ctypes.c_int, ctypes.c_int] + \
+            [ctypes.c_void_p] * 7
+        _ref_libs[dim] = L
+    return _ref_libs[dim]
+
+
+def ref_inter_search(vectors, links_ref, max_degree, queries, entries, ef=64, cand_queue_size=32, mc=1, mg=1,
+                     bloom_bits=16, hash_seed=1, burst=16):
+    """Run the reference kernel pipeline (one channel) on reference-layout data."""
+    n, dim = vectors.shape
+    L = _ref_lib(dim)
+    dp = pad16(dim)
+    db = np.zeros((n, dp + 16), dtype=np.float32)
+    db[:, :dim] = vectors
+    q = np.zeros((len(queries), dp), dtype=np.float32)
+    q[:, :dim] = queries
+    e = np.ascontiguousarray(np.broadcast_to(np.asarray(entries, dtype=np.int32), (len(queries),)))
+    lk = np.ascontiguousarray(links_ref, dtype=np.int32)
+    nq = len(queries)
+    oid = np.empty((nq, ef), dtype=np.int32)
+    od = np.empty((nq, ef), dtype=np.float32)
+    dbg = np.empty((nq, 2), dtype=np.int32)
+    rc = L.ref_inter_search(nq, ef, cand_queue_size, mc, mg, bloom_bits, hash_seed, burst, max_degree, e.ctypes.data,
+                            q.ctypes.data, db.ctypes.data, lk.ctypes.data, oid.ctypes.data, od.ctypes.data,
+                            dbg.ctypes.data)
+    if rc != 0:
+        raise ValueError("reference harness rejected arguments")
+    return oid, od, dbg[:, 0].copy(), dbg[:, 1].copy()
+
+
+# ---------------------------------------------------------------------------
+# Reference hnswlib
+# ---------------------------------------------------------------------------
+class Hnsw:
+    def __init__(self, handle, dim):
+        self.h, self.dim = handle, dim
+
+    @staticmethod
+    def _L():
+        p = os.path.join(REF_DIR, "libhnswlib_ref.so")
+        L = ctypes.CDLL(p)
+        L.hnsw_build.restype = ctypes.c_void_p
+        L.hnsw_build.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        L.hnsw_from_graph.restype = ctypes.c_void_p
+        L.hnsw_from_graph.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_int]
+        L.hnsw_info.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 4
+        L.hnsw_export_level0.argtypes = [ctypes.c_void_p] * 4
+        L.hnsw_search.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        L.hnsw_free.argtypes = [ctypes.c_void_p]
+        return L
+
+    @classmethod
+    def available(cls):
+        return os.path.exists(os.path.join(REF_DIR, "libhnswlib_ref.so"))
+
+    @classmethod
+    def build(cls, vectors, M, ef_construction, seed):
+        v = np.ascontiguousarray(vectors, dtype=np.float32)
+        h = cls._L().hnsw_build(v.shape[0], v.shape[1], M, ef_construction, seed, v.ctypes.data)
+        obj = cls(h, v.shape[1])
+        obj._keep = v
+        return obj
+
+    @classmethod
+    def from_graph(cls, vectors, adjacency, entry):
+        v = np.ascontiguousarray(vectors, dtype=np.float32)
+        adj = np.ascontiguousarray(adjacency, dtype=np.int32)
+        counts = (adj >= 0).sum(1).astype(np.int32)
+        h = cls._L().hnsw_from_graph(v.shape[0], v.shape[1], adj.shape[1], v.ctypes.data, adj.ctypes.data,
+                                     counts.ctypes.data, int(entry))
+        obj = cls(h, v.shape[1])
+        obj._keep = (v, adj, counts)
+        return obj
+
+    def level0(self):
+        L = self._L()
+        n = ctypes.c_int64()
+        md = ctypes.c_int()
+        ep = ctypes.c_int()
+        ml = ctypes.c_int()
+        L.hnsw_info(self.h, ctypes.byref(n), ctypes.byref(md), ctypes.byref(ep), ctypes.byref(ml))
+        links = np.empty((n.value, md.value), dtype=np.int32)
+        counts = np.empty(n.value, dtype=np.int32)
+        labels = np.empty(n.value, dtype=np.int32)
+        L.hnsw_export_level0(self.h, links.ctypes.data, counts.ctypes.data, labels.ctypes.data)
+        return links, counts, labels, ep.value, ml.value
+
+    def search(self, queries, k, ef, threads):
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        lab = np.empty((len(q), k), dtype=np.int64)
+        d = np.empty((len(q), k), dtype=np.float32)
+        self._L().hnsw_search(self.h, q.ctypes.data, len(q), self.dim, k, ef, threads, lab.ctypes.data, d.ctypes.data)
+        return lab, d
+
+    def free(self):
+        if self.h:
+            self._L().hnsw_free(self.h)
+            self.h = None
