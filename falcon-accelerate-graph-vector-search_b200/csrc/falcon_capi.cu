@@ -264,6 +264,31 @@ int falcon_index_info_get(const falcon_index *ix, falcon_index_info *info)
     return FALCON_OK;
 }
 
+int falcon_index_copy_storage(const falcon_index *ix, int32_t which, void *dst, int64_t bytes)
+{
+    if (!ix || !dst) return set_error(FALCON_ERR_ARG, "null argument");
+    const int64_t nd = ix->n * (int64_t)ix->dpad;
+    DeviceGuard guard(ix->device);
+    cudaError_t e = cudaSuccess;
+    if (which == FALCON_STORE_F32) {
+        if (bytes != nd * 4) return set_error(FALCON_ERR_ARG, "F32 storage is %lld bytes", (long long)(nd * 4));
+        e = cudaMemcpy(dst, ix->d_f32, bytes, cudaMemcpyDeviceToHost);
+    } else if (which == FALCON_STORE_BF16) {
+        if (!ix->d_bf16) return set_error(FALCON_ERR_ARG, "index holds no BF16 storage");
+        if (bytes != nd * 2) return set_error(FALCON_ERR_ARG, "BF16 storage is %lld bytes", (long long)(nd * 2));
+        e = cudaMemcpy(dst, ix->d_bf16, bytes, cudaMemcpyDeviceToHost);
+    } else if (which == FALCON_STORE_FP8) {
+        if (!ix->d_fp8) return set_error(FALCON_ERR_ARG, "index holds no FP8 storage");
+        if (bytes != nd + ix->n * 4) return set_error(FALCON_ERR_ARG, "FP8 storage is %lld bytes", (long long)(nd + ix->n * 4));
+        e = cudaMemcpy(dst, ix->d_fp8, nd, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy((char *)dst + nd, ix->d_scales, ix->n * 4, cudaMemcpyDeviceToHost);
+    } else {
+        return set_error(FALCON_ERR_ARG, "unknown storage %d", which);
+    }
+    if (e != cudaSuccess) return set_error(FALCON_ERR_CUDA, "copy storage: %s", cudaGetErrorString(e));
+    return FALCON_OK;
+}
+
 static bool read_file(const std::string &path, std::vector<char> &buf)
 {
     FILE *f = fopen(path.c_str(), "rb");

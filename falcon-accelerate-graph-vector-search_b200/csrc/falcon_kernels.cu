@@ -342,11 +342,17 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
     bool r_sorted = true, c_sorted = true;
     float rq0 = kLarge, cq0 = kLarge;
 
-    const int entry = A.entries ? A.entries[qi] : A.default_entry;
+    int entry = A.entries ? A.entries[qi] : A.default_entry;
     const int mc = P.mc, mg = P.mg;
+    int head = 0, inflight = 1, hops = 1, visited = 0;
+    if (entry < 0 || (int64_t)entry >= g.n) {   // bad entry from a device-memory caller: empty result
+        if (lane == 0) atomicOr(A.status, 2);
+        entry = 0;
+        inflight = 0;
+        hops = 0;
+    }
     if (lane == 0) { fifo[0] = entry; fifo_len[0] = 1; }
     __syncwarp();
-    int head = 0, inflight = 1, hops = 1, visited = 0;
     bool truncated = false;
 
     while (inflight > 0) {

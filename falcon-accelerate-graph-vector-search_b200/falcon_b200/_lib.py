@@ -87,6 +87,7 @@ SIGNATURES = {
     "falcon_index_load_fpga": (_I32, [ctypes.c_char_p, ctypes.c_char_p, _I32, _I32, _I32, ctypes.POINTER(_VP)]),
     "falcon_index_info_get": (_I32, [_VP, ctypes.POINTER(IndexInfo)]),
     "falcon_index_free": (_I32, [_VP]),
+    "falcon_index_copy_storage": (_I32, [_VP, _I32, _VP, _I64]),
     "falcon_search": (_I32, [_VP, _VP, _I64, _I64, _VP, ctypes.POINTER(SearchParams), _I32,
                              _VP, _VP, _I32, _VP, _VP, _I32, _VP]),
     "falcon_vadd": (_I32, [_I32, _I32, _I32, _I32, _I32, _I32, _I32, ctypes.c_uint32, _I32, _I32, _I32, _I64,

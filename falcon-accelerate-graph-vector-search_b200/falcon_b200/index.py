@@ -94,6 +94,25 @@ class FalconIndex:
         _lib.check(_lib.load().falcon_index_info_get(self._h, ctypes.byref(inf)))
         return inf
 
+    def storage(self, which="f32"):
+        """Copy a resident storage array back: f32 [n, dpad] float32, bf16
+        [n, dpad] uint16 codes, fp8 ([n, dpad] uint8 codes, [n] float32 scales)."""
+        inf = self.info()
+        n, dp = inf.num_vectors, inf.dim_padded
+        lib = _lib.load()
+        if which == "f32":
+            out = np.empty((n, dp), dtype=np.float32)
+        elif which == "bf16":
+            out = np.empty((n, dp), dtype=np.uint16)
+        elif which == "fp8":
+            out = np.empty(n * dp + 4 * n, dtype=np.uint8)
+        else:
+            raise ValueError(which)
+        _lib.check(lib.falcon_index_copy_storage(self._h, _STORE[which], out.ctypes.data, out.nbytes))
+        if which == "fp8":
+            return out[:n * dp].reshape(n, dp), out[n * dp:].view(np.float32).copy()
+        return out
+
     def close(self):
         if getattr(self, "_h", None):
             _lib.load().falcon_index_free(self._h)

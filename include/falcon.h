@@ -126,6 +126,15 @@ int falcon_index_load_fpga(const char *index_dir, const char *graph_type, int32_
                            int32_t device, falcon_index **out);
 
 int falcon_index_info_get(const falcon_index *ix, falcon_index_info *info);
+
+/* Copy one resident storage array of the index back to host memory (for
+   checkpointing the device-ready index, and for checking the encoders):
+   which = FALCON_STORE_F32 (n x dim_padded floats), FALCON_STORE_BF16
+   (n x dim_padded uint16 codes), FALCON_STORE_FP8 (n x dim_padded uint8 codes
+   followed by n float scales).  `bytes` must equal the array size.  The
+   reference keeps its index only in host files (hnsw.py:264-377); this has no
+   kernel-side counterpart there. */
+int falcon_index_copy_storage(const falcon_index *ix, int32_t which, void *dst, int64_t bytes);
 int falcon_index_free(falcon_index *ix);
 
 /*

@@ -1,0 +1,104 @@
+"""CPU: the oracle restatement pinned against the reference's own code.
+
+- Murmur2 KeyLen4 and the Bloom filter against golden vectors produced by the
+  reference's software hash/Bloom (unit_tests/bloom_and_hash/sw_*).
+- The systolic queue's insert+sort against std::sort ordering, as the
+  reference's priority-queue unit test checks it
+  (unit_tests/priority_queue/src/host.cpp:49-59,121-152).
+- Whole traversals against fixtures produced by the reference's inter-query
+  v1.3 kernel pipeline compiled as C++, and, when the reference-derived
+  library is present, against that pipeline live on fresh seeded graphs.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from helpers import GOLDEN, fixture, fixture_graph, oracle_graph, small_graph
+
+
+def test_murmur2_golden(oracle_mod):
+    rows = json.load(open(os.path.join(GOLDEN, "murmur2_keylen4.json")))
+    assert len(rows) >= 200
+    for r in rows:
+        assert r["murmur2"] == r["keylen4"]          # reference's two hash functions agree
+        assert oracle_mod.murmur2(r["key"], r["seed"]) == r["keylen4"]
+
+
+def test_bloom_golden_stream(oracle_mod):
+    f = fixture("bloom_sw_stream.npz")
+    valid = oracle_mod.bloom_stream(f["keys"].astype(np.uint32), bits=int(f["bits"]), seed=int(f["seed"]))
+    assert np.array_equal(valid, f["valid"])
+    # the stream contains repeats and false positives: both outcomes occur
+    assert 0 < valid.sum() < len(valid)
+
+
+@pytest.mark.parametrize("n,nin,v15", [(64, 200, False), (64, 64, False), (32, 500, True), (17, 40, False)])
+def test_queue_sort_matches_sorted(oracle_mod, n, nin, v15):
+    rng = np.random.default_rng(n * 1000 + nin)
+    vals = rng.random(nin).astype(np.float32)
+    ids, d = oracle_mod.queue_insert_sort(vals, np.arange(nin), n, v15)
+    m = min(n, nin)
+    order = np.argsort(vals, kind="stable")[:m]
+    assert np.array_equal(d[:m], vals[order])
+    assert np.array_equal(ids[:m], order)
+    assert np.all(d[m:] == np.float32(1e20)) and np.all(ids[m:] == -1)
+
+
+@pytest.mark.parametrize("name", ["traversal_d128_md32.npz", "traversal_d96_md64.npz"])
+def test_traversal_golden(oracle_mod, name):
+    f, g, q = fixture_graph(name)
+    og = oracle_graph(oracle_mod, g)
+    for i, (ef, mc, mg, cq, bits) in enumerate(f["params"]):
+        p = oracle_mod.make_params(k=int(ef), ef=int(ef), mc=int(mc), mg=int(mg), cand_queue_size=int(cq),
+                                   bloom_bits=int(bits))
+        ids, d, hops, vis, rc = oracle_mod.search(og, q, g.entry_point, p)
+        assert rc == 0
+        assert np.array_equal(ids, f["ids_%d" % i])
+        assert np.array_equal(d.view(np.uint32), f["dists_%d" % i].view(np.uint32))
+        assert np.array_equal(hops, f["hops_%d" % i])
+        assert np.array_equal(vis, f["visited_%d" % i])
+
+
+@pytest.mark.parametrize("kind,dim,md,ef,mc,mg", [
+    ("sift", 128, 32, 64, 1, 1), ("sift", 128, 32, 64, 1, 4), ("unit", 96, 64, 64, 2, 3),
+    ("unit", 384, 64, 32, 2, 2), ("sift", 128, 32, 200, 3, 5)])
+def test_traversal_live_against_reference_pipeline(oracle_mod, kind, dim, md, ef, mc, mg):
+    if not oracle_mod.ref_available(dim):
+        pytest.skip("reference-derived pipeline library not built on this host")
+    g, q = small_graph(kind, 2000, dim, md, 12, seed=3)
+    og = oracle_graph(oracle_mod, g)
+    ids, d, hops, vis, _ = oracle_mod.search(og, q, g.entry_point, oracle_mod.make_params(k=ef, ef=ef, mc=mc, mg=mg))
+    rid, rd, rh, rv = oracle_mod.ref_inter_search(g.vectors, g.links, md, q, g.entry_point, ef=ef, mc=mc, mg=mg)
+    assert np.array_equal(ids, rid)
+    assert np.array_equal(d.view(np.uint32), rd.view(np.uint32))
+    assert np.array_equal(hops, rh)
+    assert np.array_equal(vis, rv)
+
+
+def test_fp8_decode_table(oracle_mod):
+    # OCP E4M3: bias 7, subnormals m/8*2^-6, 0x7f/0xff NaN, max 448
+    assert oracle_mod.fp8_to_f32(0x00) == 0.0
+    assert oracle_mod.fp8_to_f32(0x01) == 2.0 ** -9
+    assert oracle_mod.fp8_to_f32(0x08) == 2.0 ** -6
+    assert oracle_mod.fp8_to_f32(0x38) == 1.0
+    assert oracle_mod.fp8_to_f32(0x7e) == 448.0
+    assert oracle_mod.fp8_to_f32(0xfe) == -448.0
+    assert np.isnan(oracle_mod.fp8_to_f32(0x7f))
+
+
+def test_oracle_rejects_bad_args(oracle_mod):
+    g, q = small_graph("sift", 2000, 128, 32, 4, seed=3)
+    og = oracle_graph(oracle_mod, g)
+    with pytest.raises(ValueError):
+        oracle_mod.search(og, q, g.entry_point, oracle_mod.make_params(mc=0))
+    with pytest.raises(ValueError):
+        oracle_mod.search(og, q, g.entry_point, oracle_mod.make_params(mode="intra", channels=3))
+
+
+def test_oracle_max_hops_truncates(oracle_mod):
+    g, q = small_graph("sift", 2000, 128, 32, 8, seed=3)
+    og = oracle_graph(oracle_mod, g)
+    ids, d, hops, vis, rc = oracle_mod.search(og, q, g.entry_point, oracle_mod.make_params(max_hops=5))
+    assert rc == 1 and hops.max() <= 5
