@@ -380,7 +380,10 @@ int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t qu
         any_rerank |= (qp[i].rerank != 0 && qp[i].precision != FALCON_PREC_F32);
     }
     if (out_stride < k_max) return set_error(FALCON_ERR_ARG, "out_stride %d < k %d", out_stride, k_max);
-    if (mode == FALCON_MODE_INTRA) return set_error(FALCON_ERR_UNSUPPORTED, "intra-query mode not built in this library");
+    if (mode == FALCON_MODE_INTRA)
+        for (int64_t i = 0; i < np; i++)
+            if (qp[i].channels != qp[0].channels)
+                return set_error(FALCON_ERR_UNSUPPORTED, "intra-query mode: one channel count per call");
     if (any_rerank)
         for (int64_t i = 0; i < np; i++)
             if (!(qp[i].rerank != 0 && qp[i].precision != FALCON_PREC_F32))
@@ -462,6 +465,7 @@ int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t qu
         a.ef_max = ef_max;
         a.mc_max = mc_max;
         a.mg_max = mg_max;
+        a.channels = (mode == FALCON_MODE_INTRA) ? qp[0].channels : 0;
         int32_t *final_ids = a.out_ids;
         float *final_d = a.out_d;
         if (any_rerank) {

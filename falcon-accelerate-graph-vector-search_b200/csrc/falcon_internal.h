@@ -65,6 +65,7 @@ struct SearchLaunch {
     int32_t bloom_bits_max;         // shared-memory Bloom size per warp/channel
     int32_t ef_max;
     int32_t mc_max, mg_max;
+    int32_t channels;               // 0: inter-query (warp per query); else intra-query block of `channels` warps
 };
 
 struct RerankLaunch {

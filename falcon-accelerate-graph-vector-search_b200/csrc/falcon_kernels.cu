@@ -191,66 +191,85 @@ __device__ __forceinline__ float batch_distances(const float (&q)[VROWS][ET<ELEM
 }
 
 // ---------------------------------------------------------------------------
-// Result queue: positions lane*EPL+e, sorted descending (position 0 = worst).
-// One step = optional replacement of position 0, then step A (pairs 2j,2j+1)
-// and step B (pairs 2j+1,2j+2) with swap iff q[a] < q[b]
-// (priority_queue.hpp:29-57).  Returns whether this lane swapped anything.
+// Queues.  The reference keeps both queues in a systolic odd-even array
+// (priority_queue.hpp:9-166): an insertion replaces q[0] when the new distance
+// is smaller, then runs one even and one odd compare-swap phase; sort() runs
+// n phases.  That array holds its maximum in q[0] whenever an insertion is
+// tested, so it behaves entry for entry like a list sorted by
+// (distance, insertion age) in which an insertion happens iff d < max and
+// evicts the newest of the max-valued entries, and sort() leaves equal
+// distances oldest first.  Proof sketch: every operation is a min or a max,
+// so by the 0/1 principle it is enough to look at 0/1 arrays; there, at the
+// start of every step the zeros that precede the last 1 sit at even positions
+// >= 2 with 1s on both sides, an invariant that replacement at q[0] followed
+// by the two phases preserves, hence q[0] = 1 whenever any 1 is present, i.e.
+// q[0] is the maximum.  Equal distances never swap, so they keep insertion
+// order.  The same holds for the v1.5 variant (phases only after a
+// replacement) and for pop_top (after a sort).  The kernels therefore hold the
+// queues as sorted lists: a distance that is not below the current maximum
+// costs one comparison.
+//
+// Result list: position p = lane*EPL + e in ascending order; positions >= ef
+// hold evicted entries, which stay above every later insertion because the
+// maximum never increases.
 // ---------------------------------------------------------------------------
 template <int EPL>
-__device__ __forceinline__ bool rq_step(float (&d)[EPL], int (&id)[EPL], int lane, bool replace, float nd, int nid)
+__device__ __forceinline__ void rl_insert(float (&d)[EPL], int (&id)[EPL], int lane, float x, int xid)
 {
-    if (replace && lane == 0) { d[0] = nd; id[0] = nid; }
-    bool sw = false;
+    const unsigned full = __ballot_sync(kFull, d[EPL - 1] <= x);   // lanes entirely <= x: a prefix
+    const int f = __popc(full);
+    int c = 0;
 #pragma unroll
-    for (int e = 0; e + 1 < EPL; e += 2) {
-        if (d[e] < d[e + 1]) {
-            const float td = d[e]; d[e] = d[e + 1]; d[e + 1] = td;
-            const int ti = id[e]; id[e] = id[e + 1]; id[e + 1] = ti;
-            sw = true;
-        }
-    }
-    // step B: lane-internal pairs (e, e+1), e odd; cross pair (last of lane, first of next lane)
-    const float nb_d = __shfl_down_sync(kFull, d[0], 1);
-    const int nb_i = __shfl_down_sync(kFull, id[0], 1);
-    const float pv_d = __shfl_up_sync(kFull, d[EPL - 1], 1);
-    const int pv_i = __shfl_up_sync(kFull, id[EPL - 1], 1);
+    for (int e = 0; e < EPL; e++) c += (d[e] <= x) ? 1 : 0;
+    const int cf = __shfl_sync(kFull, c, f & 31);
+    const int pos = f * EPL + ((f < 32) ? cf : 0);
+    const float pd = __shfl_up_sync(kFull, d[EPL - 1], 1);
+    const int pi = __shfl_up_sync(kFull, id[EPL - 1], 1);
 #pragma unroll
-    for (int e = 1; e + 1 < EPL; e += 2) {
-        if (d[e] < d[e + 1]) {
-            const float td = d[e]; d[e] = d[e + 1]; d[e + 1] = td;
-            const int ti = id[e]; id[e] = id[e + 1]; id[e + 1] = ti;
-            sw = true;
-        }
+    for (int e = EPL - 1; e >= 0; e--) {
+        const int p = lane * EPL + e;
+        const float sd = (e == 0) ? pd : d[(e > 0) ? e - 1 : 0];
+        const int si = (e == 0) ? pi : id[(e > 0) ? e - 1 : 0];
+        if (p > pos) { d[e] = sd; id[e] = si; }
+        else if (p == pos) { d[e] = x; id[e] = xid; }
     }
-    if (lane < 31 && d[EPL - 1] < nb_d) { d[EPL - 1] = nb_d; id[EPL - 1] = nb_i; sw = true; }
-    if (lane > 0 && pv_d < d[0]) { d[0] = pv_d; id[0] = pv_i; sw = true; }
-    return sw;
 }
 
-// Candidate queue: position = lane (<= 32 entries).
-__device__ __forceinline__ bool cq_step(float &d, int &id, int lane, bool replace, float nd, int nid)
+// Value at warp-uniform position p of the result list.
+template <int EPL>
+__device__ __forceinline__ float rl_get(const float (&d)[EPL], int p)
 {
-    if (replace && lane == 0) { d = nd; id = nid; }
-    bool sw = false;
-    {   // step A: pairs (2j, 2j+1)
-        const float pd = __shfl_xor_sync(kFull, d, 1);
-        const int pi = __shfl_xor_sync(kFull, id, 1);
-        const bool left = !(lane & 1);
-        const bool swp = left ? (d < pd) : (pd < d);
-        if (swp) { d = pd; id = pi; sw = true; }
+    const int e0 = p % EPL;
+    float v = d[0];
+#pragma unroll
+    for (int e = 1; e < EPL; e++) v = (e == e0) ? d[e] : v;
+    return __shfl_sync(kFull, v, p / EPL);
+}
+
+// Candidate list: position = lane < cq, ascending; lanes >= cq are ignored.
+__device__ __forceinline__ void cl_insert(float &d, int &id, int lane, int cq, float x, int xid)
+{
+    const int pos = __popc(__ballot_sync(kFull, lane < cq && d <= x));
+    const float ud = __shfl_up_sync(kFull, d, 1);
+    const int ui = __shfl_up_sync(kFull, id, 1);
+    if (lane < cq) {
+        if (lane > pos) { d = ud; id = ui; }
+        else if (lane == pos) { d = x; id = xid; }
     }
-    {   // step B: pairs (2j+1, 2j+2)
-        const float dn = __shfl_down_sync(kFull, d, 1);
-        const int in = __shfl_down_sync(kFull, id, 1);
-        const float du = __shfl_up_sync(kFull, d, 1);
-        const int iu = __shfl_up_sync(kFull, id, 1);
-        if (lane & 1) {
-            if (lane < 31 && d < dn) { d = dn; id = in; sw = true; }
-        } else if (lane > 0) {
-            if (du < d) { d = du; id = iu; sw = true; }
-        }
+}
+
+// pop_top (priority_queue.hpp:131-165): take the best entry, a +large
+// placeholder enters at the worst end.
+__device__ __forceinline__ int cl_pop(float &d, int &id, int lane, int cq)
+{
+    const int pid = __shfl_sync(kFull, id, 0);
+    const float dn = __shfl_down_sync(kFull, d, 1);
+    const int in = __shfl_down_sync(kFull, id, 1);
+    if (lane < cq) {
+        d = (lane == cq - 1) ? kLarge : dn;
+        id = (lane == cq - 1) ? -1 : in;
     }
-    return sw;
+    return pid;
 }
 
 // ---------------------------------------------------------------------------
@@ -334,13 +353,12 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
     int ri[EPL];
 #pragma unroll
     for (int e = 0; e < EPL; e++) {
-        rd[e] = (lane * EPL + e < P.ef) ? kLarge : -kLarge;
+        rd[e] = (lane * EPL + e < P.ef) ? kLarge : __int_as_float(0x7f800000);   // placeholders, then +inf
         ri[e] = -1;
     }
-    float cd = (lane < P.cq) ? kLarge : -kLarge;
+    float cd = kLarge;
     int ci = -1;
-    bool r_sorted = true, c_sorted = true;
-    float rq0 = kLarge, cq0 = kLarge;
+    float rmax = kLarge, cmax = kLarge;   // current maxima (warp-uniform)
 
     int entry = A.entries ? A.entries[qi] : A.default_entry;
     const int mc = P.mc, mg = P.mg;
@@ -388,21 +406,20 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
                     }
                     const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane);
                     const int nt = min(NB, V - b0);
-                    for (int t = 0; t < nt; t++) {
-                        const float d = __shfl_sync(kFull, dist, t);
-                        const int id = sids[b0 + t];
-                        const bool ins = d < rq0;
-                        if (!r_sorted || ins) {
-                            const bool sw = rq_step<EPL>(rd, ri, lane, ins, d, id);
-                            r_sorted = !__any_sync(kFull, sw);
-                            rq0 = __shfl_sync(kFull, rd[0], 0);
-                        }
-                        if (ins) {   // forwarded to the scheduler's candidate queue (insert_only)
-                            const bool cins = d < cq0;
-                            if (!c_sorted || cins) {
-                                const bool sw = cq_step(cd, ci, lane, cins, d, id);
-                                c_sorted = !__any_sync(kFull, sw);
-                                cq0 = __shfl_sync(kFull, cd, 0);
+                    // results collection (DRAM_utils.hpp:421-438) in stream order; the
+                    // maximum only decreases, so a distance not below it now never will be
+                    unsigned m = __ballot_sync(kFull, lane < nt && dist < rmax);
+                    while (m) {
+                        const int t = __ffs(m) - 1;
+                        m &= m - 1;
+                        const float dd = __shfl_sync(kFull, dist, t);
+                        if (dd < rmax) {
+                            const int id = sids[b0 + t];
+                            rl_insert<EPL>(rd, ri, lane, dd, id);
+                            rmax = rl_get<EPL>(rd, P.ef - 1);
+                            if (dd < cmax) {   // forwarded to the candidate queue (scheduler.hpp:102-110)
+                                cl_insert(cd, ci, lane, P.cq, dd, id);
+                                cmax = __shfl_sync(kFull, cd, P.cq - 1);
                             }
                         }
                     }
@@ -410,35 +427,19 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
                 __syncwarp();
             }
         }
-        // the oldest group is retired: sort both queues, read the threshold
-        while (!r_sorted) {
-            const bool sw = rq_step<EPL>(rd, ri, lane, false, 0.0f, 0);
-            r_sorted = !__any_sync(kFull, sw);
-        }
-        rq0 = __shfl_sync(kFull, rd[0], 0);
-        const float thr = rq0;
+        // the oldest group is retired (scheduler.hpp:112-155): threshold = worst result
+        const float thr = rmax;
         head = (head + 1 == mg) ? 0 : head + 1;
         inflight--;
-        while (!c_sorted) {
-            const bool sw = cq_step(cd, ci, lane, false, 0.0f, 0);
-            c_sorted = !__any_sync(kFull, sw);
-        }
-        // refill the pipeline with groups of up to mc candidates
         for (int oid = inflight; oid < mg && !truncated; oid++) {
             int slot = head + inflight;
             if (slot >= mg) slot -= mg;
             int n = 0;
             for (int bb = 0; bb < mc; bb++) {
-                const float best = __shfl_sync(kFull, cd, P.cq - 1);
+                const float best = __shfl_sync(kFull, cd, 0);
                 if (!(best <= thr && best < kLarge)) break;
                 if (P.max_hops > 0 && hops >= P.max_hops) { truncated = true; break; }
-                const int pid = __shfl_sync(kFull, ci, P.cq - 1);
-                const float ud = __shfl_up_sync(kFull, cd, 1);
-                const int ui = __shfl_up_sync(kFull, ci, 1);
-                if (lane < P.cq) {
-                    cd = (lane == 0) ? kLarge : ud;
-                    ci = (lane == 0) ? -1 : ui;
-                }
+                const int pid = cl_pop(cd, ci, lane, P.cq);
                 if (lane == 0) fifo[slot * mc + n] = pid;
                 n++;
                 hops++;
@@ -447,25 +448,22 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
             if (lane == 0) fifo_len[slot] = n;
             inflight++;
         }
-        cq0 = __shfl_sync(kFull, cd, 0);
+        cmax = __shfl_sync(kFull, cd, P.cq - 1);
         __syncwarp();
     }
 
-    // results best-first: result i is position ef-1-i (DRAM_utils.hpp:460-464)
+    // results best-first (DRAM_utils.hpp:460-464): list position i is result i
     const int nwrite = A.write_all_ef ? P.ef : P.k;
     int32_t *oid_row = A.out_ids + qi * A.out_stride;
     float *od_row = A.out_d + qi * A.out_stride;
 #pragma unroll
     for (int e = 0; e < EPL; e++) {
-        const int pos = lane * EPL + e;
-        if (pos < P.ef) {
-            const int i = P.ef - 1 - pos;
-            if (i < nwrite) {
-                int id = ri[e];
-                if (!A.write_all_ef && g.labels && id >= 0) id = g.labels[id];
-                oid_row[i] = id;
-                od_row[i] = rd[e];
-            }
+        const int i = lane * EPL + e;
+        if (i < nwrite) {
+            int id = ri[e];
+            if (!A.write_all_ef && g.labels && id >= 0) id = g.labels[id];
+            oid_row[i] = id;
+            od_row[i] = rd[e];
         }
     }
     for (int i = nwrite + lane; i < A.out_stride; i += 32) { oid_row[i] = -1; od_row[i] = kLarge; }
@@ -503,6 +501,275 @@ __global__ void __launch_bounds__(128) inter_kernel(const SearchLaunch A)
         search_one_inter<ELEM, EPL, VROWS>(A, P, (int64_t)qi, bloom, fifo, fifo_len, sids, lane);
         __syncwarp();
     }
+}
+
+// ---------------------------------------------------------------------------
+// Intra-query mode (reference intra-query v1.5): one thread block per query,
+// `channels` warps.  Per retired group the block
+//   1. routes the group's neighbour ids to channel id & (channels-1) keeping
+//      stream order (utils.hpp:396-495, split_tasks_to_channels),
+//   2. lets warp c run its own Bloom filter, gather and L2 over channel c
+//      (the reference's per-channel bloom/fetch/compute PEs),
+//   3. merges the channels in channel order into the queues in warp 0
+//      (gather_distances_from_channels, utils.hpp:497-569, merges in
+//      readiness order; channel order is one of its schedules), then the
+//      scheduler refills the group FIFO (v1.5 scheduler.hpp:94-146).
+// The stale-threshold prefilter of v1.5 (utils.hpp:277-347) is omitted: it
+// only drops distances that the result queue would reject anyway.
+// ---------------------------------------------------------------------------
+struct IntraSmem {
+    unsigned long long qi;
+    int inflight, head, hops, truncated, done;
+    int chan_cnt[kMaxChannels];
+    int chan_off[kMaxChannels + 1];
+    int chan_valid[kMaxChannels];
+    int chan_visited[kMaxChannels];
+};
+
+template <int ELEM, int EPL, int VROWS>
+__global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
+{
+    extern __shared__ uint4 smem_u4[];
+    constexpr int EPS = ET<ELEM>::EPS;
+    constexpr int NB = (VROWS == 1) ? 8 : 4;
+    const int C = blockDim.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const GraphView &g = A.g;
+    const int nseg = g.dpad * ET<ELEM>::BYTES / 16;
+    unsigned char *base_ptr = reinterpret_cast<unsigned char *>(smem_u4);
+    IntraSmem *S = reinterpret_cast<IntraSmem *>(base_ptr);
+    size_t off = (sizeof(IntraSmem) + 15) & ~(size_t)15;
+    const size_t bloom_bytes = (size_t)1 << (A.bloom_bits_max - 3);
+    uint32_t *bloom = reinterpret_cast<uint32_t *>(base_ptr + off + bloom_bytes * warp);
+    off += bloom_bytes * C;
+    const int lcap = A.mc_max * g.max_degree;
+    int *list_id = reinterpret_cast<int *>(base_ptr + off);
+    off += sizeof(int) * (size_t)lcap;
+    float *list_d = reinterpret_cast<float *>(base_ptr + off);
+    off += sizeof(float) * (size_t)lcap;
+    int *fifo = reinterpret_cast<int *>(base_ptr + off);
+    off += sizeof(int) * (size_t)(A.mc_max * A.mg_max);
+    int *fifo_len = reinterpret_cast<int *>(base_ptr + off);
+    off += sizeof(int) * (size_t)A.mg_max;
+    int *sids = reinterpret_cast<int *>(base_ptr + off) + 32 * warp;
+
+    for (;;) {
+        if (threadIdx.x == 0) S->qi = atomicAdd(reinterpret_cast<unsigned long long *>(A.work_counter), 1ull);
+        __syncthreads();
+        const unsigned long long qi = S->qi;
+        if (qi >= (unsigned long long)A.nq) break;
+        const QParams P = A.params[A.per_query ? qi : 0];
+        const int mc = P.mc, mg = P.mg;
+        float q[VROWS][EPS];
+        {
+            const float *Q = A.queries + qi * A.qstride;
+#pragma unroll
+            for (int r = 0; r < VROWS; r++) {
+                const int seg = lane + 32 * r;
+#pragma unroll
+                for (int e = 0; e < EPS; e++) {
+                    const int j = seg * EPS + e;
+                    q[r][e] = (seg < nseg && j < g.dim) ? Q[j] : 0.0f;
+                }
+            }
+        }
+        {
+            const int nvec = 1 << (P.bloom_bits - 7);
+            uint4 *b4 = reinterpret_cast<uint4 *>(bloom);
+            for (int i = lane; i < nvec; i += 32) b4[i] = make_uint4(0, 0, 0, 0);
+        }
+        const uint32_t bmask = (1u << P.bloom_bits) - 1u;
+        int visited = 0;
+        // queues live in warp 0
+        float rd[EPL];
+        int ri[EPL];
+#pragma unroll
+        for (int e = 0; e < EPL; e++) {
+            rd[e] = (lane * EPL + e < P.ef) ? kLarge : __int_as_float(0x7f800000);
+            ri[e] = -1;
+        }
+        float cd = kLarge;
+        int ci = -1;
+        float rmax = kLarge, cmax = kLarge;
+        if (threadIdx.x == 0) {
+            int entry = A.entries ? A.entries[qi] : A.default_entry;
+            S->inflight = 1;
+            S->hops = 1;
+            if (entry < 0 || (int64_t)entry >= g.n) {
+                atomicOr(A.status, 2);
+                entry = 0;
+                S->inflight = 0;
+                S->hops = 0;
+            }
+            fifo[0] = entry;
+            fifo_len[0] = 1;
+            S->head = 0;
+            S->truncated = 0;
+        }
+        __syncthreads();
+        while (S->inflight > 0) {
+            const int head = S->head;
+            const int glen = fifo_len[head];
+            // 1. route: count, then place this channel's ids in stream order
+            int count = 0;
+            for (int b = 0; b < glen; b++) {
+                const int32_t *row = g.links + (int64_t)fifo[head * mc + b] * g.lstride;
+                const int cnt = row[0];
+                for (int c0 = 0; c0 < cnt; c0 += 32) {
+                    const int nb = (c0 + lane < cnt) ? row[g.ids_off + c0 + lane] : -1;
+                    count += __popc(__ballot_sync(kFull, nb >= 0 && (nb & (C - 1)) == warp));
+                }
+            }
+            if (lane == 0) S->chan_cnt[warp] = count;
+            __syncthreads();
+            int my_off = 0;
+            for (int c = 0; c < warp; c++) my_off += S->chan_cnt[c];
+            {
+                int w = my_off;
+                for (int b = 0; b < glen; b++) {
+                    const int32_t *row = g.links + (int64_t)fifo[head * mc + b] * g.lstride;
+                    const int cnt = row[0];
+                    for (int c0 = 0; c0 < cnt; c0 += 32) {
+                        const int nb = (c0 + lane < cnt) ? row[g.ids_off + c0 + lane] : -1;
+                        const bool mine = nb >= 0 && (nb & (C - 1)) == warp;
+                        const unsigned mm = __ballot_sync(kFull, mine);
+                        if (mine) list_id[w + __popc(mm & ((1u << lane) - 1u))] = nb;
+                        w += __popc(mm);
+                    }
+                }
+            }
+            __syncwarp();
+            // 2. this channel: Bloom, gather, distances; survivors compacted in place
+            int nvalid = 0;
+            for (int c0 = 0; c0 < count; c0 += 32) {
+                const bool act = c0 + lane < count;
+                const int nb = act ? list_id[my_off + c0 + lane] : -1;
+                const bool valid = bloom_chunk(bloom, bmask, P.seed, nb, act, lane);
+                const unsigned vm = __ballot_sync(kFull, valid);
+                const int V = __popc(vm);
+                visited += V;
+                if (valid) sids[__popc(vm & ((1u << lane) - 1u))] = nb;
+                __syncwarp();
+                for (int b0 = 0; b0 < V; b0 += NB) {
+                    uint4 raw[NB][VROWS];
+                    float scale[NB];
+#pragma unroll
+                    for (int t = 0; t < NB; t++) {
+                        const bool tv = b0 + t < V;
+                        const int id = tv ? sids[b0 + t] : 0;
+                        const unsigned char *vb = g.vecs + (int64_t)id * g.vstride_bytes;
+                        scale[t] = 1.0f;
+                        if constexpr (ELEM == kFP8) scale[t] = tv ? g.scales[id] : 1.0f;
+#pragma unroll
+                        for (int r = 0; r < VROWS; r++) {
+                            const int seg = lane + 32 * r;
+                            raw[t][r] = (tv && seg < nseg) ? ld_nc_v4(vb + 16 * seg) : make_uint4(0, 0, 0, 0);
+                        }
+                    }
+                    const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane);
+                    const int nt = min(NB, V - b0);
+                    if (lane < nt) {
+                        list_id[my_off + nvalid + b0 + lane] = sids[b0 + lane];
+                        list_d[my_off + nvalid + b0 + lane] = dist;
+                    }
+                }
+                nvalid += V;
+                __syncwarp();
+            }
+            if (lane == 0) S->chan_valid[warp] = nvalid;
+            __syncthreads();
+            // 3. warp 0 merges channels in order and runs the scheduler
+            if (warp == 0) {
+                for (int c = 0, o = 0; c < C; o += S->chan_cnt[c], c++) {
+                    const int nv = S->chan_valid[c];
+                    for (int j0 = 0; j0 < nv; j0 += 32) {
+                        const float dl = (j0 + lane < nv) ? list_d[o + j0 + lane] : kLarge;
+                        unsigned m = __ballot_sync(kFull, j0 + lane < nv && dl < rmax);
+                        while (m) {
+                            const int t = __ffs(m) - 1;
+                            m &= m - 1;
+                            const float dd = __shfl_sync(kFull, dl, t);
+                            if (dd < rmax) {
+                                const int id = list_id[o + j0 + t];
+                                rl_insert<EPL>(rd, ri, lane, dd, id);
+                                rmax = rl_get<EPL>(rd, P.ef - 1);
+                                if (dd < cmax) {
+                                    cl_insert(cd, ci, lane, P.cq, dd, id);
+                                    cmax = __shfl_sync(kFull, cd, P.cq - 1);
+                                }
+                            }
+                        }
+                    }
+                }
+                const float thr = rmax;
+                int h = (head + 1 == mg) ? 0 : head + 1;
+                int inflight = S->inflight - 1;
+                int hops = S->hops;
+                bool truncated = S->truncated != 0;
+                for (int oid = inflight; oid < mg && !truncated; oid++) {
+                    int slot = h + inflight;
+                    if (slot >= mg) slot -= mg;
+                    int n = 0;
+                    for (int bb = 0; bb < mc; bb++) {
+                        const float best = __shfl_sync(kFull, cd, 0);
+                        if (!(best <= thr && best < kLarge)) break;
+                        if (P.max_hops > 0 && hops >= P.max_hops) { truncated = true; break; }
+                        const int pid = cl_pop(cd, ci, lane, P.cq);
+                        if (lane == 0) fifo[slot * mc + n] = pid;
+                        n++;
+                        hops++;
+                    }
+                    if (n == 0) break;
+                    if (lane == 0) fifo_len[slot] = n;
+                    inflight++;
+                }
+                cmax = __shfl_sync(kFull, cd, P.cq - 1);
+                if (lane == 0) {
+                    S->head = h;
+                    S->inflight = inflight;
+                    S->hops = hops;
+                    S->truncated = truncated ? 1 : 0;
+                }
+            }
+            __syncthreads();
+        }
+        if (lane == 0) S->chan_visited[warp] = visited;
+        __syncthreads();
+        if (warp == 0) {
+            const int nwrite = A.write_all_ef ? P.ef : P.k;
+            int32_t *oid_row = A.out_ids + qi * A.out_stride;
+            float *od_row = A.out_d + qi * A.out_stride;
+#pragma unroll
+            for (int e = 0; e < EPL; e++) {
+                const int i = lane * EPL + e;
+                if (i < nwrite) {
+                    int id = ri[e];
+                    if (!A.write_all_ef && g.labels && id >= 0) id = g.labels[id];
+                    oid_row[i] = id;
+                    od_row[i] = rd[e];
+                }
+            }
+            for (int i = nwrite + lane; i < A.out_stride; i += 32) { oid_row[i] = -1; od_row[i] = kLarge; }
+            if (lane == 0) {
+                int vis = 0;
+                for (int c = 0; c < C; c++) vis += S->chan_visited[c];
+                if (A.out_hops) A.out_hops[qi] = S->hops;
+                if (A.out_visited) A.out_visited[qi] = vis;
+                if (S->truncated) atomicOr(A.status, 1);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+size_t intra_smem_bytes(const SearchLaunch &a, int channels)
+{
+    size_t b = (sizeof(IntraSmem) + 15) & ~(size_t)15;
+    b += ((size_t)1 << (a.bloom_bits_max - 3)) * channels;
+    b += 2 * sizeof(int) * (size_t)a.mc_max * a.g.max_degree;
+    b += sizeof(int) * (size_t)(a.mc_max * a.mg_max + a.mg_max);
+    b += sizeof(int) * 32 * channels;
+    return (b + 15) & ~(size_t)15;
 }
 
 // ---------------------------------------------------------------------------
@@ -633,9 +900,33 @@ cudaError_t launch_inter(const SearchLaunch &a, size_t smem_block, int num_sms, 
     return cudaGetLastError();
 }
 
+template <int ELEM, int EPL, int VROWS>
+cudaError_t launch_intra(const SearchLaunch &a, int channels, int num_sms, cudaStream_t s)
+{
+    auto kern = intra_kernel<ELEM, EPL, VROWS>;
+    const size_t smem = intra_smem_bytes(a, channels);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    const int threads = 32 * channels;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    int64_t blocks = (int64_t)per_sm * num_sms;
+    if (blocks > a.nq) blocks = a.nq;
+    if (blocks < 1) blocks = 1;
+    kern<<<(unsigned)blocks, threads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
 template <int ELEM, int VROWS>
 cudaError_t dispatch_epl(const SearchLaunch &a, size_t smem_block, int num_sms, cudaStream_t s)
 {
+    if (a.channels > 0) {
+        if (a.ef_max <= 64) return launch_intra<ELEM, 2, VROWS>(a, a.channels, num_sms, s);
+        if (a.ef_max <= 128) return launch_intra<ELEM, 4, VROWS>(a, a.channels, num_sms, s);
+        return launch_intra<ELEM, 8, VROWS>(a, a.channels, num_sms, s);
+    }
     if (a.ef_max <= 64) return launch_inter<ELEM, 2, VROWS>(a, smem_block, num_sms, s);
     if (a.ef_max <= 128) return launch_inter<ELEM, 4, VROWS>(a, smem_block, num_sms, s);
     return launch_inter<ELEM, 8, VROWS>(a, smem_block, num_sms, s);

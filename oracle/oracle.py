@@ -110,7 +110,9 @@ class OracleGraph:
 
 
 def make_params(k=10, ef=64, mc=1, mg=1, cand_queue_size=32, bloom_bits=16, hash_seed=1, mode="inter",
-                channels=4, rerank=False, max_hops=0):
+                channels=4, rerank=False, max_hops=0, precision=None):
+    """precision is accepted for symmetry with the product's parameters; the
+    traversal storage is chosen by the OracleGraph the search runs on."""
     p = FoParams()
     p.k, p.ef, p.mc, p.mg = k, ef, mc, mg
     p.cand_queue_size, p.bloom_bits, p.hash_seed = cand_queue_size, bloom_bits, hash_seed

@@ -250,3 +250,46 @@ def test_full_size_properties():
     sub = slice(0, 300)
     ids, d, hops, vis, _ = oracle.search(og, q[sub], g.entry_point, oracle.make_params(k=10, ef=64, mc=1, mg=4))
     assert _same(r.ids[sub], r.dists[sub], ids, d) and np.array_equal(r.visited[sub], vis)
+
+
+INTRA_CASES = [
+    # kind, dim, md, ef, mc, mg, channels, bits, precision
+    ("unit", 96, 64, 64, 1, 1, 4, 16, "f32"),
+    ("unit", 96, 64, 64, 2, 6, 4, 16, "f32"),
+    ("unit", 96, 64, 128, 4, 3, 8, 15, "f32"),
+    ("sift", 128, 32, 64, 2, 2, 2, 17, "f32"),
+    ("sift", 128, 32, 32, 1, 4, 1, 16, "f32"),
+    ("unit", 384, 64, 64, 2, 2, 4, 16, "bf16"),
+    ("unit", 96, 64, 256, 8, 4, 4, 16, "fp8"),
+]
+
+
+@pytest.mark.parametrize("kind,dim,md,ef,mc,mg,ch,bits,prec", INTRA_CASES)
+def test_gpu_intra_matches_oracle(oracle_mod, kind, dim, md, ef, mc, mg, ch, bits, prec):
+    g, q = small_graph(kind, 4000, dim, md, 64, seed=13)
+    ix = _index(g, storage=("f32", prec))
+    r = ix.search(q, k=10, ef=ef, mc=mc, mg=mg, mode="intra", channels=ch, bloom_bits=bits, precision=prec)
+    if prec == "f32":
+        og = oracle_graph(oracle_mod, g)
+    elif prec == "bf16":
+        og = oracle_graph(oracle_mod, g, elem=oracle_mod.BF16, stored=ix.storage("bf16"))
+    else:
+        codes, scales = ix.storage("fp8")
+        og = oracle_graph(oracle_mod, g, elem=oracle_mod.FP8, stored=codes, scales=scales)
+    ids, d, hops, vis, _ = oracle_mod.search(og, q, g.entry_point, oracle_mod.make_params(
+        k=10, ef=ef, mc=mc, mg=mg, mode="intra", channels=ch, bloom_bits=bits))
+    assert _same(r.ids, r.dists, ids, d)
+    assert np.array_equal(r.hops, hops) and np.array_equal(r.visited, vis)
+
+
+def test_gpu_intra_mixed_params_and_truncation(oracle_mod):
+    g, q = small_graph("unit", 4000, 96, 64, 64, seed=13)
+    rng = np.random.default_rng(8)
+    pq = [dict(k=int(rng.choice([1, 10, 50])), ef=int(rng.choice([32, 64, 128])), mc=int(rng.choice([1, 2, 4])),
+               mg=int(rng.integers(1, 5)), mode="intra", channels=4, max_hops=int(rng.choice([0, 0, 9])))
+          for _ in range(len(q))]
+    r = _index(g).search(q, per_query=pq)
+    ids, d, hops, vis, _ = oracle_mod.search(oracle_graph(oracle_mod, g), q, g.entry_point,
+                                             [oracle_mod.make_params(**p) for p in pq], out_stride=r.ids.shape[1])
+    assert _same(r.ids, r.dists, ids, d)
+    assert np.array_equal(r.hops, hops) and np.array_equal(r.visited, vis)

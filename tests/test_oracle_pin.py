@@ -102,3 +102,62 @@ def test_oracle_max_hops_truncates(oracle_mod):
     og = oracle_graph(oracle_mod, g)
     ids, d, hops, vis, rc = oracle_mod.search(og, q, g.entry_point, oracle_mod.make_params(max_hops=5))
     assert rc == 1 and hops.max() <= 5
+
+
+def _sorted_list_model(values, ids, n):
+    """The queue model the GPU kernels use: ascending by (distance, age);
+    insert iff d < max, evicting the newest max-valued entry."""
+    lst = [(np.float32(1e20), -1, -1)] * n          # (dist, age, id); placeholders
+    for age, (v, i) in enumerate(zip(values, ids)):
+        if v < lst[-1][0]:
+            lst.pop()                                # last = max dist, newest among ties
+            pos = sum(1 for e in lst if e[0] <= v)   # after equal distances (older)
+            lst.insert(pos, (v, age, i))
+    return np.array([e[2] for e in lst]), np.array([e[0] for e in lst], dtype=np.float32)
+
+
+@pytest.mark.parametrize("v15", [False, True])
+def test_systolic_queue_equals_sorted_list_model(oracle_mod, v15):
+    """The reference's odd-even queue and the sorted-list model agree on ids and
+    order, including heavy ties, for many random streams."""
+    rng = np.random.default_rng(123 + v15)
+    for trial in range(300):
+        n = int(rng.integers(1, 70))
+        nin = int(rng.integers(0, 200))
+        if trial % 3 == 0:
+            vals = rng.integers(0, 5, nin).astype(np.float32)        # many ties
+        elif trial % 3 == 1:
+            vals = np.sort(rng.random(nin).astype(np.float32))[::-1].copy()   # descending stream
+        else:
+            vals = rng.random(nin).astype(np.float32)
+        ids = np.arange(nin, dtype=np.int32) + 1000
+        oi, od = oracle_mod.queue_insert_sort(vals, ids, n, v15)
+        mi, md = _sorted_list_model(vals, ids, n)
+        assert np.array_equal(oi, mi), (trial, n, nin)
+        assert np.array_equal(od, md)
+
+
+def test_intra_one_channel_equals_inter(oracle_mod):
+    """With one channel the v1.5 intra-query order and queue variant give the
+    v1.3 inter-query results exactly (the phases they skip are no-ops)."""
+    g, q = small_graph("unit", 2000, 96, 64, 24, seed=4)
+    og = oracle_graph(oracle_mod, g)
+    for mc, mg in ((1, 1), (2, 3), (4, 6)):
+        a = oracle_mod.search(og, q, g.entry_point, oracle_mod.make_params(ef=64, mc=mc, mg=mg))
+        b = oracle_mod.search(og, q, g.entry_point, oracle_mod.make_params(ef=64, mc=mc, mg=mg, mode="intra",
+                                                                            channels=1))
+        for x, y in zip(a[:4], b[:4]):
+            assert np.array_equal(x, y)
+
+
+def test_intra_channels_change_visits_not_quality(oracle_mod):
+    from falcon_b200.groundtruth import brute_force_f64, recall_at_k
+    g, q = small_graph("unit", 2000, 96, 64, 24, seed=4)
+    og = oracle_graph(oracle_mod, g)
+    gt, _ = brute_force_f64(g.vectors, q, 10)
+    recs = []
+    for ch in (1, 2, 4, 8):
+        ids, d, hops, vis, _ = oracle_mod.search(og, q, g.entry_point, oracle_mod.make_params(
+            ef=64, mc=2, mg=4, mode="intra", channels=ch, bloom_bits=14))
+        recs.append(recall_at_k(ids, gt, 10))
+    assert max(recs) - min(recs) < 0.1
