@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdarg>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -562,3 +563,142 @@ int falcon_vadd(int32_t query_num, int32_t query_batch_size, int32_t ef, int32_t
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Helpers for falcon_search_noalloc (falcon_noalloc.cu): the same validation
+// and launch sequence as falcon_search, with every device buffer supplied by
+// the caller.
+// ---------------------------------------------------------------------------
+namespace falcon {
+
+int set_error_code(int code, const char *msg) { return set_error(code, "%s", msg); }
+
+int index_device(const falcon_index *ix) { return ix->device; }
+
+// Validates a no-allocation request; needs ef >= k in every struct so the
+// caller's structs can be copied to the device unchanged (the kernels'
+// QParams has the same layout, checked below).
+int prepare_search(const falcon_index *ix, int64_t nq, const falcon_search_params *params, int32_t per_query_params,
+                   int32_t out_stride, SearchPlan *plan)
+{
+    static_assert(sizeof(QParams) == sizeof(falcon_search_params), "QParams layout");
+    static_assert(offsetof(QParams, k) == offsetof(falcon_search_params, k) &&
+                      offsetof(QParams, ef) == offsetof(falcon_search_params, ef) &&
+                      offsetof(QParams, mc) == offsetof(falcon_search_params, mc) &&
+                      offsetof(QParams, mg) == offsetof(falcon_search_params, mg) &&
+                      offsetof(QParams, cq) == offsetof(falcon_search_params, cand_queue_size) &&
+                      offsetof(QParams, bloom_bits) == offsetof(falcon_search_params, bloom_bits) &&
+                      offsetof(QParams, seed) == offsetof(falcon_search_params, hash_seed) &&
+                      offsetof(QParams, mode) == offsetof(falcon_search_params, mode) &&
+                      offsetof(QParams, channels) == offsetof(falcon_search_params, channels) &&
+                      offsetof(QParams, precision) == offsetof(falcon_search_params, precision) &&
+                      offsetof(QParams, rerank) == offsetof(falcon_search_params, rerank) &&
+                      offsetof(QParams, max_hops) == offsetof(falcon_search_params, max_hops),
+                  "QParams layout");
+    plan->per_query = per_query_params != 0;
+    plan->np = plan->per_query ? nq : 1;
+    int prec = -1, mode = -1, channels = -1;
+    for (int64_t i = 0; i < plan->np; i++) {
+        const falcon_search_params &p = params[i];
+        const int rc = check_params(p, ix, i);
+        if (rc != FALCON_OK) return rc;
+        if (p.ef < p.k)
+            return set_error(FALCON_ERR_ARG, "falcon_search_noalloc: query %lld has ef %d < k %d (needs ef >= k)",
+                             (long long)i, p.ef, p.k);
+        if (prec >= 0 && prec != p.precision) return set_error(FALCON_ERR_UNSUPPORTED, "one call must use one precision");
+        if (mode >= 0 && mode != p.mode) return set_error(FALCON_ERR_UNSUPPORTED, "one call must use one mode");
+        if (p.mode == FALCON_MODE_INTRA && channels >= 0 && p.channels != channels)
+            return set_error(FALCON_ERR_UNSUPPORTED, "intra-query mode: one channel count per call");
+        prec = p.precision;
+        mode = p.mode;
+        if (p.mode == FALCON_MODE_INTRA) channels = p.channels;
+        plan->ef_max = p.ef > plan->ef_max ? p.ef : plan->ef_max;
+        plan->k_max = p.k > plan->k_max ? p.k : plan->k_max;
+        plan->mc_max = p.mc > plan->mc_max ? p.mc : plan->mc_max;
+        plan->mg_max = p.mg > plan->mg_max ? p.mg : plan->mg_max;
+        plan->bits_max = p.bloom_bits > plan->bits_max ? p.bloom_bits : plan->bits_max;
+        const bool rr = p.rerank != 0 && p.precision != FALCON_PREC_F32;
+        if (i > 0 && rr != plan->any_rerank)
+            return set_error(FALCON_ERR_UNSUPPORTED, "rerank must be set for all queries of a call or none");
+        plan->any_rerank = rr;
+    }
+    plan->prec = prec;
+    plan->mode = mode;
+    plan->channels = (mode == FALCON_MODE_INTRA) ? channels : 0;
+    if (out_stride < plan->k_max) return set_error(FALCON_ERR_ARG, "out_stride %d < k %d", out_stride, plan->k_max);
+    return FALCON_OK;
+}
+
+int run_search_plan(const falcon_index *ix, const SearchPlan &plan, int64_t nq, const float *queries,
+                    int64_t query_stride, const int32_t *entry_points, QParams *d_params, int32_t *d_scratch,
+                    int32_t *d_cand_ids, float *d_cand_d, int32_t *out_ids, float *out_dists, int32_t out_stride,
+                    int32_t *out_hops, int32_t *out_visited, cudaStream_t s)
+{
+    if (query_stride < ix->dim)
+        return set_error(FALCON_ERR_ARG, "query_stride %lld < dim %d", (long long)query_stride, ix->dim);
+    SearchLaunch a;
+    memset(&a, 0, sizeof(a));
+    a.g.vecs = reinterpret_cast<const unsigned char *>(ix->d_f32);
+    a.g.vstride_bytes = (int64_t)ix->dpad * 4;
+    if (plan.prec == FALCON_PREC_BF16) {
+        a.g.vecs = reinterpret_cast<const unsigned char *>(ix->d_bf16);
+        a.g.vstride_bytes = (int64_t)ix->dpad * 2;
+    } else if (plan.prec == FALCON_PREC_FP8) {
+        a.g.vecs = ix->d_fp8;
+        a.g.vstride_bytes = ix->dpad;
+    }
+    a.g.scales = ix->d_scales;
+    a.g.vecs32 = reinterpret_cast<const unsigned char *>(ix->d_f32);
+    a.g.vstride32_bytes = (int64_t)ix->dpad * 4;
+    a.g.links = ix->d_links;
+    a.g.lstride = ix->link_stride;
+    a.g.ids_off = ix->ids_offset;
+    a.g.max_degree = ix->max_degree;
+    a.g.dim = ix->dim;
+    a.g.dpad = ix->dpad;
+    a.g.n = ix->n;
+    a.g.labels = ix->d_labels;
+    a.queries = queries;
+    a.qstride = query_stride;
+    a.entries = entry_points;
+    a.default_entry = ix->entry;
+    a.nq = nq;
+    a.params = d_params;
+    a.per_query = plan.per_query ? 1 : 0;
+    a.out_ids = plan.any_rerank ? d_cand_ids : out_ids;
+    a.out_d = plan.any_rerank ? d_cand_d : out_dists;
+    a.out_stride = plan.any_rerank ? plan.ef_max : out_stride;
+    a.write_all_ef = plan.any_rerank ? 1 : 0;
+    a.out_hops = out_hops;
+    a.out_visited = out_visited;
+    a.work_counter = d_scratch;
+    a.status = d_scratch + 2;
+    a.bloom_bits_max = plan.bits_max;
+    a.ef_max = plan.ef_max;
+    a.mc_max = plan.mc_max;
+    a.mg_max = plan.mg_max;
+    a.channels = plan.channels;
+    const int elem = plan.prec == FALCON_PREC_BF16 ? kBF16 : (plan.prec == FALCON_PREC_FP8 ? kFP8 : kF32);
+    cudaError_t e = launch_search(a, elem, ix->num_sms, s);
+    if (e != cudaSuccess) return set_error(FALCON_ERR_CUDA, "search launch: %s", cudaGetErrorString(e));
+    if (plan.any_rerank) {
+        RerankLaunch r;
+        memset(&r, 0, sizeof(r));
+        r.g = a.g;
+        r.queries = queries;
+        r.qstride = query_stride;
+        r.nq = nq;
+        r.params = d_params;
+        r.per_query = a.per_query;
+        r.cand_ids = d_cand_ids;
+        r.cand_stride = plan.ef_max;
+        r.out_ids = out_ids;
+        r.out_d = out_dists;
+        r.out_stride = out_stride;
+        e = launch_rerank(r, plan.ef_max, ix->num_sms, s);
+        if (e != cudaSuccess) return set_error(FALCON_ERR_CUDA, "rerank launch: %s", cudaGetErrorString(e));
+    }
+    return FALCON_OK;
+}
+
+}  // namespace falcon

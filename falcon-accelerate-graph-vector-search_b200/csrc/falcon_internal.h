@@ -1,6 +1,7 @@
 // Internal structures shared by the traversal kernels and the C-ABI layer.
 #pragma once
 #include <cstdint>
+
 #include <cuda_runtime.h>
 
 namespace falcon {
@@ -80,6 +81,15 @@ struct RerankLaunch {
     int32_t *out_ids;
     float *out_d;
     int32_t out_stride;
+};
+
+// A validated search request (host side), used by falcon_search_noalloc.
+struct SearchPlan {
+    int64_t np = 0;                 // number of parameter structs (1 or nq)
+    int ef_max = 0, k_max = 0, mc_max = 1, mg_max = 1, bits_max = 10;
+    int prec = 0, mode = 0, channels = 0;
+    bool any_rerank = false;
+    bool per_query = false;
 };
 
 // Launchers (falcon_kernels.cu).  Return cudaError_t of the launch.

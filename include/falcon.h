@@ -164,6 +164,28 @@ int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t qu
                   int32_t *out_visited, int32_t memory, void *stream);
 
 /*
+ * Search without allocating: for callers that cannot allocate device memory
+ * on their query path -- serving threads with a fixed, pre-reserved
+ * device-memory budget, hosts embedding this library inside a runtime that
+ * owns every device allocation, and latency-critical loops that cannot take
+ * the implicit synchronisation of cudaMalloc/cudaFree.  It has no counterpart
+ * in the reference (whose host migrates buffers before each kernel call).
+ * Same results as falcon_search with FALCON_MEM_DEVICE; every data pointer is
+ * a device pointer on the index's device and `params` are host structs, each
+ * with ef >= k.  Scratch lives in one static 4 MiB device array per GPU (held
+ * until the process exits); a call needing more (256 B + 48 B per params
+ * struct + 8 B x nq x ef_max for a reduced-precision search with rerank) fails
+ * with FALCON_ERR_ARG.  The first call on a device looks the array up with
+ * cudaGetSymbolAddress and should come before any stream capture.  All calls
+ * share the array: calls whose kernels overlap on the GPU race and must be
+ * serialised by the caller.  Nothing is allocated by this call.
+ */
+int falcon_search_noalloc(falcon_index *ix, const float *queries, int64_t nq, int64_t query_stride,
+                          const int32_t *entry_points, const falcon_search_params *params,
+                          int32_t per_query_params, int32_t *out_ids, float *out_dists, int32_t out_stride,
+                          int32_t *out_hops, int32_t *out_visited, void *stream);
+
+/*
  * The reference kernel's own argument list (vadd.cpp:11-95, one channel),
  * on host buffers in the reference layout, for hosts that bind `vadd`
  * directly: query_vectors nq x pad16(dim) floats, db_vectors and links_base
