@@ -33,7 +33,12 @@ MAX_DEGREE = 64
 K = 10
 RECALL_TARGET = 0.95
 WORKLOAD = "deep1m_hnsw_m32: 1M x 96 unit-normal base, 10k queries, degree-64 single-layer graph, k=10"
-SWEEP = [(ef, mc, mg) for ef in (64, 128, 256) for mc in (1, 2, 4) for mg in (1, 4)]
+# (ef, mc, mg, cand_queue_size, bloom_bits): the configuration's ef values with
+# the reference's 32-entry candidate queue and 2^16-bit Bloom filter, then
+# larger ef, queues and filters (a query here visits 10^4-10^5 nodes, which
+# saturates a 2^16-bit filter)
+SWEEP = ([(ef, mc, mg, 32, 16) for ef in (64, 128, 256) for mc in (1, 2, 4) for mg in (1, 4)] +
+         [(ef, mc, 1, cq, 20) for ef in (256, 512, 1024) for cq in (64, 256) for mc in (1, 2)])
 
 
 def log(*a):
@@ -140,19 +145,20 @@ def sweep(ix, q, gt):
     import torch
     res = []
     dq = torch.from_numpy(q).cuda()
-    for ef, mc, mg in SWEEP:
-        r = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg)
+    for ef, mc, mg, cq, bits in SWEEP:
+        r = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
         torch.cuda.synchronize()
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record()
-        r = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg)
+        r = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
         t1.record()
         torch.cuda.synchronize()
         ms = t0.elapsed_time(t1)
         rec = recall_at_k(r.ids.cpu().numpy(), gt, K)
-        res.append(dict(ef=ef, mc=mc, mg=mg, recall=rec, ms=ms, qps=len(q) / ms * 1e3))
-        log("sweep ef=%d mc=%d mg=%d recall=%.4f %.2f ms %.0f QPS" % (ef, mc, mg, rec, ms, len(q) / ms * 1e3))
+        res.append(dict(ef=ef, mc=mc, mg=mg, cq=cq, bits=bits, recall=rec, ms=ms, qps=len(q) / ms * 1e3))
+        log("sweep ef=%d mc=%d mg=%d cq=%d bits=%d recall=%.4f %.2f ms %.0f QPS" % (
+            ef, mc, mg, cq, bits, rec, ms, len(q) / ms * 1e3))
     ok = [r for r in res if r["recall"] >= RECALL_TARGET]
     best = max(ok, key=lambda r: r["qps"]) if ok else max(res, key=lambda r: (r["recall"], r["qps"]))
     return best, bool(ok), res
@@ -203,7 +209,7 @@ def run_reference(args):
     # pick the smallest ef reaching the recall target on a sample
     n = 2000
     ef_sel, rec_sel = 256, 0.0
-    for ef in (64, 128, 256):
+    for ef in (64, 128, 256, 512, 1024, 2048):
         lab, _ = h.search(q[:n], K, ef, threads)
         rec = recall_at_k(lab, gt[:n], K)
         log("reference ef=%d recall=%.4f" % (ef, rec))
@@ -245,23 +251,35 @@ def run_ours(args):
     from falcon_b200.groundtruth import recall_at_k
     x, q, g, gt = make_workload(rank, dev)
     ix = FalconIndex(g, storage=("f32", "bf16"), device=local)
-    best, reached, table = sweep(ix, q, gt)
-    ef, mc, mg = best["ef"], best["mc"], best["mg"]
+    if args.fixed:
+        ef_, mc_, mg_, cq_, bits_ = [int(v) for v in args.fixed.split(",")]
+        best, reached, table = dict(ef=ef_, mc=mc_, mg=mg_, cq=cq_, bits=bits_), None, []
+    else:
+        best, reached, table = sweep(ix, q, gt)
+    ef, mc, mg, cq, bits = best["ef"], best["mc"], best["mg"], best["cq"], best["bits"]
     dq = torch.from_numpy(q).to(dev)
     for _ in range(args.warmup):
-        r = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg)
+        r = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
     torch.cuda.synchronize()
     if ws > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    if args.profile_region:
+        torch.cuda.profiler.start()
     with ClockSampler(local) as clk:
         ev0.record()
         for _ in range(args.steps):
-            r = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg)
+            r = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
         ev1.record()
         torch.cuda.synchronize()
+    if args.profile_region:
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profiled_steps": args.steps, "ef": ef, "mc": mc, "mg": mg, "cq": cq,
+                          "ms_per_step": ev0.elapsed_time(ev1) / args.steps}))
+        ix.close()
+        return 0
     ms = ev0.elapsed_time(ev1)
     if ws > 1:
         t = torch.tensor([ms], device=dev)
@@ -282,7 +300,7 @@ def run_ours(args):
     for i in range(args.warmup + args.steps):
         torch.cuda.synchronize()
         t = time.perf_counter()
-        rh = ix.search(qh_np, k=K, ef=ef, mc=mc, mg=mg)
+        rh = ix.search(qh_np, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
         if i >= args.warmup:
             e2e_times.append(time.perf_counter() - t)
     e2e_ms = sum(e2e_times) / len(e2e_times) * 1e3
@@ -298,20 +316,20 @@ def run_ours(args):
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record()
-        ix.search(dq[i:i + 1], k=K, ef=ef, mc=mc, mg=mg)
+        ix.search(dq[i:i + 1], k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
         b.record()
         b.synchronize()
         lat.append(a.elapsed_time(b))
     lat = np.array(lat[10:])
 
     # BF16 + exact FP32 rerank at the same point
-    rb = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, precision="bf16", rerank=True)
+    rb = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, precision="bf16", rerank=True)
     torch.cuda.synchronize()
     a = torch.cuda.Event(enable_timing=True)
     b = torch.cuda.Event(enable_timing=True)
     a.record()
     for _ in range(3):
-        rb = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, precision="bf16", rerank=True)
+        rb = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, precision="bf16", rerank=True)
     b.record()
     torch.cuda.synchronize()
     bf_ms = a.elapsed_time(b) / 3
@@ -322,7 +340,7 @@ def run_ours(args):
     achieved = alg / (ms_step / 1e3) / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": None, "peak_kind": peak_kind,
-            "bytes_per_query": alg / N_QUERIES, "kernel": "inter_kernel<f32,EPL=%d,VROWS=1>" % (2 if ef <= 64 else 4 if ef <= 128 else 8)}
+            "bytes_per_query": alg / N_QUERIES, "kernel": "inter_kernel<f32>"}
     tp = os.path.join(REPO, "profiles", "traffic.json")
     if os.path.exists(tp):
         tr = json.load(open(tp))
@@ -337,7 +355,7 @@ def run_ours(args):
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded unit-normal stand-in for Deep1M)",
-        "config": {"workload": WORKLOAD, "k": K, "ef": ef, "mc": mc, "mg": mg, "mode": "inter",
+        "config": {"workload": WORKLOAD, "k": K, "ef": ef, "mc": mc, "mg": mg, "cand_queue_size": cq, "bloom_bits": bits, "mode": "inter",
                    "recall@10": recall, "recall_target_reached": reached, "queries_per_step": N_QUERIES,
                    "parallelism": "replicas" if ws > 1 else "single",
                    "l2": "inputs larger than L2 (384 MB vectors + 320 MB links vs 126 MB L2)",
@@ -369,6 +387,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--n-base", type=int, default=None, help="scaled-down runs for quick checks only")
     ap.add_argument("--n-queries", type=int, default=None)
+    ap.add_argument("--fixed", default=None, help="ef,mc,mg,cq,bloom_bits: skip the sweep")
+    ap.add_argument("--profile-region", action="store_true",
+                    help="bracket only the timed steps with cudaProfilerStart/Stop and exit after them")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -361,6 +361,7 @@ int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t qu
         return set_error(FALCON_ERR_ARG, "per-query params must be host memory");
     const int64_t np = per_query_params ? nq : 1;
     int ef_max = 0, k_max = 0, mc_max = 1, mg_max = 1, bits_max = kMinBloomBits, prec = -1, mode = -1, ch_max = 1;
+    int cq_max = 1;
     bool any_rerank = false;
     std::vector<QParams> qp((size_t)np);
     for (int64_t i = 0; i < np; i++) {
@@ -377,6 +378,7 @@ int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t qu
         mc_max = qp[i].mc > mc_max ? qp[i].mc : mc_max;
         mg_max = qp[i].mg > mg_max ? qp[i].mg : mg_max;
         bits_max = qp[i].bloom_bits > bits_max ? qp[i].bloom_bits : bits_max;
+        cq_max = qp[i].cq > cq_max ? qp[i].cq : cq_max;
         if (qp[i].mode == FALCON_MODE_INTRA && qp[i].channels > ch_max) ch_max = qp[i].channels;
         any_rerank |= (qp[i].rerank != 0 && qp[i].precision != FALCON_PREC_F32);
     }
@@ -405,6 +407,7 @@ int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t qu
     float *d_d = nullptr, *d_cand_d = nullptr;
     QParams *d_params = nullptr;
     int32_t *d_scratch = nullptr;   // [0..1] work counter (u64), [2] status
+    uint32_t *d_bloom = nullptr;    // global Bloom filters when bloom_bits > kMaxSmemBloomBits
     int32_t status_h = 0;
     SearchLaunch a;
     memset(&a, 0, sizeof(a));
@@ -467,6 +470,7 @@ int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t qu
         a.mc_max = mc_max;
         a.mg_max = mg_max;
         a.channels = (mode == FALCON_MODE_INTRA) ? qp[0].channels : 0;
+        a.cq_max = cq_max;
         int32_t *final_ids = a.out_ids;
         float *final_d = a.out_d;
         if (any_rerank) {
@@ -478,6 +482,12 @@ int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t qu
             a.write_all_ef = 1;
         }
         const int elem = prec == FALCON_PREC_BF16 ? kBF16 : (prec == FALCON_PREC_FP8 ? kFP8 : kF32);
+        if (bits_max > kMaxSmemBloomBits) {
+            int64_t slots = 0;
+            FALCON_CUDA(search_bloom_slots(a, elem, ix->num_sms, &slots));
+            FALCON_CUDA(cudaMallocAsync((void **)&d_bloom, (size_t)slots << (bits_max - 3), s));
+            a.bloom_global = d_bloom;
+        }
         FALCON_CUDA(launch_search(a, elem, ix->num_sms, s));
         if (any_rerank) {
             RerankLaunch r;
@@ -505,7 +515,7 @@ int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t qu
     }
 done:
     for (void *p : {(void *)d_q, (void *)d_entries, (void *)d_ids, (void *)d_d, (void *)d_hops, (void *)d_vis,
-                    (void *)d_params, (void *)d_scratch, (void *)d_cand, (void *)d_cand_d})
+                    (void *)d_params, (void *)d_scratch, (void *)d_cand, (void *)d_cand_d, (void *)d_bloom})
         if (p) cudaFreeAsync(p, s);
     if (rc == FALCON_OK && host) {
         cudaError_t e = cudaStreamSynchronize(s);
@@ -617,6 +627,7 @@ int prepare_search(const falcon_index *ix, int64_t nq, const falcon_search_param
         plan->mc_max = p.mc > plan->mc_max ? p.mc : plan->mc_max;
         plan->mg_max = p.mg > plan->mg_max ? p.mg : plan->mg_max;
         plan->bits_max = p.bloom_bits > plan->bits_max ? p.bloom_bits : plan->bits_max;
+        plan->cq_max = p.cand_queue_size > plan->cq_max ? p.cand_queue_size : plan->cq_max;
         const bool rr = p.rerank != 0 && p.precision != FALCON_PREC_F32;
         if (i > 0 && rr != plan->any_rerank)
             return set_error(FALCON_ERR_UNSUPPORTED, "rerank must be set for all queries of a call or none");
@@ -625,6 +636,9 @@ int prepare_search(const falcon_index *ix, int64_t nq, const falcon_search_param
     plan->prec = prec;
     plan->mode = mode;
     plan->channels = (mode == FALCON_MODE_INTRA) ? channels : 0;
+    if (plan->bits_max > kMaxSmemBloomBits)
+        return set_error(FALCON_ERR_ARG, "falcon_search_noalloc: bloom_bits above %d need per-warp filters in "
+                         "global memory, which do not fit the static scratch; use falcon_search", kMaxSmemBloomBits);
     if (out_stride < plan->k_max) return set_error(FALCON_ERR_ARG, "out_stride %d < k %d", out_stride, plan->k_max);
     return FALCON_OK;
 }
@@ -678,6 +692,7 @@ int run_search_plan(const falcon_index *ix, const SearchPlan &plan, int64_t nq, 
     a.mc_max = plan.mc_max;
     a.mg_max = plan.mg_max;
     a.channels = plan.channels;
+    a.cq_max = plan.cq_max;
     const int elem = plan.prec == FALCON_PREC_BF16 ? kBF16 : (plan.prec == FALCON_PREC_FP8 ? kFP8 : kF32);
     cudaError_t e = launch_search(a, elem, ix->num_sms, s);
     if (e != cudaSuccess) return set_error(FALCON_ERR_CUDA, "search launch: %s", cudaGetErrorString(e));

@@ -11,12 +11,13 @@ constexpr float kLarge = 1e20f;   // constants.hpp:14 large_float
 enum Elem { kF32 = 0, kBF16 = 1, kFP8 = 2 };
 
 // Limits of the built kernels.
-constexpr int kMaxEf = 256;
-constexpr int kMaxCandQueue = 32;
+constexpr int kMaxEf = 1024;
+constexpr int kMaxCandQueue = 256;
 constexpr int kMaxMc = 8;
 constexpr int kMaxMg = 16;
 constexpr int kMaxDegree = 128;
-constexpr int kMaxBloomBits = 18;
+constexpr int kMaxBloomBits = 24;
+constexpr int kMaxSmemBloomBits = 18;   // larger filters live in global memory, one slot per warp/channel
 constexpr int kMinBloomBits = 10;
 constexpr int kMaxDimPadded = 512;
 constexpr int kMaxChannels = 8;
@@ -67,6 +68,8 @@ struct SearchLaunch {
     int32_t ef_max;
     int32_t mc_max, mg_max;
     int32_t channels;               // 0: inter-query (warp per query); else intra-query block of `channels` warps
+    int32_t cq_max;                 // largest candidate queue of the call
+    uint32_t *bloom_global;         // bloom_bits_max > kMaxSmemBloomBits: per-warp filters in global memory
 };
 
 struct RerankLaunch {
@@ -86,7 +89,7 @@ struct RerankLaunch {
 // A validated search request (host side), used by falcon_search_noalloc.
 struct SearchPlan {
     int64_t np = 0;                 // number of parameter structs (1 or nq)
-    int ef_max = 0, k_max = 0, mc_max = 1, mg_max = 1, bits_max = 10;
+    int ef_max = 0, k_max = 0, mc_max = 1, mg_max = 1, bits_max = 10, cq_max = 1;
     int prec = 0, mode = 0, channels = 0;
     bool any_rerank = false;
     bool per_query = false;
@@ -94,6 +97,9 @@ struct SearchPlan {
 
 // Launchers (falcon_kernels.cu).  Return cudaError_t of the launch.
 cudaError_t launch_search(const SearchLaunch &a, int elem, int num_sms, cudaStream_t s);
+// Number of Bloom-filter slots (warps or channel warps) launch_search will
+// use for this launch; the global filter buffer must hold that many filters.
+cudaError_t search_bloom_slots(const SearchLaunch &a, int elem, int num_sms, int64_t *slots);
 cudaError_t launch_rerank(const RerankLaunch &a, int ef_max, int num_sms, cudaStream_t s);
 cudaError_t launch_encode_bf16(const float *src, int64_t src_stride, int64_t n, int dim, int dpad, uint16_t *dst,
                                cudaStream_t s);

@@ -246,31 +246,52 @@ __device__ __forceinline__ float rl_get(const float (&d)[EPL], int p)
     return __shfl_sync(kFull, v, p / EPL);
 }
 
-// Candidate list: position = lane < cq, ascending; lanes >= cq are ignored.
-__device__ __forceinline__ void cl_insert(float &d, int &id, int lane, int cq, float x, int xid)
+// Candidate list: position p = lane*CPL + e < cq, ascending; positions >= cq
+// are ignored (they may hold stale entries after pops).
+template <int CPL>
+__device__ __forceinline__ void cl_insert(float (&d)[CPL], int (&id)[CPL], int lane, int cq, float x, int xid)
 {
-    const int pos = __popc(__ballot_sync(kFull, lane < cq && d <= x));
-    const float ud = __shfl_up_sync(kFull, d, 1);
-    const int ui = __shfl_up_sync(kFull, id, 1);
-    if (lane < cq) {
-        if (lane > pos) { d = ud; id = ui; }
-        else if (lane == pos) { d = x; id = xid; }
+    const bool lane_le = (lane * CPL + CPL - 1 < cq) && d[CPL - 1] <= x;
+    const int f = __popc(__ballot_sync(kFull, lane_le));
+    int c = 0;
+#pragma unroll
+    for (int e = 0; e < CPL; e++) c += (lane * CPL + e < cq && d[e] <= x) ? 1 : 0;
+    const int cf = __shfl_sync(kFull, c, f & 31);
+    const int pos = f * CPL + ((f < 32) ? cf : 0);
+    const float pd = __shfl_up_sync(kFull, d[CPL - 1], 1);
+    const int pi = __shfl_up_sync(kFull, id[CPL - 1], 1);
+#pragma unroll
+    for (int e = CPL - 1; e >= 0; e--) {
+        const int p = lane * CPL + e;
+        const float sd = (e == 0) ? pd : d[(e > 0) ? e - 1 : 0];
+        const int si = (e == 0) ? pi : id[(e > 0) ? e - 1 : 0];
+        if (p < cq) {
+            if (p > pos) { d[e] = sd; id[e] = si; }
+            else if (p == pos) { d[e] = x; id[e] = xid; }
+        }
     }
 }
 
 // pop_top (priority_queue.hpp:131-165): take the best entry, a +large
 // placeholder enters at the worst end.
-__device__ __forceinline__ int cl_pop(float &d, int &id, int lane, int cq)
+template <int CPL>
+__device__ __forceinline__ int cl_pop(float (&d)[CPL], int (&id)[CPL], int lane, int cq)
 {
-    const int pid = __shfl_sync(kFull, id, 0);
-    const float dn = __shfl_down_sync(kFull, d, 1);
-    const int in = __shfl_down_sync(kFull, id, 1);
-    if (lane < cq) {
-        d = (lane == cq - 1) ? kLarge : dn;
-        id = (lane == cq - 1) ? -1 : in;
+    const int pid = __shfl_sync(kFull, id[0], 0);
+    const float nd = __shfl_down_sync(kFull, d[0], 1);
+    const int ni = __shfl_down_sync(kFull, id[0], 1);
+#pragma unroll
+    for (int e = 0; e < CPL; e++) {
+        const int p = lane * CPL + e;
+        const float sd = (e + 1 < CPL) ? d[(e + 1 < CPL) ? e + 1 : 0] : nd;
+        const int si = (e + 1 < CPL) ? id[(e + 1 < CPL) ? e + 1 : 0] : ni;
+        if (p < cq - 1) { d[e] = sd; id[e] = si; }
+        else if (p == cq - 1) { d[e] = kLarge; id[e] = -1; }
     }
     return pid;
 }
+
+template <int EPL> struct CandPerLane { static constexpr int value = (EPL >= 8) ? EPL / 4 : 1; };
 
 // ---------------------------------------------------------------------------
 // Bloom filter check of one 32-id chunk of the neighbour stream, with the
@@ -356,8 +377,11 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
         rd[e] = (lane * EPL + e < P.ef) ? kLarge : __int_as_float(0x7f800000);   // placeholders, then +inf
         ri[e] = -1;
     }
-    float cd = kLarge;
-    int ci = -1;
+    constexpr int CPL = CandPerLane<EPL>::value;
+    float cd[CPL];
+    int ci[CPL];
+#pragma unroll
+    for (int e = 0; e < CPL; e++) { cd[e] = kLarge; ci[e] = -1; }
     float rmax = kLarge, cmax = kLarge;   // current maxima (warp-uniform)
 
     int entry = A.entries ? A.entries[qi] : A.default_entry;
@@ -418,8 +442,8 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
                             rl_insert<EPL>(rd, ri, lane, dd, id);
                             rmax = rl_get<EPL>(rd, P.ef - 1);
                             if (dd < cmax) {   // forwarded to the candidate queue (scheduler.hpp:102-110)
-                                cl_insert(cd, ci, lane, P.cq, dd, id);
-                                cmax = __shfl_sync(kFull, cd, P.cq - 1);
+                                cl_insert<CPL>(cd, ci, lane, P.cq, dd, id);
+                                cmax = rl_get<CPL>(cd, P.cq - 1);
                             }
                         }
                     }
@@ -436,10 +460,10 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
             if (slot >= mg) slot -= mg;
             int n = 0;
             for (int bb = 0; bb < mc; bb++) {
-                const float best = __shfl_sync(kFull, cd, 0);
+                const float best = __shfl_sync(kFull, cd[0], 0);
                 if (!(best <= thr && best < kLarge)) break;
                 if (P.max_hops > 0 && hops >= P.max_hops) { truncated = true; break; }
-                const int pid = cl_pop(cd, ci, lane, P.cq);
+                const int pid = cl_pop<CPL>(cd, ci, lane, P.cq);
                 if (lane == 0) fifo[slot * mc + n] = pid;
                 n++;
                 hops++;
@@ -448,7 +472,7 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
             if (lane == 0) fifo_len[slot] = n;
             inflight++;
         }
-        cmax = __shfl_sync(kFull, cd, P.cq - 1);
+        cmax = rl_get<CPL>(cd, P.cq - 1);
         __syncwarp();
     }
 
@@ -474,9 +498,9 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
     }
 }
 
-__device__ __forceinline__ size_t warp_smem_bytes(int bloom_bits_max, int mc_max, int mg_max)
+__host__ __device__ __forceinline__ size_t warp_smem_bytes(int bloom_bits_max, int mc_max, int mg_max)
 {
-    size_t b = (size_t)1 << (bloom_bits_max - 3);
+    size_t b = (bloom_bits_max <= kMaxSmemBloomBits) ? ((size_t)1 << (bloom_bits_max - 3)) : 0;
     b += sizeof(int) * (size_t)(mc_max * mg_max + mg_max + 32);
     return (b + 15) & ~(size_t)15;
 }
@@ -488,8 +512,11 @@ __global__ void __launch_bounds__(128) inter_kernel(const SearchLaunch A)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const size_t wbytes = warp_smem_bytes(A.bloom_bits_max, A.mc_max, A.mg_max);
     unsigned char *wbase = reinterpret_cast<unsigned char *>(smem_u4) + wbytes * warp;
-    uint32_t *bloom = reinterpret_cast<uint32_t *>(wbase);
-    int *fifo = reinterpret_cast<int *>(wbase + ((size_t)1 << (A.bloom_bits_max - 3)));
+    const bool smem_bloom = A.bloom_bits_max <= kMaxSmemBloomBits;
+    const size_t bloom_bytes = (size_t)1 << (A.bloom_bits_max - 3);
+    uint32_t *bloom = smem_bloom ? reinterpret_cast<uint32_t *>(wbase)
+                                 : A.bloom_global + ((size_t)blockIdx.x * 4 + warp) * (bloom_bytes / 4);
+    int *fifo = reinterpret_cast<int *>(wbase + (smem_bloom ? bloom_bytes : 0));
     int *fifo_len = fifo + A.mc_max * A.mg_max;
     int *sids = fifo_len + A.mg_max;
     for (;;) {
@@ -540,8 +567,10 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
     IntraSmem *S = reinterpret_cast<IntraSmem *>(base_ptr);
     size_t off = (sizeof(IntraSmem) + 15) & ~(size_t)15;
     const size_t bloom_bytes = (size_t)1 << (A.bloom_bits_max - 3);
-    uint32_t *bloom = reinterpret_cast<uint32_t *>(base_ptr + off + bloom_bytes * warp);
-    off += bloom_bytes * C;
+    const bool smem_bloom = A.bloom_bits_max <= kMaxSmemBloomBits;
+    uint32_t *bloom = smem_bloom ? reinterpret_cast<uint32_t *>(base_ptr + off + bloom_bytes * warp)
+                                 : A.bloom_global + ((size_t)blockIdx.x * C + warp) * (bloom_bytes / 4);
+    if (smem_bloom) off += bloom_bytes * C;
     const int lcap = A.mc_max * g.max_degree;
     int *list_id = reinterpret_cast<int *>(base_ptr + off);
     off += sizeof(int) * (size_t)lcap;
@@ -588,8 +617,11 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
             rd[e] = (lane * EPL + e < P.ef) ? kLarge : __int_as_float(0x7f800000);
             ri[e] = -1;
         }
-        float cd = kLarge;
-        int ci = -1;
+        constexpr int CPL = CandPerLane<EPL>::value;
+        float cd[CPL];
+        int ci[CPL];
+#pragma unroll
+        for (int e = 0; e < CPL; e++) { cd[e] = kLarge; ci[e] = -1; }
         float rmax = kLarge, cmax = kLarge;
         if (threadIdx.x == 0) {
             int entry = A.entries ? A.entries[qi] : A.default_entry;
@@ -694,8 +726,8 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
                                 rl_insert<EPL>(rd, ri, lane, dd, id);
                                 rmax = rl_get<EPL>(rd, P.ef - 1);
                                 if (dd < cmax) {
-                                    cl_insert(cd, ci, lane, P.cq, dd, id);
-                                    cmax = __shfl_sync(kFull, cd, P.cq - 1);
+                                    cl_insert<CPL>(cd, ci, lane, P.cq, dd, id);
+                                    cmax = rl_get<CPL>(cd, P.cq - 1);
                                 }
                             }
                         }
@@ -711,10 +743,10 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
                     if (slot >= mg) slot -= mg;
                     int n = 0;
                     for (int bb = 0; bb < mc; bb++) {
-                        const float best = __shfl_sync(kFull, cd, 0);
+                        const float best = __shfl_sync(kFull, cd[0], 0);
                         if (!(best <= thr && best < kLarge)) break;
                         if (P.max_hops > 0 && hops >= P.max_hops) { truncated = true; break; }
-                        const int pid = cl_pop(cd, ci, lane, P.cq);
+                        const int pid = cl_pop<CPL>(cd, ci, lane, P.cq);
                         if (lane == 0) fifo[slot * mc + n] = pid;
                         n++;
                         hops++;
@@ -723,7 +755,7 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
                     if (lane == 0) fifo_len[slot] = n;
                     inflight++;
                 }
-                cmax = __shfl_sync(kFull, cd, P.cq - 1);
+                cmax = rl_get<CPL>(cd, P.cq - 1);
                 if (lane == 0) {
                     S->head = h;
                     S->inflight = inflight;
@@ -765,7 +797,7 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
 size_t intra_smem_bytes(const SearchLaunch &a, int channels)
 {
     size_t b = (sizeof(IntraSmem) + 15) & ~(size_t)15;
-    b += ((size_t)1 << (a.bloom_bits_max - 3)) * channels;
+    if (a.bloom_bits_max <= kMaxSmemBloomBits) b += ((size_t)1 << (a.bloom_bits_max - 3)) * channels;
     b += 2 * sizeof(int) * (size_t)a.mc_max * a.g.max_degree;
     b += sizeof(int) * (size_t)(a.mc_max * a.mg_max + a.mg_max);
     b += sizeof(int) * 32 * channels;
@@ -883,7 +915,7 @@ __global__ void encode_fp8_kernel(const float *src, int64_t src_stride, int64_t 
 }
 
 template <int ELEM, int EPL, int VROWS>
-cudaError_t launch_inter(const SearchLaunch &a, size_t smem_block, int num_sms, cudaStream_t s)
+cudaError_t launch_inter(const SearchLaunch &a, size_t smem_block, int num_sms, cudaStream_t s, int64_t *slots)
 {
     auto kern = inter_kernel<ELEM, EPL, VROWS>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_block);
@@ -896,12 +928,16 @@ cudaError_t launch_inter(const SearchLaunch &a, size_t smem_block, int num_sms, 
     const int64_t need = (a.nq + 3) / 4;
     if (blocks > need) blocks = need;
     if (blocks < 1) blocks = 1;
+    if (slots) {
+        *slots = blocks * 4;
+        return cudaSuccess;
+    }
     kern<<<(unsigned)blocks, 128, smem_block, s>>>(a);
     return cudaGetLastError();
 }
 
 template <int ELEM, int EPL, int VROWS>
-cudaError_t launch_intra(const SearchLaunch &a, int channels, int num_sms, cudaStream_t s)
+cudaError_t launch_intra(const SearchLaunch &a, int channels, int num_sms, cudaStream_t s, int64_t *slots)
 {
     auto kern = intra_kernel<ELEM, EPL, VROWS>;
     const size_t smem = intra_smem_bytes(a, channels);
@@ -915,49 +951,86 @@ cudaError_t launch_intra(const SearchLaunch &a, int channels, int num_sms, cudaS
     int64_t blocks = (int64_t)per_sm * num_sms;
     if (blocks > a.nq) blocks = a.nq;
     if (blocks < 1) blocks = 1;
+    if (slots) {
+        *slots = blocks * channels;
+        return cudaSuccess;
+    }
     kern<<<(unsigned)blocks, threads, smem, s>>>(a);
     return cudaGetLastError();
 }
 
-template <int ELEM, int VROWS>
-cudaError_t dispatch_epl(const SearchLaunch &a, size_t smem_block, int num_sms, cudaStream_t s)
+// Entries per lane: the result list needs ef <= 32*EPL, the candidate list
+// cq <= 32*CPL with CPL = EPL/4 for EPL >= 8.
+inline int pick_epl(int ef_max, int cq_max)
 {
-    if (a.channels > 0) {
-        if (a.ef_max <= 64) return launch_intra<ELEM, 2, VROWS>(a, a.channels, num_sms, s);
-        if (a.ef_max <= 128) return launch_intra<ELEM, 4, VROWS>(a, a.channels, num_sms, s);
-        return launch_intra<ELEM, 8, VROWS>(a, a.channels, num_sms, s);
+    int epl = 2;
+    while (32 * epl < ef_max) epl *= 2;
+    if (cq_max > 32) {
+        int cpl = 2;
+        while (32 * cpl < cq_max) cpl *= 2;
+        if (4 * cpl > epl) epl = 4 * cpl;
     }
-    if (a.ef_max <= 64) return launch_inter<ELEM, 2, VROWS>(a, smem_block, num_sms, s);
-    if (a.ef_max <= 128) return launch_inter<ELEM, 4, VROWS>(a, smem_block, num_sms, s);
-    return launch_inter<ELEM, 8, VROWS>(a, smem_block, num_sms, s);
+    return epl;
+}
+
+template <int ELEM, int VROWS>
+cudaError_t dispatch_epl(const SearchLaunch &a, size_t smem_block, int num_sms, cudaStream_t s, int64_t *slots)
+{
+    const int epl = pick_epl(a.ef_max, a.cq_max);
+    if (a.channels > 0) {
+        switch (epl) {
+            case 2: return launch_intra<ELEM, 2, VROWS>(a, a.channels, num_sms, s, slots);
+            case 4: return launch_intra<ELEM, 4, VROWS>(a, a.channels, num_sms, s, slots);
+            case 8: return launch_intra<ELEM, 8, VROWS>(a, a.channels, num_sms, s, slots);
+            case 16: return launch_intra<ELEM, 16, VROWS>(a, a.channels, num_sms, s, slots);
+            case 32: return launch_intra<ELEM, 32, VROWS>(a, a.channels, num_sms, s, slots);
+        }
+        return cudaErrorInvalidValue;
+    }
+    switch (epl) {
+        case 2: return launch_inter<ELEM, 2, VROWS>(a, smem_block, num_sms, s, slots);
+        case 4: return launch_inter<ELEM, 4, VROWS>(a, smem_block, num_sms, s, slots);
+        case 8: return launch_inter<ELEM, 8, VROWS>(a, smem_block, num_sms, s, slots);
+        case 16: return launch_inter<ELEM, 16, VROWS>(a, smem_block, num_sms, s, slots);
+        case 32: return launch_inter<ELEM, 32, VROWS>(a, smem_block, num_sms, s, slots);
+    }
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace
 
-cudaError_t launch_search(const SearchLaunch &a, int elem, int num_sms, cudaStream_t s)
+static cudaError_t search_dispatch(const SearchLaunch &a, int elem, int num_sms, cudaStream_t s, int64_t *slots)
 {
-    const size_t wbytes = ((((size_t)1 << (a.bloom_bits_max - 3)) +
-                            sizeof(int) * (size_t)(a.mc_max * a.mg_max + a.mg_max + 32)) + 15) & ~(size_t)15;
-    const size_t smem_block = wbytes * 4;
+    const size_t smem_block = warp_smem_bytes(a.bloom_bits_max, a.mc_max, a.mg_max) * 4;
     const int seg_bytes = (elem == kF32) ? 4 : (elem == kBF16 ? 2 : 1);
     const int nseg = a.g.dpad * seg_bytes / 16;
     const int vrows = (nseg + 31) / 32;
     if (elem == kF32) {
         switch (vrows) {
-            case 1: return dispatch_epl<kF32, 1>(a, smem_block, num_sms, s);
-            case 2: return dispatch_epl<kF32, 2>(a, smem_block, num_sms, s);
-            case 3: return dispatch_epl<kF32, 3>(a, smem_block, num_sms, s);
-            case 4: return dispatch_epl<kF32, 4>(a, smem_block, num_sms, s);
+            case 1: return dispatch_epl<kF32, 1>(a, smem_block, num_sms, s, slots);
+            case 2: return dispatch_epl<kF32, 2>(a, smem_block, num_sms, s, slots);
+            case 3: return dispatch_epl<kF32, 3>(a, smem_block, num_sms, s, slots);
+            case 4: return dispatch_epl<kF32, 4>(a, smem_block, num_sms, s, slots);
         }
     } else if (elem == kBF16) {
         switch (vrows) {
-            case 1: return dispatch_epl<kBF16, 1>(a, smem_block, num_sms, s);
-            case 2: return dispatch_epl<kBF16, 2>(a, smem_block, num_sms, s);
+            case 1: return dispatch_epl<kBF16, 1>(a, smem_block, num_sms, s, slots);
+            case 2: return dispatch_epl<kBF16, 2>(a, smem_block, num_sms, s, slots);
         }
     } else if (elem == kFP8) {
-        if (vrows == 1) return dispatch_epl<kFP8, 1>(a, smem_block, num_sms, s);
+        if (vrows == 1) return dispatch_epl<kFP8, 1>(a, smem_block, num_sms, s, slots);
     }
     return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_search(const SearchLaunch &a, int elem, int num_sms, cudaStream_t s)
+{
+    return search_dispatch(a, elem, num_sms, s, nullptr);
+}
+
+cudaError_t search_bloom_slots(const SearchLaunch &a, int elem, int num_sms, int64_t *slots)
+{
+    return search_dispatch(a, elem, num_sms, nullptr, slots);
 }
 
 cudaError_t launch_rerank(const RerankLaunch &a, int ef_max, int num_sms, cudaStream_t s)

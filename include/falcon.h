@@ -96,11 +96,11 @@ typedef struct falcon_index_info {
  */
 typedef struct falcon_search_params {
     int32_t k;
-    int32_t ef;                     /* result queue size, 1..256 */
+    int32_t ef;                     /* result queue size, 1..1024 (the reference hardware: <= 64) */
     int32_t mc;                     /* candidates per group, 1..8 */
     int32_t mg;                     /* groups in flight, 1..16 */
-    int32_t cand_queue_size;        /* 1..32 */
-    int32_t bloom_bits;             /* 10..18 */
+    int32_t cand_queue_size;        /* 1..256 (the reference hardware: <= 32) */
+    int32_t bloom_bits;             /* 10..24; above 18 the filters live in global memory */
     uint32_t hash_seed;
     int32_t mode;                   /* FALCON_MODE_* */
     int32_t channels;               /* intra mode: 1,2,4,8 */

@@ -48,6 +48,14 @@ CASES = [
     ("unit", 4000, 384, 64, 10, 64, 2, 2, 32, 16),
     ("unit", 4000, 200, 48, 10, 96, 3, 16, 24, 14),
     ("sift", 4000, 50, 20, 5, 33, 1, 5, 31, 13),
+    # beyond the reference hardware's ef <= 64 and 32-entry candidate queue
+    ("unit", 6000, 96, 64, 10, 512, 1, 2, 64, 16),
+    ("unit", 6000, 96, 64, 10, 1024, 2, 4, 256, 17),
+    ("sift", 6000, 128, 32, 50, 300, 4, 3, 100, 16),
+    ("unit", 4000, 384, 64, 10, 700, 1, 1, 128, 16),
+    # Bloom filters above 2^18 bits live in global memory
+    ("unit", 6000, 96, 64, 10, 256, 2, 2, 64, 20),
+    ("sift", 6000, 128, 32, 10, 1024, 1, 3, 256, 22),
 ]
 
 
@@ -214,8 +222,8 @@ def test_bad_parameters_are_errors():
     from falcon_b200 import _lib
     g, q = small_graph("sift", 6000, 128, 32, 8, seed=7)
     ix = _index(g)
-    for kw in (dict(mc=0), dict(mc=9), dict(mg=17), dict(ef=257), dict(cand_queue_size=33), dict(bloom_bits=9),
-               dict(bloom_bits=19), dict(precision="bf16"), dict(k=0)):
+    for kw in (dict(mc=0), dict(mc=9), dict(mg=17), dict(ef=1025), dict(cand_queue_size=257), dict(bloom_bits=9),
+               dict(bloom_bits=25), dict(precision="bf16"), dict(k=0)):
         with pytest.raises(_lib.FalconError) as e:
             ix.search(q, **kw)
         assert e.value.code == _lib.FALCON_ERR_ARG, kw
@@ -261,6 +269,9 @@ INTRA_CASES = [
     ("sift", 128, 32, 32, 1, 4, 1, 16, "f32"),
     ("unit", 384, 64, 64, 2, 2, 4, 16, "bf16"),
     ("unit", 96, 64, 256, 8, 4, 4, 16, "fp8"),
+    ("unit", 96, 64, 1024, 2, 2, 4, 16, "f32"),
+    ("unit", 96, 64, 512, 1, 2, 4, 21, "f32"),
+    ("sift", 128, 32, 256, 2, 2, 2, 20, "bf16"),
 ]
 
 
@@ -268,7 +279,9 @@ INTRA_CASES = [
 def test_gpu_intra_matches_oracle(oracle_mod, kind, dim, md, ef, mc, mg, ch, bits, prec):
     g, q = small_graph(kind, 4000, dim, md, 64, seed=13)
     ix = _index(g, storage=("f32", prec))
-    r = ix.search(q, k=10, ef=ef, mc=mc, mg=mg, mode="intra", channels=ch, bloom_bits=bits, precision=prec)
+    cq = 256 if ef > 256 else 32
+    r = ix.search(q, k=10, ef=ef, mc=mc, mg=mg, mode="intra", channels=ch, bloom_bits=bits, precision=prec,
+                  cand_queue_size=cq)
     if prec == "f32":
         og = oracle_graph(oracle_mod, g)
     elif prec == "bf16":
@@ -277,7 +290,7 @@ def test_gpu_intra_matches_oracle(oracle_mod, kind, dim, md, ef, mc, mg, ch, bit
         codes, scales = ix.storage("fp8")
         og = oracle_graph(oracle_mod, g, elem=oracle_mod.FP8, stored=codes, scales=scales)
     ids, d, hops, vis, _ = oracle_mod.search(og, q, g.entry_point, oracle_mod.make_params(
-        k=10, ef=ef, mc=mc, mg=mg, mode="intra", channels=ch, bloom_bits=bits))
+        k=10, ef=ef, mc=mc, mg=mg, mode="intra", channels=ch, bloom_bits=bits, cand_queue_size=cq))
     assert _same(r.ids, r.dists, ids, d)
     assert np.array_equal(r.hops, hops) and np.array_equal(r.visited, vis)
 
