@@ -205,6 +205,14 @@ int falcon_index_create(const falcon_index_desc *d, falcon_index **out)
         cudaDeviceProp prop;
         FALCON_CUDA(cudaGetDeviceProperties(&prop, ix->device));
         ix->num_sms = prop.multiProcessorCount;
+        {   // keep freed per-call scratch in the device's default pool instead of
+            // returning it to the driver at every synchronisation
+            cudaMemPool_t pool;
+            if (cudaDeviceGetDefaultMemPool(&pool, ix->device) == cudaSuccess) {
+                uint64_t keep = ~0ull;
+                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            }
+        }
         FALCON_CUDA(cudaMalloc(&ix->d_f32, f32_bytes));
         FALCON_CUDA(cudaMemset(ix->d_f32, 0, f32_bytes));
         FALCON_CUDA(cudaMemcpy2D(ix->d_f32, ix->dpad * sizeof(float), d->vectors, d->vector_stride * sizeof(float),

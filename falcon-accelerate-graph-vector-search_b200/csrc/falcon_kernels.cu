@@ -293,6 +293,60 @@ __device__ __forceinline__ int cl_pop(float (&d)[CPL], int (&id)[CPL], int lane,
 
 template <int EPL> struct CandPerLane { static constexpr int value = (EPL >= 8) ? EPL / 4 : 1; };
 
+// For ef > 256 the result list is held as a 32-ary max-heap on
+// key = (distance bits, insertion age) in shared memory instead of 32 entries
+// per lane in registers.  The root is the maximum and, among equal maximal
+// distances, the newest entry -- exactly the entry the sorted-list model
+// evicts; a final sort by key gives the list order (ties oldest first).
+// Distances are >= +0, so their bit patterns order like the floats.
+__device__ __forceinline__ uint64_t heap_key(float d, uint32_t age)
+{
+    return ((uint64_t)__float_as_uint(d) << 32) | age;
+}
+
+__device__ __forceinline__ void heap_replace_root(uint64_t *key, int *id, int n, uint64_t k, int kid, int lane)
+{
+    int pos = 0;
+    for (;;) {
+        const int c0 = 32 * pos + 1;
+        if (c0 >= n) break;
+        const int c = c0 + lane;
+        const uint64_t ck = (c < n) ? key[c] : 0ull;
+        const uint32_t mhi = __reduce_max_sync(kFull, (uint32_t)(ck >> 32));
+        const uint32_t mlo = __reduce_max_sync(kFull, ((uint32_t)(ck >> 32) == mhi) ? (uint32_t)ck : 0u);
+        const uint64_t mk = ((uint64_t)mhi << 32) | mlo;
+        if (mk <= k) break;
+        const int src = __ffs(__ballot_sync(kFull, c < n && ck == mk)) - 1;
+        const int cidx = c0 + src;
+        const int cid = __shfl_sync(kFull, (c < n) ? id[c] : -1, src);
+        if (lane == 0) { key[pos] = mk; id[pos] = cid; }
+        pos = cidx;
+        __syncwarp();
+    }
+    if (lane == 0) { key[pos] = k; id[pos] = kid; }
+    __syncwarp();
+}
+
+// Ascending bitonic sort of the first n2 (a power of two) keys, ids alongside.
+__device__ __forceinline__ void warp_bitonic_sort(uint64_t *key, int *id, int n2, int lane)
+{
+    for (int size = 2; size <= n2; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = lane; t < n2 / 2; t += 32) {
+                const int lo = 2 * t - (t & (stride - 1));
+                const int hi = lo + stride;
+                const bool up = ((lo & size) == 0);
+                const uint64_t a = key[lo], b = key[hi];
+                if ((a > b) == up) {
+                    key[lo] = b; key[hi] = a;
+                    const int ia = id[lo]; id[lo] = id[hi]; id[hi] = ia;
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Bloom filter check of one 32-id chunk of the neighbour stream, with the
 // sequential semantics of check_update (bloom_filter.hpp:159-200): a key is
@@ -315,11 +369,11 @@ __device__ __forceinline__ bool bloom_chunk(uint32_t *words, uint32_t mask, uint
     }
     __syncwarp();
     bool coll = false;
-    if (active) {
+    if (active) {   // bits that were already set need no atomic (and dirty no line)
         uint32_t o;
-        o = atomicOr(&words[h0 >> 5], 1u << (h0 & 31)); coll |= ((o >> (h0 & 31)) & 1u) && !p0;
-        o = atomicOr(&words[h1 >> 5], 1u << (h1 & 31)); coll |= ((o >> (h1 & 31)) & 1u) && !p1;
-        o = atomicOr(&words[h2 >> 5], 1u << (h2 & 31)); coll |= ((o >> (h2 & 31)) & 1u) && !p2;
+        if (!p0) { o = atomicOr(&words[h0 >> 5], 1u << (h0 & 31)); coll |= (o >> (h0 & 31)) & 1u; }
+        if (!p1) { o = atomicOr(&words[h1 >> 5], 1u << (h1 & 31)); coll |= (o >> (h1 & 31)) & 1u; }
+        if (!p2) { o = atomicOr(&words[h2 >> 5], 1u << (h2 & 31)); coll |= (o >> (h2 & 31)) & 1u; }
     }
     if (__any_sync(kFull, coll)) {
         const unsigned act_mask = __ballot_sync(kFull, active);
@@ -343,8 +397,10 @@ __device__ __forceinline__ bool bloom_chunk(uint32_t *words, uint32_t mask, uint
 // ---------------------------------------------------------------------------
 template <int ELEM, int EPL, int VROWS>
 __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_t qi, uint32_t *bloom, int *fifo,
-                                 int *fifo_len, int *sids, int lane)
+                                 int *fifo_len, int *sids, uint64_t *hkey, int *hid, int lane)
 {
+    constexpr bool HEAP = EPL > 8;            // result list as a shared-memory heap
+    constexpr int REPL = HEAP ? 1 : EPL;      // register entries per lane
     constexpr int EPS = ET<ELEM>::EPS;
     constexpr int NB = (VROWS == 1) ? 8 : 4;
     const GraphView &g = A.g;
@@ -370,12 +426,16 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
     }
     const uint32_t bmask = (1u << P.bloom_bits) - 1u;
 
-    float rd[EPL];
-    int ri[EPL];
+    float rd[REPL];
+    int ri[REPL];
 #pragma unroll
-    for (int e = 0; e < EPL; e++) {
+    for (int e = 0; e < REPL; e++) {
         rd[e] = (lane * EPL + e < P.ef) ? kLarge : __int_as_float(0x7f800000);   // placeholders, then +inf
         ri[e] = -1;
+    }
+    uint32_t age = 0;
+    if constexpr (HEAP) {
+        for (int i = lane; i < P.ef; i += 32) { hkey[i] = heap_key(kLarge, 0u); hid[i] = -1; }
     }
     constexpr int CPL = CandPerLane<EPL>::value;
     float cd[CPL];
@@ -439,8 +499,13 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
                         const float dd = __shfl_sync(kFull, dist, t);
                         if (dd < rmax) {
                             const int id = sids[b0 + t];
-                            rl_insert<EPL>(rd, ri, lane, dd, id);
-                            rmax = rl_get<EPL>(rd, P.ef - 1);
+                            if constexpr (HEAP) {
+                                heap_replace_root(hkey, hid, P.ef, heap_key(dd, ++age), id, lane);
+                                rmax = __uint_as_float((uint32_t)(hkey[0] >> 32));
+                            } else {
+                                rl_insert<EPL>(rd, ri, lane, dd, id);
+                                rmax = rl_get<EPL>(rd, P.ef - 1);
+                            }
                             if (dd < cmax) {   // forwarded to the candidate queue (scheduler.hpp:102-110)
                                 cl_insert<CPL>(cd, ci, lane, P.cq, dd, id);
                                 cmax = rl_get<CPL>(cd, P.cq - 1);
@@ -480,14 +545,29 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
     const int nwrite = A.write_all_ef ? P.ef : P.k;
     int32_t *oid_row = A.out_ids + qi * A.out_stride;
     float *od_row = A.out_d + qi * A.out_stride;
-#pragma unroll
-    for (int e = 0; e < EPL; e++) {
-        const int i = lane * EPL + e;
-        if (i < nwrite) {
-            int id = ri[e];
+    if constexpr (HEAP) {
+        int n2 = 1;
+        while (n2 < P.ef) n2 <<= 1;
+        for (int i = P.ef + lane; i < n2; i += 32) { hkey[i] = ~0ull; hid[i] = -1; }
+        __syncwarp();
+        warp_bitonic_sort(hkey, hid, n2, lane);
+        for (int i = lane; i < nwrite; i += 32) {
+            int id = hid[i];
             if (!A.write_all_ef && g.labels && id >= 0) id = g.labels[id];
             oid_row[i] = id;
-            od_row[i] = rd[e];
+            od_row[i] = __uint_as_float((uint32_t)(hkey[i] >> 32));
+        }
+        __syncwarp();
+    } else {
+#pragma unroll
+        for (int e = 0; e < REPL; e++) {
+            const int i = lane * EPL + e;
+            if (i < nwrite) {
+                int id = ri[e];
+                if (!A.write_all_ef && g.labels && id >= 0) id = g.labels[id];
+                oid_row[i] = id;
+                od_row[i] = rd[e];
+            }
         }
     }
     for (int i = nwrite + lane; i < A.out_stride; i += 32) { oid_row[i] = -1; od_row[i] = kLarge; }
@@ -498,9 +578,10 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
     }
 }
 
-__host__ __device__ __forceinline__ size_t warp_smem_bytes(int bloom_bits_max, int mc_max, int mg_max)
+__host__ __device__ __forceinline__ size_t warp_smem_bytes(int bloom_bits_max, int mc_max, int mg_max, int heap_cap)
 {
     size_t b = (bloom_bits_max <= kMaxSmemBloomBits) ? ((size_t)1 << (bloom_bits_max - 3)) : 0;
+    b += (size_t)heap_cap * (sizeof(uint64_t) + sizeof(int));
     b += sizeof(int) * (size_t)(mc_max * mg_max + mg_max + 32);
     return (b + 15) & ~(size_t)15;
 }
@@ -510,13 +591,17 @@ __global__ void __launch_bounds__(128) inter_kernel(const SearchLaunch A)
 {
     extern __shared__ uint4 smem_u4[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const size_t wbytes = warp_smem_bytes(A.bloom_bits_max, A.mc_max, A.mg_max);
+    constexpr int HEAP_CAP = (EPL > 8) ? 32 * EPL : 0;
+    const size_t wbytes = warp_smem_bytes(A.bloom_bits_max, A.mc_max, A.mg_max, HEAP_CAP);
     unsigned char *wbase = reinterpret_cast<unsigned char *>(smem_u4) + wbytes * warp;
     const bool smem_bloom = A.bloom_bits_max <= kMaxSmemBloomBits;
     const size_t bloom_bytes = (size_t)1 << (A.bloom_bits_max - 3);
     uint32_t *bloom = smem_bloom ? reinterpret_cast<uint32_t *>(wbase)
                                  : A.bloom_global + ((size_t)blockIdx.x * 4 + warp) * (bloom_bytes / 4);
-    int *fifo = reinterpret_cast<int *>(wbase + (smem_bloom ? bloom_bytes : 0));
+    unsigned char *after_bloom = wbase + (smem_bloom ? bloom_bytes : 0);
+    uint64_t *hkey = reinterpret_cast<uint64_t *>(after_bloom);
+    int *hid = reinterpret_cast<int *>(after_bloom + sizeof(uint64_t) * HEAP_CAP);
+    int *fifo = reinterpret_cast<int *>(after_bloom + (sizeof(uint64_t) + sizeof(int)) * HEAP_CAP);
     int *fifo_len = fifo + A.mc_max * A.mg_max;
     int *sids = fifo_len + A.mg_max;
     for (;;) {
@@ -525,7 +610,7 @@ __global__ void __launch_bounds__(128) inter_kernel(const SearchLaunch A)
         qi = __shfl_sync(kFull, qi, 0);
         if (qi >= (unsigned long long)A.nq) break;
         const QParams P = A.params[A.per_query ? qi : 0];
-        search_one_inter<ELEM, EPL, VROWS>(A, P, (int64_t)qi, bloom, fifo, fifo_len, sids, lane);
+        search_one_inter<ELEM, EPL, VROWS>(A, P, (int64_t)qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
         __syncwarp();
     }
 }
@@ -559,6 +644,9 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
     extern __shared__ uint4 smem_u4[];
     constexpr int EPS = ET<ELEM>::EPS;
     constexpr int NB = (VROWS == 1) ? 8 : 4;
+    constexpr bool HEAP = EPL > 8;
+    constexpr int REPL = HEAP ? 1 : EPL;
+    constexpr int HEAP_CAP = HEAP ? 32 * EPL : 0;
     const int C = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const GraphView &g = A.g;
@@ -581,6 +669,10 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
     int *fifo_len = reinterpret_cast<int *>(base_ptr + off);
     off += sizeof(int) * (size_t)A.mg_max;
     int *sids = reinterpret_cast<int *>(base_ptr + off) + 32 * warp;
+    off += sizeof(int) * 32 * C;
+    off = (off + 15) & ~(size_t)15;
+    uint64_t *hkey = reinterpret_cast<uint64_t *>(base_ptr + off);
+    int *hid = reinterpret_cast<int *>(base_ptr + off + sizeof(uint64_t) * HEAP_CAP);
 
     for (;;) {
         if (threadIdx.x == 0) S->qi = atomicAdd(reinterpret_cast<unsigned long long *>(A.work_counter), 1ull);
@@ -610,12 +702,17 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
         const uint32_t bmask = (1u << P.bloom_bits) - 1u;
         int visited = 0;
         // queues live in warp 0
-        float rd[EPL];
-        int ri[EPL];
+        float rd[REPL];
+        int ri[REPL];
 #pragma unroll
-        for (int e = 0; e < EPL; e++) {
+        for (int e = 0; e < REPL; e++) {
             rd[e] = (lane * EPL + e < P.ef) ? kLarge : __int_as_float(0x7f800000);
             ri[e] = -1;
+        }
+        uint32_t age = 0;
+        if constexpr (HEAP) {
+            if (warp == 0)
+                for (int i = lane; i < P.ef; i += 32) { hkey[i] = heap_key(kLarge, 0u); hid[i] = -1; }
         }
         constexpr int CPL = CandPerLane<EPL>::value;
         float cd[CPL];
@@ -723,8 +820,13 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
                             const float dd = __shfl_sync(kFull, dl, t);
                             if (dd < rmax) {
                                 const int id = list_id[o + j0 + t];
-                                rl_insert<EPL>(rd, ri, lane, dd, id);
-                                rmax = rl_get<EPL>(rd, P.ef - 1);
+                                if constexpr (HEAP) {
+                                    heap_replace_root(hkey, hid, P.ef, heap_key(dd, ++age), id, lane);
+                                    rmax = __uint_as_float((uint32_t)(hkey[0] >> 32));
+                                } else {
+                                    rl_insert<EPL>(rd, ri, lane, dd, id);
+                                    rmax = rl_get<EPL>(rd, P.ef - 1);
+                                }
                                 if (dd < cmax) {
                                     cl_insert<CPL>(cd, ci, lane, P.cq, dd, id);
                                     cmax = rl_get<CPL>(cd, P.cq - 1);
@@ -771,14 +873,29 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
             const int nwrite = A.write_all_ef ? P.ef : P.k;
             int32_t *oid_row = A.out_ids + qi * A.out_stride;
             float *od_row = A.out_d + qi * A.out_stride;
-#pragma unroll
-            for (int e = 0; e < EPL; e++) {
-                const int i = lane * EPL + e;
-                if (i < nwrite) {
-                    int id = ri[e];
+            if constexpr (HEAP) {
+                int n2 = 1;
+                while (n2 < P.ef) n2 <<= 1;
+                for (int i = P.ef + lane; i < n2; i += 32) { hkey[i] = ~0ull; hid[i] = -1; }
+                __syncwarp();
+                warp_bitonic_sort(hkey, hid, n2, lane);
+                for (int i = lane; i < nwrite; i += 32) {
+                    int id = hid[i];
                     if (!A.write_all_ef && g.labels && id >= 0) id = g.labels[id];
                     oid_row[i] = id;
-                    od_row[i] = rd[e];
+                    od_row[i] = __uint_as_float((uint32_t)(hkey[i] >> 32));
+                }
+                __syncwarp();
+            } else {
+#pragma unroll
+                for (int e = 0; e < REPL; e++) {
+                    const int i = lane * EPL + e;
+                    if (i < nwrite) {
+                        int id = ri[e];
+                        if (!A.write_all_ef && g.labels && id >= 0) id = g.labels[id];
+                        oid_row[i] = id;
+                        od_row[i] = rd[e];
+                    }
                 }
             }
             for (int i = nwrite + lane; i < A.out_stride; i += 32) { oid_row[i] = -1; od_row[i] = kLarge; }
@@ -794,13 +911,15 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
     }
 }
 
-size_t intra_smem_bytes(const SearchLaunch &a, int channels)
+size_t intra_smem_bytes(const SearchLaunch &a, int channels, int heap_cap)
 {
     size_t b = (sizeof(IntraSmem) + 15) & ~(size_t)15;
     if (a.bloom_bits_max <= kMaxSmemBloomBits) b += ((size_t)1 << (a.bloom_bits_max - 3)) * channels;
     b += 2 * sizeof(int) * (size_t)a.mc_max * a.g.max_degree;
     b += sizeof(int) * (size_t)(a.mc_max * a.mg_max + a.mg_max);
     b += sizeof(int) * 32 * channels;
+    b = (b + 15) & ~(size_t)15;
+    b += (size_t)heap_cap * (sizeof(uint64_t) + sizeof(int));
     return (b + 15) & ~(size_t)15;
 }
 
@@ -915,9 +1034,10 @@ __global__ void encode_fp8_kernel(const float *src, int64_t src_stride, int64_t 
 }
 
 template <int ELEM, int EPL, int VROWS>
-cudaError_t launch_inter(const SearchLaunch &a, size_t smem_block, int num_sms, cudaStream_t s, int64_t *slots)
+cudaError_t launch_inter(const SearchLaunch &a, size_t, int num_sms, cudaStream_t s, int64_t *slots)
 {
     auto kern = inter_kernel<ELEM, EPL, VROWS>;
+    const size_t smem_block = warp_smem_bytes(a.bloom_bits_max, a.mc_max, a.mg_max, (EPL > 8) ? 32 * EPL : 0) * 4;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_block);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -940,7 +1060,7 @@ template <int ELEM, int EPL, int VROWS>
 cudaError_t launch_intra(const SearchLaunch &a, int channels, int num_sms, cudaStream_t s, int64_t *slots)
 {
     auto kern = intra_kernel<ELEM, EPL, VROWS>;
-    const size_t smem = intra_smem_bytes(a, channels);
+    const size_t smem = intra_smem_bytes(a, channels, (EPL > 8) ? 32 * EPL : 0);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -1001,7 +1121,7 @@ cudaError_t dispatch_epl(const SearchLaunch &a, size_t smem_block, int num_sms, 
 
 static cudaError_t search_dispatch(const SearchLaunch &a, int elem, int num_sms, cudaStream_t s, int64_t *slots)
 {
-    const size_t smem_block = warp_smem_bytes(a.bloom_bits_max, a.mc_max, a.mg_max) * 4;
+    const size_t smem_block = 0;   // each launcher sizes its own shared memory
     const int seg_bytes = (elem == kF32) ? 4 : (elem == kBF16 ? 2 : 1);
     const int nseg = a.g.dpad * seg_bytes / 16;
     const int vrows = (nseg + 31) / 32;
