@@ -591,6 +591,44 @@ namespace falcon {
 
 int set_error_code(int code, const char *msg) { return set_error(code, "%s", msg); }
 
+int check_search_params(const falcon_search_params &p, const falcon_index *ix, int64_t qi)
+{
+    return check_params(p, ix, qi);
+}
+
+// Device view of an index for one traversal precision (the serving kernel's
+// per-request graph).  Fails if the index does not hold that storage.
+int index_graph_view(const falcon_index *ix, int precision, GraphView *v, int *dim, int *entry)
+{
+    memset(v, 0, sizeof(*v));
+    if (precision == FALCON_PREC_F32) {
+        v->vecs = reinterpret_cast<const unsigned char *>(ix->d_f32);
+        v->vstride_bytes = (int64_t)ix->dpad * 4;
+    } else if (precision == FALCON_PREC_BF16 && ix->d_bf16) {
+        v->vecs = reinterpret_cast<const unsigned char *>(ix->d_bf16);
+        v->vstride_bytes = (int64_t)ix->dpad * 2;
+    } else if (precision == FALCON_PREC_FP8 && ix->d_fp8) {
+        v->vecs = ix->d_fp8;
+        v->vstride_bytes = ix->dpad;
+    } else {
+        return set_error(FALCON_ERR_ARG, "index holds no storage for precision %d", precision);
+    }
+    v->scales = ix->d_scales;
+    v->vecs32 = reinterpret_cast<const unsigned char *>(ix->d_f32);
+    v->vstride32_bytes = (int64_t)ix->dpad * 4;
+    v->links = ix->d_links;
+    v->lstride = ix->link_stride;
+    v->ids_off = ix->ids_offset;
+    v->max_degree = ix->max_degree;
+    v->dim = ix->dim;
+    v->dpad = ix->dpad;
+    v->n = ix->n;
+    v->labels = ix->d_labels;
+    *dim = ix->dim;
+    *entry = ix->entry;
+    return FALCON_OK;
+}
+
 int index_device(const falcon_index *ix) { return ix->device; }
 
 // Validates a no-allocation request; needs ef >= k in every struct so the

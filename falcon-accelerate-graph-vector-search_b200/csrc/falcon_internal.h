@@ -86,6 +86,59 @@ struct RerankLaunch {
     int32_t out_stride;
 };
 
+// Serving: one published request (device ring entry).
+struct ServeDesc {
+    int32_t index;                  // registered index
+    int32_t precision;              // kF32 / kBF16 / kFP8
+    int32_t entry;                  // entry point
+    int32_t pad;
+    unsigned long long seq;         // request sequence number
+    QParams p;
+};
+
+struct ServeCtl {
+    unsigned long long head;        // requests claimed by warps
+    unsigned long long tail;        // requests published by the host
+    int32_t stop;                   // host: leave when idle
+    int32_t error;
+};
+
+struct ServeLaunch {
+    const GraphView *views;
+    int32_t nviews;
+    const ServeDesc *ring;
+    int32_t ring_cap;
+    const float *qpool;             // ring_cap x qstride (device)
+    int32_t qstride;
+    int32_t *out_ids;               // ring_cap x out_stride (host-mapped)
+    float *out_d;
+    int32_t out_stride;
+    int32_t *out_hops;              // ring_cap (host-mapped)
+    int32_t *out_visited;
+    unsigned long long *done;       // ring_cap (host-mapped): seq + 1 when the entry's result is complete
+    ServeCtl *ctl;
+    int32_t *status;
+    uint32_t *bloom_global;
+    int32_t bloom_bits_max, mc_max, mg_max, ef_max, cq_max;
+    int32_t *cand_ids;              // per warp ef_max (rerank candidates)
+    float *cand_d;
+    long long idle_ns;
+};
+
+__host__ __device__ inline size_t serve_warp_smem_bytes(int bloom_bits_max, int mc_max, int mg_max, int heap_cap,
+                                                        int ef_max)
+{
+    size_t b = (bloom_bits_max <= kMaxSmemBloomBits) ? ((size_t)1 << (bloom_bits_max - 3)) : 0;
+    b += (size_t)heap_cap * (sizeof(uint64_t) + sizeof(int));
+    b += (size_t)ef_max * (sizeof(float) + sizeof(int));
+    b += sizeof(int) * (size_t)(mc_max * mg_max + mg_max + 32);
+    return (b + 15) & ~(size_t)15;
+}
+
+// Serving kernel launch configuration for entries-per-lane `epl` (8 or 32).
+cudaError_t serve_config(const ServeLaunch &s, int epl, int num_sms, int *grid, size_t *smem);
+cudaError_t launch_serve(const ServeLaunch &s, int epl, int grid, size_t smem, cudaStream_t st);
+
 // A validated search request (host side), used by falcon_search_noalloc.
 struct SearchPlan {
     int64_t np = 0;                 // number of parameter structs (1 or nq)

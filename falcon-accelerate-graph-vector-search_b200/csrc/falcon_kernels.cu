@@ -415,7 +415,7 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
 #pragma unroll
             for (int e = 0; e < EPS; e++) {
                 const int j = seg * EPS + e;
-                q[r][e] = (seg < nseg && j < g.dim) ? Q[j] : 0.0f;
+                q[r][e] = (seg < nseg && j < g.dim) ? __ldcg(Q + j) : 0.0f;
             }
         }
     }
@@ -929,72 +929,237 @@ size_t intra_smem_bytes(const SearchLaunch &a, int channels, int heap_cap)
 // adder tree on the FP32 vectors, stable ascending order (ties keep the
 // traversal order), top k written with labels.
 // ---------------------------------------------------------------------------
+// One query's rerank: FP32 tree distances of its ef candidates (physical ids,
+// best-first, -1 = empty), stable ascending order, top k written with labels.
+// sd/si: ef floats/ints of per-warp scratch (shared memory).
+template <int VROWS>
+__device__ void rerank_one(const GraphView &g, const QParams &P, const float *Q, const int32_t *cand, int32_t *orow,
+                           float *drow, int out_stride, float *sd, int *si, int lane)
+{
+    constexpr int NB = (VROWS == 1) ? 8 : 4;
+    const int nseg = g.dpad * 4 / 16;
+    float q[VROWS][4];
+#pragma unroll
+    for (int r = 0; r < VROWS; r++) {
+        const int seg = lane + 32 * r;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int j = seg * 4 + e;
+            q[r][e] = (seg < nseg && j < g.dim) ? __ldcg(Q + j) : 0.0f;
+        }
+    }
+    for (int b0 = 0; b0 < P.ef; b0 += NB) {
+        uint4 raw[NB][VROWS];
+        float scale[NB];
+        int ids[NB];
+#pragma unroll
+        for (int t = 0; t < NB; t++) {
+            const bool tv = b0 + t < P.ef;
+            ids[t] = tv ? cand[b0 + t] : -1;
+            const int id = ids[t] >= 0 ? ids[t] : 0;
+            scale[t] = 1.0f;
+            const unsigned char *base = g.vecs32 + (int64_t)id * g.vstride32_bytes;
+#pragma unroll
+            for (int r = 0; r < VROWS; r++) {
+                const int seg = lane + 32 * r;
+                raw[t][r] = (ids[t] >= 0 && seg < nseg) ? ld_nc_v4(base + 16 * seg) : make_uint4(0, 0, 0, 0);
+            }
+        }
+        const float dist = batch_distances<kF32, VROWS, NB>(q, raw, scale, lane);
+        if (lane < NB && b0 + lane < P.ef) {
+            const int id = ids[lane];
+            sd[b0 + lane] = (id >= 0) ? dist : kLarge;
+            si[b0 + lane] = id;
+        }
+    }
+    __syncwarp();
+    for (int i = lane; i < P.ef; i += 32) {
+        const float di = sd[i];
+        int rank = 0;
+        for (int j = 0; j < P.ef; j++) {
+            const float dj = sd[j];
+            rank += (dj < di) || (dj == di && j < i);
+        }
+        if (rank < P.k) {
+            int id = si[i];
+            if (g.labels && id >= 0) id = g.labels[id];
+            orow[rank] = id;
+            drow[rank] = di;
+        }
+    }
+    for (int i = P.k + lane; i < out_stride; i += 32) { orow[i] = -1; drow[i] = kLarge; }
+    __syncwarp();
+}
+
 template <int VROWS>
 __global__ void __launch_bounds__(128) rerank_kernel(const RerankLaunch A)
 {
     __shared__ float sd[4][kMaxEf];
     __shared__ int si[4][kMaxEf];
-    constexpr int NB = (VROWS == 1) ? 8 : 4;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const GraphView &g = A.g;
-    const int nseg = g.dpad * 4 / 16;
     for (int64_t qi = (int64_t)blockIdx.x * 4 + warp; qi < A.nq; qi += (int64_t)gridDim.x * 4) {
         const QParams P = A.params[A.per_query ? qi : 0];
-        float q[VROWS][4];
-        const float *Q = A.queries + qi * A.qstride;
-#pragma unroll
-        for (int r = 0; r < VROWS; r++) {
-            const int seg = lane + 32 * r;
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-                const int j = seg * 4 + e;
-                q[r][e] = (seg < nseg && j < g.dim) ? Q[j] : 0.0f;
+        rerank_one<VROWS>(A.g, P, A.queries + qi * A.qstride, A.cand_ids + qi * A.cand_stride,
+                          A.out_ids + qi * A.out_stride, A.out_d + qi * A.out_stride, A.out_stride, sd[warp],
+                          si[warp], lane);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Serving kernel: a persistent grid whose warps pull requests one at a time
+// from a device ring that the host keeps appending to while the kernel runs
+// (continuous batching: a request admitted while others are in flight starts
+// as soon as a warp is free).  A request names a resident index, its
+// precision and its own k/ef/mc/mg; results, hops and visited go to
+// host-mapped memory, then a per-entry done word (seq + 1) is released to the
+// host.  Claiming uses compare-and-swap so no request is ever claimed before
+// it is published.  Every wait is bounded: a warp that finds no work sleeps
+// and leaves after `idle_ns` of idleness (or at once when `stop` is set); the
+// host relaunches the kernel when new work arrives.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long load_acquire_u64(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ long long global_ns()
+{
+    long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+template <int ELEM, int EPL, int VROWS>
+__device__ __forceinline__ void serve_search(SearchLaunch &A2, const QParams &P, int64_t qi, uint32_t *bloom,
+                                             int *fifo, int *fifo_len, int *sids, uint64_t *hkey, int *hid, int lane)
+{
+    search_one_inter<ELEM, EPL, VROWS>(A2, P, qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+}
+
+template <int EPL>
+__global__ void __launch_bounds__(128) serve_kernel(const ServeLaunch S)
+{
+    extern __shared__ uint4 smem_u4[];
+    constexpr int HEAP_CAP = (EPL > 8) ? 32 * EPL : 0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const size_t wbytes = serve_warp_smem_bytes(S.bloom_bits_max, S.mc_max, S.mg_max, HEAP_CAP, S.ef_max);
+    unsigned char *wbase = reinterpret_cast<unsigned char *>(smem_u4) + wbytes * warp;
+    const bool smem_bloom = S.bloom_bits_max <= kMaxSmemBloomBits;
+    const size_t bloom_bytes = (size_t)1 << (S.bloom_bits_max - 3);
+    uint32_t *bloom = smem_bloom ? reinterpret_cast<uint32_t *>(wbase)
+                                 : S.bloom_global + ((size_t)blockIdx.x * 4 + warp) * (bloom_bytes / 4);
+    unsigned char *p = wbase + (smem_bloom ? bloom_bytes : 0);
+    uint64_t *hkey = reinterpret_cast<uint64_t *>(p);
+    p += sizeof(uint64_t) * HEAP_CAP;
+    int *hid = reinterpret_cast<int *>(p);
+    p += sizeof(int) * HEAP_CAP;
+    float *rsd = reinterpret_cast<float *>(p);
+    p += sizeof(float) * S.ef_max;
+    int *rsi = reinterpret_cast<int *>(p);
+    p += sizeof(int) * S.ef_max;
+    int *fifo = reinterpret_cast<int *>(p);
+    int *fifo_len = fifo + S.mc_max * S.mg_max;
+    int *sids = fifo_len + S.mg_max;
+    const size_t gw = (size_t)blockIdx.x * 4 + warp;
+    int32_t *cand_ids = S.cand_ids + gw * S.ef_max;
+    float *cand_d = S.cand_d + gw * S.ef_max;
+
+    long long idle_since = global_ns();
+    for (;;) {
+        unsigned long long h = ~0ull;
+        if (lane == 0) {
+            for (int tries = 0; tries < 256; tries++) {
+                const unsigned long long hd = atomicAdd(&S.ctl->head, 0ull);
+                const unsigned long long tl = load_acquire_u64(&S.ctl->tail);
+                if (hd >= tl) break;
+                if (atomicCAS(&S.ctl->head, hd, hd + 1) == hd) { h = hd; break; }
             }
         }
-        const int32_t *cand = A.cand_ids + qi * A.cand_stride;
-        for (int b0 = 0; b0 < P.ef; b0 += NB) {
-            uint4 raw[NB][VROWS];
-            float scale[NB];
-            int ids[NB];
+        h = __shfl_sync(kFull, h, 0);
+        if (h == ~0ull) {
+            int stop = 0;
+            if (lane == 0) stop = *reinterpret_cast<volatile int *>(&S.ctl->stop);
+            stop = __shfl_sync(kFull, stop, 0);
+            if (stop || global_ns() - idle_since > S.idle_ns) break;
+            __nanosleep(2000);
+            continue;
+        }
+        const int e = (int)(h % (unsigned long long)S.ring_cap);
+        ServeDesc D;
+        {
+            const int *src = reinterpret_cast<const int *>(S.ring + e);
+            int *dst = reinterpret_cast<int *>(&D);
 #pragma unroll
-            for (int t = 0; t < NB; t++) {
-                const bool tv = b0 + t < P.ef;
-                ids[t] = tv ? cand[b0 + t] : -1;
-                const int id = ids[t] >= 0 ? ids[t] : 0;
-                scale[t] = 1.0f;
-                const unsigned char *base = g.vecs32 + (int64_t)id * g.vstride32_bytes;
-#pragma unroll
-                for (int r = 0; r < VROWS; r++) {
-                    const int seg = lane + 32 * r;
-                    raw[t][r] = (ids[t] >= 0 && seg < nseg) ? ld_nc_v4(base + 16 * seg) : make_uint4(0, 0, 0, 0);
-                }
-            }
-            const float dist = batch_distances<kF32, VROWS, NB>(q, raw, scale, lane);
-            if (lane < NB && b0 + lane < P.ef) {
-                const int id = ids[lane];
-                sd[warp][b0 + lane] = (id >= 0) ? dist : kLarge;
-                si[warp][b0 + lane] = id;
-            }
+            for (int w = 0; w < (int)(sizeof(ServeDesc) / sizeof(int)); w++) dst[w] = __ldcg(src + w);
+        }
+        const GraphView &v = S.views[D.index];
+        SearchLaunch A2;
+        A2.g = v;
+        A2.queries = S.qpool;
+        A2.qstride = S.qstride;
+        A2.entries = nullptr;
+        A2.default_entry = D.entry;
+        A2.nq = S.ring_cap;
+        A2.params = nullptr;
+        A2.per_query = 0;
+        const bool rerank = D.p.rerank != 0 && D.precision != kF32;
+        A2.out_ids = rerank ? cand_ids : S.out_ids;
+        A2.out_d = rerank ? cand_d : S.out_d;
+        A2.out_stride = rerank ? S.ef_max : S.out_stride;
+        A2.write_all_ef = rerank ? 1 : 0;
+        A2.out_hops = S.out_hops;
+        A2.out_visited = S.out_visited;
+        A2.work_counter = nullptr;
+        A2.status = S.status;
+        A2.bloom_bits_max = S.bloom_bits_max;
+        A2.ef_max = S.ef_max;
+        A2.mc_max = S.mc_max;
+        A2.mg_max = S.mg_max;
+        A2.channels = 0;
+        A2.cq_max = S.cq_max;
+        A2.bloom_global = S.bloom_global;
+        // per-request output row: the ring entry (rerank candidates: this warp's row 0)
+        const int64_t row = rerank ? 0 : e;
+        if (rerank) {   // hops/visited still go to the ring entry
+            A2.out_hops = S.out_hops + e;
+            A2.out_visited = S.out_visited + e;
+            A2.queries = S.qpool + (int64_t)e * S.qstride;
+        }
+        const int64_t qi = rerank ? 0 : e;
+        const int seg_bytes = (D.precision == kF32) ? 4 : (D.precision == kBF16 ? 2 : 1);
+        const int vrows = (v.dpad * seg_bytes / 16 + 31) / 32;
+        if (D.precision == kF32) {
+            if (vrows == 1) serve_search<kF32, EPL, 1>(A2, D.p, qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            else if (vrows == 2) serve_search<kF32, EPL, 2>(A2, D.p, qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            else if (vrows == 3) serve_search<kF32, EPL, 3>(A2, D.p, qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            else serve_search<kF32, EPL, 4>(A2, D.p, qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+        } else if (D.precision == kBF16) {
+            if (vrows == 1) serve_search<kBF16, EPL, 1>(A2, D.p, qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            else serve_search<kBF16, EPL, 2>(A2, D.p, qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+        } else {
+            serve_search<kFP8, EPL, 1>(A2, D.p, qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+        }
+        (void)row;
+        if (rerank) {
+            __syncwarp();
+            const int vr32 = (v.dpad * 4 / 16 + 31) / 32;
+            const float *Q = S.qpool + (int64_t)e * S.qstride;
+            int32_t *orow = S.out_ids + (int64_t)e * S.out_stride;
+            float *drow = S.out_d + (int64_t)e * S.out_stride;
+            if (vr32 == 1) rerank_one<1>(v, D.p, Q, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
+            else if (vr32 == 2) rerank_one<2>(v, D.p, Q, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
+            else if (vr32 == 3) rerank_one<3>(v, D.p, Q, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
+            else rerank_one<4>(v, D.p, Q, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
         }
         __syncwarp();
-        int32_t *orow = A.out_ids + qi * A.out_stride;
-        float *drow = A.out_d + qi * A.out_stride;
-        for (int i = lane; i < P.ef; i += 32) {
-            const float di = sd[warp][i];
-            int rank = 0;
-            for (int j = 0; j < P.ef; j++) {
-                const float dj = sd[warp][j];
-                rank += (dj < di) || (dj == di && j < i);
-            }
-            if (rank < P.k) {
-                int id = si[warp][i];
-                if (g.labels && id >= 0) id = g.labels[id];
-                orow[rank] = id;
-                drow[rank] = di;
-            }
+        if (lane == 0) {
+            __threadfence_system();
+            *reinterpret_cast<volatile unsigned long long *>(S.done + e) = D.seq + 1;
         }
-        for (int i = P.k + lane; i < A.out_stride; i += 32) { orow[i] = -1; drow[i] = kLarge; }
         __syncwarp();
+        idle_since = global_ns();
     }
 }
 
@@ -1151,6 +1316,35 @@ cudaError_t launch_search(const SearchLaunch &a, int elem, int num_sms, cudaStre
 cudaError_t search_bloom_slots(const SearchLaunch &a, int elem, int num_sms, int64_t *slots)
 {
     return search_dispatch(a, elem, num_sms, nullptr, slots);
+}
+
+cudaError_t serve_config(const ServeLaunch &sv, int epl, int num_sms, int *grid, size_t *smem)
+{
+    const int heap_cap = (epl > 8) ? 32 * epl : 0;
+    *smem = serve_warp_smem_bytes(sv.bloom_bits_max, sv.mc_max, sv.mg_max, heap_cap, sv.ef_max) * 4;
+    cudaError_t e;
+    int per_sm = 0;
+    if (epl == 8) {
+        e = cudaFuncSetAttribute(serve_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel<8>, 128, *smem);
+    } else if (epl == 32) {
+        e = cudaFuncSetAttribute(serve_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel<32>, 128, *smem);
+    } else {
+        return cudaErrorInvalidValue;
+    }
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    *grid = per_sm * num_sms;
+    return cudaSuccess;
+}
+
+cudaError_t launch_serve(const ServeLaunch &sv, int epl, int grid, size_t smem, cudaStream_t st)
+{
+    if (epl == 8) serve_kernel<8><<<grid, 128, smem, st>>>(sv);
+    else if (epl == 32) serve_kernel<32><<<grid, 128, smem, st>>>(sv);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
 }
 
 cudaError_t launch_rerank(const RerankLaunch &a, int ef_max, int num_sms, cudaStream_t s)

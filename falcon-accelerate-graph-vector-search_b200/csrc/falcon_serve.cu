@@ -1,0 +1,497 @@
+// Serving: continuous batching of single-query requests against several
+// device-resident indexes.
+//
+// The host appends requests to a device ring (descriptor + query vector,
+// copied on a copy stream, then the ring's tail counter); a persistent
+// serve_kernel (falcon_kernels.cu) whose launch is captured once in a CUDA
+// graph pulls them one at a time, so a request admitted while others are on
+// the GPU starts as soon as a warp frees up and its work overlaps theirs.
+// Each request carries its own index, precision, k, ef, mc, mg (mixed freely).
+// Results go to host-mapped memory and complete with a per-entry done word,
+// so the host collects them without any CUDA call.  The ring's size is
+// chosen from the free device memory at creation (admission by memory): a
+// request is refused (not queued) while its ring entry is still in use.
+// The kernel leaves after `idle_exit_us` without work and is relaunched by the
+// next submit or poll, so an idle server holds no SMs.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "../../include/falcon.h"
+#include "falcon_internal.h"
+
+using namespace falcon;
+
+namespace falcon {
+int set_error_code(int code, const char *msg);
+int index_device(const falcon_index *ix);
+int index_graph_view(const falcon_index *ix, int precision, GraphView *v, int *dim, int *entry);
+int check_search_params(const falcon_search_params &p, const falcon_index *ix, int64_t qi);
+}  // namespace falcon
+
+struct falcon_server {
+    falcon_server_config cfg;
+    int device = 0, num_sms = 0, epl = 8, grid = 0;
+    size_t smem = 0;
+    int cap = 0;                          // ring entries
+    int qstride = 0;                      // floats per query slot
+    std::mutex mu;
+    cudaStream_t kstream = nullptr, cstream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    cudaEvent_t kernel_done = nullptr;
+    bool launched = false;
+    int64_t launches = 0;
+    // device
+    GraphView *d_views = nullptr;
+    ServeDesc *d_ring = nullptr;
+    float *d_qpool = nullptr;
+    ServeCtl *d_ctl = nullptr;
+    int32_t *d_status = nullptr;
+    uint32_t *d_bloom = nullptr;
+    int32_t *d_cand_ids = nullptr;
+    float *d_cand_d = nullptr;
+    // host pinned (staging) and host-mapped (results)
+    ServeDesc *h_desc = nullptr;
+    float *h_qstage = nullptr;
+    unsigned long long *h_tail = nullptr;       // one pinned value per ring entry (async copy source)
+    int32_t *h_out_ids = nullptr;
+    float *h_out_d = nullptr;
+    int32_t *h_hops = nullptr, *h_vis = nullptr;
+    unsigned long long *h_done = nullptr;
+    // bookkeeping
+    std::vector<const falcon_index *> indexes;
+    std::vector<int> index_dim, index_entry;
+    std::vector<unsigned long long> entry_seq;  // seq occupying each entry, or ~0 when free
+    std::vector<int> entry_k;
+    unsigned long long next_seq = 0;
+    int64_t in_flight = 0;
+    int64_t device_bytes = 0;
+    ServeLaunch launch;
+};
+
+namespace {
+
+int cuda_fail(cudaError_t e, const char *what)
+{
+    char buf[256];
+    snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+    return set_error_code(e == cudaErrorMemoryAllocation ? FALCON_ERR_OOM : FALCON_ERR_CUDA, buf);
+}
+
+void free_server(falcon_server *sv)
+{
+    if (sv->graph) cudaGraphExecDestroy(sv->graph);
+    if (sv->kernel_done) cudaEventDestroy(sv->kernel_done);
+    if (sv->kstream) cudaStreamDestroy(sv->kstream);
+    if (sv->cstream) cudaStreamDestroy(sv->cstream);
+    cudaFree(sv->d_views);
+    cudaFree(sv->d_ring);
+    cudaFree(sv->d_qpool);
+    cudaFree(sv->d_ctl);
+    cudaFree(sv->d_status);
+    cudaFree(sv->d_bloom);
+    cudaFree(sv->d_cand_ids);
+    cudaFree(sv->d_cand_d);
+    cudaFreeHost(sv->h_desc);
+    cudaFreeHost(sv->h_qstage);
+    cudaFreeHost(sv->h_tail);
+    cudaFreeHost(sv->h_out_ids);
+    cudaFreeHost(sv->h_out_d);
+    cudaFreeHost(sv->h_hops);
+    cudaFreeHost(sv->h_vis);
+    cudaFreeHost(sv->h_done);
+    delete sv;
+}
+
+// Launch the serving kernel (graph) unless it is still running.  Caller holds mu.
+int ensure_running(falcon_server *sv)
+{
+    if (sv->launched) {
+        const cudaError_t q = cudaEventQuery(sv->kernel_done);
+        if (q == cudaErrorNotReady) return FALCON_OK;
+        if (q != cudaSuccess) return cuda_fail(q, "serve kernel");
+    }
+    cudaError_t e = cudaGraphLaunch(sv->graph, sv->kstream);
+    if (e == cudaSuccess) e = cudaEventRecord(sv->kernel_done, sv->kstream);
+    if (e != cudaSuccess) return cuda_fail(e, "serve kernel launch");
+    sv->launched = true;
+    sv->launches++;
+    return FALCON_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void falcon_server_default_config(falcon_server_config *c)
+{
+    if (!c) return;
+    memset(c, 0, sizeof(*c));
+    c->device = 0;
+    c->ring_capacity = 16384;
+    c->max_k = 100;
+    c->ef_max = 256;
+    c->cand_queue_max = 64;
+    c->bloom_bits_max = 16;
+    c->mc_max = 4;
+    c->mg_max = 8;
+    c->dim_max = 512;
+    c->idle_exit_us = 2000;
+    c->memory_fraction = 0.25;
+}
+
+int falcon_server_create(const falcon_server_config *c, falcon_server **out)
+{
+    if (!c || !out) return set_error_code(FALCON_ERR_ARG, "falcon_server_create: null argument");
+    *out = nullptr;
+    if (c->ring_capacity < 1 || c->max_k < 1 || c->ef_max < 1 || c->ef_max > kMaxEf || c->max_k > c->ef_max ||
+        c->cand_queue_max < 1 || c->cand_queue_max > kMaxCandQueue || c->bloom_bits_max < kMinBloomBits ||
+        c->bloom_bits_max > kMaxBloomBits || c->mc_max < 1 || c->mc_max > kMaxMc || c->mg_max < 1 ||
+        c->mg_max > kMaxMg || c->dim_max < 1 || c->dim_max > kMaxDimPadded || c->idle_exit_us < 1 ||
+        !(c->memory_fraction > 0.0 && c->memory_fraction <= 1.0))
+        return set_error_code(FALCON_ERR_ARG, "falcon_server_create: invalid configuration");
+    if (cudaSetDevice(c->device) != cudaSuccess)
+        return set_error_code(FALCON_ERR_CUDA, "falcon_server_create: cannot select device");
+    falcon_server *sv = new falcon_server;
+    sv->cfg = *c;
+    sv->device = c->device;
+    sv->epl = (c->ef_max <= 256 && c->cand_queue_max <= 64) ? 8 : 32;
+    sv->qstride = (c->dim_max + 15) / 16 * 16;
+    cudaError_t e;
+    cudaDeviceProp prop;
+    if ((e = cudaGetDeviceProperties(&prop, c->device)) != cudaSuccess) { free_server(sv); return cuda_fail(e, "properties"); }
+    sv->num_sms = prop.multiProcessorCount;
+    // admission by free device memory: per-entry device state is the query
+    // slot and the descriptor
+    size_t free_b = 0, total_b = 0;
+    if ((e = cudaMemGetInfo(&free_b, &total_b)) != cudaSuccess) { free_server(sv); return cuda_fail(e, "mem info"); }
+    const size_t per_entry = sizeof(float) * sv->qstride + sizeof(ServeDesc);
+    const size_t budget = (size_t)(c->memory_fraction * (double)free_b);
+    int64_t cap = c->ring_capacity;
+    if ((int64_t)(budget / per_entry) < cap) cap = (int64_t)(budget / per_entry);
+    if (cap < 1) { free_server(sv); return set_error_code(FALCON_ERR_OOM, "falcon_server_create: no device memory for requests"); }
+    sv->cap = (int)cap;
+    // kernel configuration (needs the launch struct's sizes)
+    ServeLaunch &L = sv->launch;
+    memset(&L, 0, sizeof(L));
+    L.ring_cap = sv->cap;
+    L.qstride = sv->qstride;
+    L.out_stride = c->max_k;
+    L.bloom_bits_max = c->bloom_bits_max;
+    L.mc_max = c->mc_max;
+    L.mg_max = c->mg_max;
+    L.ef_max = c->ef_max;
+    L.cq_max = c->cand_queue_max;
+    L.idle_ns = (long long)c->idle_exit_us * 1000;
+    if ((e = serve_config(L, sv->epl, sv->num_sms, &sv->grid, &sv->smem)) != cudaSuccess) {
+        free_server(sv);
+        return cuda_fail(e, "serve kernel configuration");
+    }
+    const size_t warps = (size_t)sv->grid * 4;
+#define SV_ALLOC(call, what)                      \
+    if ((e = (call)) != cudaSuccess) {            \
+        free_server(sv);                          \
+        return cuda_fail(e, what);                \
+    }
+    SV_ALLOC(cudaStreamCreateWithFlags(&sv->kstream, cudaStreamNonBlocking), "stream");
+    SV_ALLOC(cudaStreamCreateWithFlags(&sv->cstream, cudaStreamNonBlocking), "stream");
+    SV_ALLOC(cudaEventCreateWithFlags(&sv->kernel_done, cudaEventDisableTiming), "event");
+    SV_ALLOC(cudaMalloc(&sv->d_views, sizeof(GraphView) * 48), "views");
+    SV_ALLOC(cudaMalloc(&sv->d_ring, sizeof(ServeDesc) * sv->cap), "ring");
+    SV_ALLOC(cudaMalloc(&sv->d_qpool, sizeof(float) * (size_t)sv->qstride * sv->cap), "query pool");
+    SV_ALLOC(cudaMalloc(&sv->d_ctl, sizeof(ServeCtl)), "control");
+    SV_ALLOC(cudaMemset(sv->d_ctl, 0, sizeof(ServeCtl)), "control");
+    SV_ALLOC(cudaMalloc(&sv->d_status, sizeof(int32_t)), "status");
+    SV_ALLOC(cudaMemset(sv->d_status, 0, sizeof(int32_t)), "status");
+    SV_ALLOC(cudaMalloc(&sv->d_cand_ids, sizeof(int32_t) * warps * c->ef_max), "rerank scratch");
+    SV_ALLOC(cudaMalloc(&sv->d_cand_d, sizeof(float) * warps * c->ef_max), "rerank scratch");
+    if (c->bloom_bits_max > kMaxSmemBloomBits)
+        SV_ALLOC(cudaMalloc(&sv->d_bloom, warps << (c->bloom_bits_max - 3)), "Bloom filters");
+    SV_ALLOC(cudaHostAlloc(&sv->h_desc, sizeof(ServeDesc) * sv->cap, cudaHostAllocDefault), "pinned");
+    SV_ALLOC(cudaHostAlloc(&sv->h_qstage, sizeof(float) * (size_t)sv->qstride * sv->cap, cudaHostAllocDefault), "pinned");
+    SV_ALLOC(cudaHostAlloc(&sv->h_tail, sizeof(unsigned long long) * sv->cap, cudaHostAllocDefault), "pinned");
+    SV_ALLOC(cudaHostAlloc(&sv->h_out_ids, sizeof(int32_t) * (size_t)c->max_k * sv->cap, cudaHostAllocMapped), "mapped");
+    SV_ALLOC(cudaHostAlloc(&sv->h_out_d, sizeof(float) * (size_t)c->max_k * sv->cap, cudaHostAllocMapped), "mapped");
+    SV_ALLOC(cudaHostAlloc(&sv->h_hops, sizeof(int32_t) * sv->cap, cudaHostAllocMapped), "mapped");
+    SV_ALLOC(cudaHostAlloc(&sv->h_vis, sizeof(int32_t) * sv->cap, cudaHostAllocMapped), "mapped");
+    SV_ALLOC(cudaHostAlloc(&sv->h_done, sizeof(unsigned long long) * sv->cap, cudaHostAllocMapped), "mapped");
+    memset(sv->h_done, 0, sizeof(unsigned long long) * sv->cap);
+    memset(sv->h_qstage, 0, sizeof(float) * (size_t)sv->qstride * sv->cap);
+    sv->device_bytes = (int64_t)(sizeof(ServeDesc) + sizeof(float) * sv->qstride) * sv->cap +
+                       (int64_t)warps * c->ef_max * 8 +
+                       (c->bloom_bits_max > kMaxSmemBloomBits ? (int64_t)(warps << (c->bloom_bits_max - 3)) : 0);
+    void *dp;
+    L.views = sv->d_views;
+    L.ring = sv->d_ring;
+    L.qpool = sv->d_qpool;
+    SV_ALLOC(cudaHostGetDevicePointer(&dp, sv->h_out_ids, 0), "mapped pointer");
+    L.out_ids = (int32_t *)dp;
+    SV_ALLOC(cudaHostGetDevicePointer(&dp, sv->h_out_d, 0), "mapped pointer");
+    L.out_d = (float *)dp;
+    SV_ALLOC(cudaHostGetDevicePointer(&dp, sv->h_hops, 0), "mapped pointer");
+    L.out_hops = (int32_t *)dp;
+    SV_ALLOC(cudaHostGetDevicePointer(&dp, sv->h_vis, 0), "mapped pointer");
+    L.out_visited = (int32_t *)dp;
+    SV_ALLOC(cudaHostGetDevicePointer(&dp, sv->h_done, 0), "mapped pointer");
+    L.done = (unsigned long long *)dp;
+    L.ctl = sv->d_ctl;
+    L.status = sv->d_status;
+    L.bloom_global = sv->d_bloom;
+    L.cand_ids = sv->d_cand_ids;
+    L.cand_d = sv->d_cand_d;
+    // capture the persistent launch once; every (re)start replays the graph
+    {
+        cudaGraph_t g = nullptr;
+        SV_ALLOC(cudaStreamBeginCapture(sv->kstream, cudaStreamCaptureModeThreadLocal), "capture");
+        e = launch_serve(L, sv->epl, sv->grid, sv->smem, sv->kstream);
+        cudaError_t e2 = cudaStreamEndCapture(sv->kstream, &g);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&sv->graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) { free_server(sv); return cuda_fail(e, "serve graph"); }
+    }
+#undef SV_ALLOC
+    sv->entry_seq.assign(sv->cap, ~0ull);
+    sv->entry_k.assign(sv->cap, 0);
+    *out = sv;
+    return FALCON_OK;
+}
+
+int falcon_server_add_index(falcon_server *sv, falcon_index *ix, int32_t *index_id)
+{
+    if (!sv || !ix || !index_id) return set_error_code(FALCON_ERR_ARG, "falcon_server_add_index: null argument");
+    std::lock_guard<std::mutex> lock(sv->mu);
+    if (index_device(ix) != sv->device) return set_error_code(FALCON_ERR_ARG, "index lives on another device");
+    if (sv->indexes.size() >= 16) return set_error_code(FALCON_ERR_ARG, "at most 16 indexes per server");
+    GraphView v;
+    int dim = 0, entry = 0;
+    int rc = index_graph_view(ix, FALCON_PREC_F32, &v, &dim, &entry);
+    if (rc != FALCON_OK) return rc;
+    if (dim > sv->cfg.dim_max) return set_error_code(FALCON_ERR_ARG, "index dimension above the server's dim_max");
+    const int id = (int)sv->indexes.size();
+    // one device view per precision the index holds: slot id*3 + precision
+    GraphView views[3];
+    for (int pr = 0; pr < 3; pr++) {
+        int d2 = 0, e2 = 0;
+        if (index_graph_view(ix, pr, &views[pr], &d2, &e2) != FALCON_OK) views[pr] = v;
+    }
+    cudaError_t e = cudaMemcpy(sv->d_views + 3 * id, views, sizeof(views), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "register index");
+    sv->indexes.push_back(ix);
+    sv->index_dim.push_back(dim);
+    sv->index_entry.push_back(entry);
+    *index_id = id;
+    return FALCON_OK;
+}
+
+int falcon_server_submit(falcon_server *sv, int32_t n, const int32_t *index_ids, const float *queries,
+                         int64_t query_stride, const falcon_search_params *params, int32_t per_request_params,
+                         int64_t *request_ids)
+{
+    if (!sv || n < 0 || (n > 0 && (!index_ids || !queries || !params || !request_ids)))
+        return set_error_code(FALCON_ERR_ARG, "falcon_server_submit: null argument");
+    std::lock_guard<std::mutex> lock(sv->mu);
+    if (cudaSetDevice(sv->device) != cudaSuccess) return set_error_code(FALCON_ERR_CUDA, "select device");
+    // validate, then admit while ring entries are free
+    int admitted = 0;
+    const unsigned long long first = sv->next_seq;
+    for (int i = 0; i < n; i++) {
+        const int idx = index_ids[i];
+        if (idx < 0 || idx >= (int)sv->indexes.size()) return set_error_code(FALCON_ERR_ARG, "unknown index id");
+        const falcon_search_params &p = params[per_request_params ? i : 0];
+        int rc = check_search_params(p, sv->indexes[idx], i);
+        if (rc != FALCON_OK) return rc;
+        const int ef = p.ef < p.k ? p.k : p.ef;
+        if (p.k > sv->cfg.max_k || ef > sv->cfg.ef_max || p.cand_queue_size > sv->cfg.cand_queue_max ||
+            p.bloom_bits > sv->cfg.bloom_bits_max || p.mc > sv->cfg.mc_max || p.mg > sv->cfg.mg_max ||
+            p.mode != FALCON_MODE_INTER)
+            return set_error_code(FALCON_ERR_ARG, "request parameters exceed the server's configuration");
+        if (query_stride < sv->index_dim[idx]) return set_error_code(FALCON_ERR_ARG, "query_stride < dim");
+        const unsigned long long seq = first + (unsigned long long)i;
+        const int e = (int)(seq % (unsigned long long)sv->cap);
+        if (sv->entry_seq[e] != ~0ull) break;   // entry still in use: stop admitting
+        ServeDesc &d = sv->h_desc[e];
+        d.index = 3 * idx + p.precision;
+        d.precision = p.precision;
+        d.entry = sv->index_entry[idx];
+        d.pad = 0;
+        d.seq = seq;
+        d.p.k = p.k;
+        d.p.ef = ef;
+        d.p.mc = p.mc;
+        d.p.mg = p.mg;
+        d.p.cq = p.cand_queue_size;
+        d.p.bloom_bits = p.bloom_bits;
+        d.p.seed = p.hash_seed;
+        d.p.mode = 0;
+        d.p.channels = 0;
+        d.p.precision = p.precision;
+        d.p.rerank = p.rerank;
+        d.p.max_hops = p.max_hops;
+        float *qs = sv->h_qstage + (size_t)e * sv->qstride;
+        memcpy(qs, queries + (size_t)i * query_stride, sizeof(float) * sv->index_dim[idx]);
+        for (int j = sv->index_dim[idx]; j < sv->qstride; j++) qs[j] = 0.0f;
+        sv->entry_seq[e] = seq;
+        sv->entry_k[e] = p.k;
+        request_ids[i] = (int64_t)seq;
+        admitted++;
+    }
+    if (admitted == 0) return 0;
+    // copy descriptors and queries (at most two contiguous ranges), then publish the tail
+    const int e0 = (int)(first % (unsigned long long)sv->cap);
+    const int run1 = admitted < sv->cap - e0 ? admitted : sv->cap - e0;
+    cudaError_t err = cudaSuccess;
+    for (int part = 0; part < 2 && err == cudaSuccess; part++) {
+        const int s0 = part == 0 ? e0 : 0;
+        const int cnt = part == 0 ? run1 : admitted - run1;
+        if (cnt <= 0) continue;
+        err = cudaMemcpyAsync(sv->d_qpool + (size_t)s0 * sv->qstride, sv->h_qstage + (size_t)s0 * sv->qstride,
+                              sizeof(float) * (size_t)sv->qstride * cnt, cudaMemcpyHostToDevice, sv->cstream);
+        if (err == cudaSuccess)
+            err = cudaMemcpyAsync(sv->d_ring + s0, sv->h_desc + s0, sizeof(ServeDesc) * cnt, cudaMemcpyHostToDevice,
+                                  sv->cstream);
+    }
+    const unsigned long long tail = first + admitted;
+    const int te = (int)((tail - 1) % (unsigned long long)sv->cap);
+    sv->h_tail[te] = tail;
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(&sv->d_ctl->tail, &sv->h_tail[te], sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                              sv->cstream);
+    if (err != cudaSuccess) return cuda_fail(err, "publish requests");
+    sv->next_seq = tail;
+    sv->in_flight += admitted;
+    const int rc = ensure_running(sv);
+    return rc != FALCON_OK ? rc : admitted;
+}
+
+int falcon_server_poll(falcon_server *sv, int64_t request_id, int32_t *out_ids, float *out_dists, int32_t *hops,
+                       int32_t *visited)
+{
+    if (!sv || request_id < 0) return set_error_code(FALCON_ERR_ARG, "falcon_server_poll: bad argument");
+    const unsigned long long seq = (unsigned long long)request_id;
+    const int e = (int)(seq % (unsigned long long)sv->cap);
+    std::lock_guard<std::mutex> lock(sv->mu);
+    if (sv->entry_seq[e] != seq) return set_error_code(FALCON_ERR_ARG, "unknown or already collected request");
+    const unsigned long long d = *reinterpret_cast<volatile unsigned long long *>(sv->h_done + e);
+    if (d != seq + 1) {
+        // the kernel may have left on idleness just before this request was published
+        cudaSetDevice(sv->device);
+        const int rc = ensure_running(sv);
+        return rc != FALCON_OK ? rc : 0;
+    }
+    std::atomic_thread_fence(std::memory_order_acquire);
+    const int k = sv->entry_k[e];
+    if (out_ids) memcpy(out_ids, sv->h_out_ids + (size_t)e * sv->cfg.max_k, sizeof(int32_t) * k);
+    if (out_dists) memcpy(out_dists, sv->h_out_d + (size_t)e * sv->cfg.max_k, sizeof(float) * k);
+    if (hops) *hops = sv->h_hops[e];
+    if (visited) *visited = sv->h_vis[e];
+    sv->entry_seq[e] = ~0ull;
+    sv->in_flight--;
+    return 1;
+}
+
+int falcon_server_wait(falcon_server *sv, int64_t request_id, int64_t timeout_us, int32_t *out_ids,
+                       float *out_dists, int32_t *hops, int32_t *visited)
+{
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        const int rc = falcon_server_poll(sv, request_id, out_ids, out_dists, hops, visited);
+        if (rc != 0) return rc == 1 ? FALCON_OK : rc;
+        const auto us = std::chrono::duration_cast<std::chrono::microseconds>(std::chrono::steady_clock::now() - t0).count();
+        if (us > timeout_us) return set_error_code(FALCON_ERR_CUDA, "falcon_server_wait: timed out");
+        std::this_thread::yield();
+    }
+}
+
+int falcon_server_replay(falcon_server *sv, int32_t n, const int32_t *index_ids, const float *queries,
+                         int64_t query_stride, const falcon_search_params *params, int32_t per_request_params,
+                         const double *arrival_us, double *latency_us, int32_t *out_ids, int32_t out_stride,
+                         float *out_dists, int32_t *hops, int32_t *visited, double *elapsed_us)
+{
+    if (!sv || n < 0 || !arrival_us || !latency_us || (n > 0 && (!index_ids || !queries || !params)))
+        return set_error_code(FALCON_ERR_ARG, "falcon_server_replay: null argument");
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
+    auto now_us = [&]() { return std::chrono::duration<double, std::micro>(clk::now() - t0).count(); };
+    std::vector<int64_t> rid((size_t)n, -1);
+    std::vector<int> pending;            // submitted, not collected
+    pending.reserve(n > 0 ? (size_t)n : 1);
+    int next = 0, done = 0;
+    std::vector<int32_t> tmp_ids(sv->cfg.max_k);
+    std::vector<float> tmp_d(sv->cfg.max_k);
+    const int kBatch = 512;
+    while (done < n) {
+        const double t = now_us();
+        // submit everything that has arrived (in order), as ring entries allow
+        int end = next;
+        while (end < n && arrival_us[end] <= t && end - next < kBatch) end++;
+        if (end > next) {
+            const int cnt = end - next;
+            const int rc = falcon_server_submit(sv, cnt, index_ids + next, queries + (size_t)next * query_stride,
+                                                query_stride, params + (per_request_params ? next : 0),
+                                                per_request_params, rid.data() + next);
+            if (rc < 0) return rc;
+            for (int i = 0; i < rc; i++) pending.push_back(next + i);
+            next += rc;
+        }
+        // collect completions
+        for (size_t j = 0; j < pending.size();) {
+            const int i = pending[j];
+            int32_t h = 0, v = 0;
+            const int rc = falcon_server_poll(sv, rid[i], out_ids ? out_ids + (size_t)i * out_stride : tmp_ids.data(),
+                                              out_dists ? out_dists + (size_t)i * out_stride : tmp_d.data(), &h, &v);
+            if (rc < 0) return rc;
+            if (rc == 1) {
+                latency_us[i] = now_us() - arrival_us[i];
+                if (hops) hops[i] = h;
+                if (visited) visited[i] = v;
+                pending[j] = pending.back();
+                pending.pop_back();
+                done++;
+            } else {
+                j++;
+            }
+        }
+        if (pending.empty() && next < n) {   // idle until the next arrival
+            while (now_us() < arrival_us[next]) std::this_thread::yield();
+        }
+    }
+    if (elapsed_us) *elapsed_us = now_us();
+    return FALCON_OK;
+}
+
+int falcon_server_info_get(falcon_server *sv, falcon_server_info *info)
+{
+    if (!sv || !info) return set_error_code(FALCON_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lock(sv->mu);
+    info->ring_entries = sv->cap;
+    info->in_flight = sv->in_flight;
+    info->submitted = (int64_t)sv->next_seq;
+    info->kernel_launches = sv->launches;
+    info->warps = sv->grid * 4;
+    info->device_bytes = sv->device_bytes;
+    return FALCON_OK;
+}
+
+int falcon_server_free(falcon_server *sv)
+{
+    if (!sv) return FALCON_OK;
+    cudaSetDevice(sv->device);
+    {
+        std::lock_guard<std::mutex> lock(sv->mu);
+        const int32_t stop = 1;
+        cudaMemcpy(&sv->d_ctl->stop, &stop, sizeof(stop), cudaMemcpyHostToDevice);
+    }
+    cudaStreamSynchronize(sv->cstream);
+    cudaStreamSynchronize(sv->kstream);
+    free_server(sv);
+    return FALCON_OK;
+}
+
+}  // extern "C"

@@ -77,6 +77,27 @@ class SearchParams(ctypes.Structure):
     ]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int32),
+        ("ring_capacity", ctypes.c_int32),
+        ("max_k", ctypes.c_int32),
+        ("ef_max", ctypes.c_int32),
+        ("cand_queue_max", ctypes.c_int32),
+        ("bloom_bits_max", ctypes.c_int32),
+        ("mc_max", ctypes.c_int32),
+        ("mg_max", ctypes.c_int32),
+        ("dim_max", ctypes.c_int32),
+        ("idle_exit_us", ctypes.c_int64),
+        ("memory_fraction", ctypes.c_double),
+    ]
+
+
+class ServerInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in
+                ("ring_entries", "in_flight", "submitted", "kernel_launches", "warps", "device_bytes")]
+
+
 # Every symbol include/falcon.h declares, with its ctypes signature.
 _VP = ctypes.c_void_p
 _I32 = ctypes.c_int32
@@ -94,6 +115,16 @@ SIGNATURES = {
                                      _VP, _VP, _I32, _VP, _VP, _VP]),
     "falcon_vadd": (_I32, [_I32, _I32, _I32, _I32, _I32, _I32, _I32, ctypes.c_uint32, _I32, _I32, _I32, _I64,
                            _VP, _VP, _VP, _VP, _VP, _VP, _VP, _I32]),
+    "falcon_server_default_config": (None, [ctypes.POINTER(ServerConfig)]),
+    "falcon_server_create": (_I32, [ctypes.POINTER(ServerConfig), ctypes.POINTER(_VP)]),
+    "falcon_server_add_index": (_I32, [_VP, _VP, ctypes.POINTER(ctypes.c_int32)]),
+    "falcon_server_submit": (_I32, [_VP, _I32, _VP, _VP, _I64, ctypes.POINTER(SearchParams), _I32, _VP]),
+    "falcon_server_poll": (_I32, [_VP, _I64, _VP, _VP, ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
+    "falcon_server_wait": (_I32, [_VP, _I64, _I64, _VP, _VP, ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
+    "falcon_server_replay": (_I32, [_VP, _I32, _VP, _VP, _I64, ctypes.POINTER(SearchParams), _I32, _VP, _VP, _VP,
+                                    _I32, _VP, _VP, _VP, _VP]),
+    "falcon_server_info_get": (_I32, [_VP, ctypes.POINTER(ServerInfo)]),
+    "falcon_server_free": (_I32, [_VP]),
     "falcon_last_error": (ctypes.c_char_p, []),
     "falcon_build_info": (ctypes.c_char_p, []),
 }

@@ -9,7 +9,7 @@ CSRC = os.path.join(SRC_ROOT, "csrc")
 REPO = os.path.dirname(SRC_ROOT)
 LIB_PATH = os.path.join(PKG_DIR, "libfalcon_b200.so")
 
-SOURCES = ["falcon_kernels.cu", "falcon_capi.cu", "falcon_noalloc.cu"]
+SOURCES = ["falcon_kernels.cu", "falcon_capi.cu", "falcon_noalloc.cu", "falcon_serve.cu"]
 HEADERS = ["falcon_internal.h"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

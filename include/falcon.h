@@ -201,6 +201,68 @@ int falcon_vadd(int32_t query_num, int32_t query_batch_size, int32_t ef, int32_t
                 const void *db_vectors, const void *links_base, int32_t *out_id, float *out_dist,
                 int32_t *mem_debug, int32_t device);
 
+/*
+ * Serving: continuous batching of single-query requests against several
+ * device-resident indexes.  Extends the reference's networked serving path
+ * (networked_FPGA/CPU_programs/README.md:50-72, CPU_client.cpp:455-612: a
+ * client streams query batches to the FPGA and collects per-query results)
+ * with on-device admission.  A persistent kernel, launched from a captured
+ * CUDA graph, pulls requests from a device ring while the host keeps
+ * appending, so requests that arrive while others run start as soon as a warp
+ * is free; each request has its own index, precision, k, ef, mc, mg.  The ring
+ * is sized from free device memory (memory_fraction); falcon_server_submit
+ * admits requests in order while ring entries are free and returns how many it
+ * admitted (the caller keeps the rest and retries after collecting results).
+ * Results are collected with falcon_server_poll / falcon_server_wait.
+ * Only inter-query mode is served.
+ */
+typedef struct falcon_server falcon_server;
+
+typedef struct falcon_server_config {
+    int32_t device;
+    int32_t ring_capacity;          /* most requests admitted and not yet collected */
+    int32_t max_k;                  /* largest k of any request */
+    int32_t ef_max;                 /* largest ef (1..1024) */
+    int32_t cand_queue_max;         /* largest cand_queue_size (1..256) */
+    int32_t bloom_bits_max;         /* largest bloom_bits (10..24) */
+    int32_t mc_max, mg_max;
+    int32_t dim_max;                /* largest dimension of a registered index */
+    int64_t idle_exit_us;           /* the kernel leaves after this long without work */
+    double memory_fraction;         /* share of free device memory for per-request state */
+} falcon_server_config;
+
+typedef struct falcon_server_info {
+    int64_t ring_entries, in_flight, submitted, kernel_launches, warps, device_bytes;
+} falcon_server_info;
+
+void falcon_server_default_config(falcon_server_config *c);
+int falcon_server_create(const falcon_server_config *c, falcon_server **out);
+/* Register a resident index (same device); *index_id names it in requests. */
+int falcon_server_add_index(falcon_server *sv, falcon_index *ix, int32_t *index_id);
+/* Submit n requests (host queries, row stride query_stride floats; one params
+   struct or n of them).  Returns the number admitted (>= 0; the first ones in
+   order) and their ids in request_ids, or a negative error. */
+int falcon_server_submit(falcon_server *sv, int32_t n, const int32_t *index_ids, const float *queries,
+                         int64_t query_stride, const falcon_search_params *params, int32_t per_request_params,
+                         int64_t *request_ids);
+/* 1 and the k results if done (the request is then collected), 0 if pending. */
+int falcon_server_poll(falcon_server *sv, int64_t request_id, int32_t *out_ids, float *out_dists, int32_t *hops,
+                       int32_t *visited);
+/* Poll until done or timeout_us; FALCON_OK when done. */
+int falcon_server_wait(falcon_server *sv, int64_t request_id, int64_t timeout_us, int32_t *out_ids,
+                       float *out_dists, int32_t *hops, int32_t *visited);
+/* Load driver: replay an arrival schedule (microsecond offsets from the call,
+   ascending) from the calling thread.  Each request is submitted when it has
+   arrived and a ring entry is free, completions are detected by polling, and
+   latency_us[i] = completion - arrival (queueing included).  Results go to
+   out_ids / out_dists (n x out_stride, may be NULL), hops, visited. */
+int falcon_server_replay(falcon_server *sv, int32_t n, const int32_t *index_ids, const float *queries,
+                         int64_t query_stride, const falcon_search_params *params, int32_t per_request_params,
+                         const double *arrival_us, double *latency_us, int32_t *out_ids, int32_t out_stride,
+                         float *out_dists, int32_t *hops, int32_t *visited, double *elapsed_us);
+int falcon_server_info_get(falcon_server *sv, falcon_server_info *info);
+int falcon_server_free(falcon_server *sv);
+
 /* Thread-local description of the last error on this thread. */
 const char *falcon_last_error(void);
 
