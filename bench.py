@@ -166,6 +166,41 @@ def sweep(ix, q, gt):
     return best, bool(ok), res
 
 
+def serve_measurements(ix, q, gt, ef, mc, mg, cq, bits, batched_bf16_qps):
+    """Continuous batching: single-query requests with Poisson arrivals through
+    the serving kernel (BF16 traversal + exact FP32 rerank), at fractions of the
+    batched BF16 throughput and at saturation.  Reports sustained QPS (completed
+    requests / wall time), p50/p99 latency (arrival to completion, queueing
+    included) and recall@10 of the served results."""
+    from falcon_b200 import make_params
+    from falcon_b200.groundtruth import recall_at_k
+    from falcon_b200.serving import FalconServer, poisson_arrivals
+    sv = FalconServer(ring_capacity=65536, max_k=K, ef_max=ef, cand_queue_max=cq, bloom_bits_max=bits,
+                      mc_max=max(mc, 1), mg_max=max(mg, 1), dim_max=DIM, idle_exit_us=5000)
+    iid = sv.add_index(ix)
+    p = make_params(k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, precision="bf16", rerank=True)
+    n = 2 * N_QUERIES
+    qq = np.concatenate([q, q])
+    out = {"precision": "bf16+fp32 rerank", "requests_per_point": n, "points": []}
+    sv.replay(np.full(1000, iid), qq[:1000], p, poisson_arrivals(1000, batched_bf16_qps, 9), K)   # warm-up
+    for frac in (0.5, 0.8, 10.0):
+        rate = batched_bf16_qps * frac
+        arr = poisson_arrivals(n, rate, seed=int(frac * 100))
+        lat, ids, d, hops, vis, el = sv.replay(np.full(n, iid), qq, p, arr, K)
+        rec = recall_at_k(ids[:N_QUERIES], gt, K)
+        pt = {"offered_qps": rate if frac < 10 else None, "offered": "saturation" if frac >= 10 else "%.0f%%" % (frac * 100),
+              "sustained_qps": n / (el / 1e6), "p50_ms": float(np.percentile(lat, 50)) / 1e3,
+              "p99_ms": float(np.percentile(lat, 99)) / 1e3, "recall@10": rec}
+        log("served %s: %.0f QPS sustained, p50 %.2f ms, p99 %.2f ms, recall %.4f" % (
+            pt["offered"], pt["sustained_qps"], pt["p50_ms"], pt["p99_ms"], rec))
+        out["points"].append(pt)
+    inf = sv.info()
+    out["kernel_launches"] = int(inf.kernel_launches)
+    out["ring_entries"] = int(inf.ring_entries)
+    sv.close()
+    return out
+
+
 def cpu_baseline(x, q, g, gt, ef, threads, budget_s=15.0):
     """Reference CPU search (vendored hnswlib, built from the reference's
     headers) on the same graph, all host threads, bounded sample."""
@@ -351,6 +386,8 @@ def run_ours(args):
     torch.cuda.synchronize()
     bf_ms = a.elapsed_time(b) / 3
     bf_recall = recall_at_k(rb.ids.cpu().numpy(), gt, K)
+    served = None if args.no_serve else serve_measurements(ix, q, gt, ef, mc, mg, cq, bits,
+                                                           N_QUERIES / (bf_ms / 1e3))
 
     peak, peak_kind = measured_peak()
     alg = algorithmic_bytes(hops, vis, ef)
@@ -383,6 +420,7 @@ def run_ours(args):
         "e2e": {"value": e2e_qps, "unit": "queries/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(q.nbytes), "d2h_bytes_per_step": int(N_QUERIES * K * 8 + N_QUERIES * 8)},
         "bf16_rerank": {"value": N_QUERIES / (bf_ms / 1e3), "unit": "queries/s", "recall@10": bf_recall},
+        "served": served,
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
         "roofline": roof,
@@ -403,6 +441,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the continuous-batching measurements")
     ap.add_argument("--n-base", type=int, default=None, help="scaled-down runs for quick checks only")
     ap.add_argument("--n-queries", type=int, default=None)
     ap.add_argument("--fixed", default=None, help="ef,mc,mg,cq,bloom_bits: skip the sweep")

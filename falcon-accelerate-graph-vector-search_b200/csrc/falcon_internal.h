@@ -99,6 +99,7 @@ struct ServeDesc {
 struct ServeCtl {
     unsigned long long head;        // requests claimed by warps
     unsigned long long tail;        // requests published by the host
+    long long last_active_ns;       // last claim or completion (globaltimer)
     int32_t stop;                   // host: leave when idle
     int32_t error;
 };
@@ -130,14 +131,14 @@ __host__ __device__ inline size_t serve_warp_smem_bytes(int bloom_bits_max, int 
 {
     size_t b = (bloom_bits_max <= kMaxSmemBloomBits) ? ((size_t)1 << (bloom_bits_max - 3)) : 0;
     b += (size_t)heap_cap * (sizeof(uint64_t) + sizeof(int));
-    b += (size_t)ef_max * (sizeof(float) + sizeof(int));
+    if (heap_cap == 0) b += (size_t)ef_max * (sizeof(float) + sizeof(int));   // else the heap is reused
     b += sizeof(int) * (size_t)(mc_max * mg_max + mg_max + 32);
     return (b + 15) & ~(size_t)15;
 }
 
 // Serving kernel launch configuration for entries-per-lane `epl` (8 or 32).
-cudaError_t serve_config(const ServeLaunch &s, int epl, int num_sms, int *grid, size_t *smem);
-cudaError_t launch_serve(const ServeLaunch &s, int epl, int grid, size_t smem, cudaStream_t st);
+cudaError_t serve_config(const ServeLaunch &s, int epl, int vmax, int num_sms, int *grid, size_t *smem);
+cudaError_t launch_serve(const ServeLaunch &s, int epl, int vmax, int grid, size_t smem, cudaStream_t st);
 
 // A validated search request (host side), used by falcon_search_noalloc.
 struct SearchPlan {

@@ -395,20 +395,32 @@ __device__ __forceinline__ bool bloom_chunk(uint32_t *words, uint32_t mask, uint
 // ---------------------------------------------------------------------------
 // One query, inter-query semantics (v1.3).
 // ---------------------------------------------------------------------------
+// Per-query inputs and outputs of search_one_inter.
+struct QueryIO {
+    const float *query;             // dim floats
+    int entry;
+    int32_t *out_ids;               // result row
+    float *out_d;
+    int out_stride;                 // row length (filled with -1 / large past the results)
+    int write_all_ef;               // 1: write ef results, physical ids (rerank input)
+    int32_t *hops;                  // per-query counters (may be null)
+    int32_t *visited;
+    int32_t *status;
+};
+
 template <int ELEM, int EPL, int VROWS>
-__device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_t qi, uint32_t *bloom, int *fifo,
+__device__ void search_one_inter(const GraphView &g, const QParams &P, const QueryIO &io, uint32_t *bloom, int *fifo,
                                  int *fifo_len, int *sids, uint64_t *hkey, int *hid, int lane)
 {
     constexpr bool HEAP = EPL > 8;            // result list as a shared-memory heap
     constexpr int REPL = HEAP ? 1 : EPL;      // register entries per lane
     constexpr int EPS = ET<ELEM>::EPS;
     constexpr int NB = (VROWS == 1) ? 8 : 4;
-    const GraphView &g = A.g;
     const int nseg = g.dpad * ET<ELEM>::BYTES / 16;
 
     float q[VROWS][EPS];
     {
-        const float *Q = A.queries + qi * A.qstride;
+        const float *Q = io.query;
 #pragma unroll
         for (int r = 0; r < VROWS; r++) {
             const int seg = lane + 32 * r;
@@ -444,11 +456,11 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
     for (int e = 0; e < CPL; e++) { cd[e] = kLarge; ci[e] = -1; }
     float rmax = kLarge, cmax = kLarge;   // current maxima (warp-uniform)
 
-    int entry = A.entries ? A.entries[qi] : A.default_entry;
+    int entry = io.entry;
     const int mc = P.mc, mg = P.mg;
     int head = 0, inflight = 1, hops = 1, visited = 0;
     if (entry < 0 || (int64_t)entry >= g.n) {   // bad entry from a device-memory caller: empty result
-        if (lane == 0) atomicOr(A.status, 2);
+        if (lane == 0) atomicOr(io.status, 2);
         entry = 0;
         inflight = 0;
         hops = 0;
@@ -542,9 +554,9 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
     }
 
     // results best-first (DRAM_utils.hpp:460-464): list position i is result i
-    const int nwrite = A.write_all_ef ? P.ef : P.k;
-    int32_t *oid_row = A.out_ids + qi * A.out_stride;
-    float *od_row = A.out_d + qi * A.out_stride;
+    const int nwrite = io.write_all_ef ? P.ef : P.k;
+    int32_t *oid_row = io.out_ids;
+    float *od_row = io.out_d;
     if constexpr (HEAP) {
         int n2 = 1;
         while (n2 < P.ef) n2 <<= 1;
@@ -553,7 +565,7 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
         warp_bitonic_sort(hkey, hid, n2, lane);
         for (int i = lane; i < nwrite; i += 32) {
             int id = hid[i];
-            if (!A.write_all_ef && g.labels && id >= 0) id = g.labels[id];
+            if (!io.write_all_ef && g.labels && id >= 0) id = g.labels[id];
             oid_row[i] = id;
             od_row[i] = __uint_as_float((uint32_t)(hkey[i] >> 32));
         }
@@ -564,17 +576,17 @@ __device__ void search_one_inter(const SearchLaunch &A, const QParams &P, int64_
             const int i = lane * EPL + e;
             if (i < nwrite) {
                 int id = ri[e];
-                if (!A.write_all_ef && g.labels && id >= 0) id = g.labels[id];
+                if (!io.write_all_ef && g.labels && id >= 0) id = g.labels[id];
                 oid_row[i] = id;
                 od_row[i] = rd[e];
             }
         }
     }
-    for (int i = nwrite + lane; i < A.out_stride; i += 32) { oid_row[i] = -1; od_row[i] = kLarge; }
+    for (int i = nwrite + lane; i < io.out_stride; i += 32) { oid_row[i] = -1; od_row[i] = kLarge; }
     if (lane == 0) {
-        if (A.out_hops) A.out_hops[qi] = hops;
-        if (A.out_visited) A.out_visited[qi] = visited;
-        if (truncated) atomicOr(A.status, 1);
+        if (io.hops) *io.hops = hops;
+        if (io.visited) *io.visited = visited;
+        if (truncated) atomicOr(io.status, 1);
     }
 }
 
@@ -610,7 +622,17 @@ __global__ void __launch_bounds__(128) inter_kernel(const SearchLaunch A)
         qi = __shfl_sync(kFull, qi, 0);
         if (qi >= (unsigned long long)A.nq) break;
         const QParams P = A.params[A.per_query ? qi : 0];
-        search_one_inter<ELEM, EPL, VROWS>(A, P, (int64_t)qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+        QueryIO io;
+        io.query = A.queries + (int64_t)qi * A.qstride;
+        io.entry = A.entries ? A.entries[qi] : A.default_entry;
+        io.out_ids = A.out_ids + (int64_t)qi * A.out_stride;
+        io.out_d = A.out_d + (int64_t)qi * A.out_stride;
+        io.out_stride = A.out_stride;
+        io.write_all_ef = A.write_all_ef;
+        io.hops = A.out_hops ? A.out_hops + qi : nullptr;
+        io.visited = A.out_visited ? A.out_visited + qi : nullptr;
+        io.status = A.status;
+        search_one_inter<ELEM, EPL, VROWS>(A.g, P, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
         __syncwarp();
     }
 }
@@ -1031,15 +1053,10 @@ __device__ __forceinline__ long long global_ns()
     return t;
 }
 
-template <int ELEM, int EPL, int VROWS>
-__device__ __forceinline__ void serve_search(SearchLaunch &A2, const QParams &P, int64_t qi, uint32_t *bloom,
-                                             int *fifo, int *fifo_len, int *sids, uint64_t *hkey, int *hid, int lane)
-{
-    search_one_inter<ELEM, EPL, VROWS>(A2, P, qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-}
-
-template <int EPL>
-__global__ void __launch_bounds__(128) serve_kernel(const ServeLaunch S)
+// VMAX: FP32 16-byte rows per lane the server's largest dimension needs
+// (ceil(dpad/128)); only the traversal variants up to it are compiled in.
+template <int EPL, int VMAX>
+__global__ void __launch_bounds__(128, 4) serve_kernel(const ServeLaunch S)
 {
     extern __shared__ uint4 smem_u4[];
     constexpr int HEAP_CAP = (EPL > 8) ? 32 * EPL : 0;
@@ -1055,10 +1072,10 @@ __global__ void __launch_bounds__(128) serve_kernel(const ServeLaunch S)
     p += sizeof(uint64_t) * HEAP_CAP;
     int *hid = reinterpret_cast<int *>(p);
     p += sizeof(int) * HEAP_CAP;
-    float *rsd = reinterpret_cast<float *>(p);
-    p += sizeof(float) * S.ef_max;
-    int *rsi = reinterpret_cast<int *>(p);
-    p += sizeof(int) * S.ef_max;
+    // rerank scratch: the heap's space once the traversal has written its results
+    float *rsd = HEAP_CAP ? reinterpret_cast<float *>(hkey) : reinterpret_cast<float *>(p);
+    int *rsi = HEAP_CAP ? reinterpret_cast<int *>(hkey) + S.ef_max : reinterpret_cast<int *>(p) + S.ef_max;
+    if (!HEAP_CAP) p += (sizeof(float) + sizeof(int)) * S.ef_max;
     int *fifo = reinterpret_cast<int *>(p);
     int *fifo_len = fifo + S.mc_max * S.mg_max;
     int *sids = fifo_len + S.mg_max;
@@ -1066,7 +1083,6 @@ __global__ void __launch_bounds__(128) serve_kernel(const ServeLaunch S)
     int32_t *cand_ids = S.cand_ids + gw * S.ef_max;
     float *cand_d = S.cand_d + gw * S.ef_max;
 
-    long long idle_since = global_ns();
     for (;;) {
         unsigned long long h = ~0ull;
         if (lane == 0) {
@@ -1076,14 +1092,19 @@ __global__ void __launch_bounds__(128) serve_kernel(const ServeLaunch S)
                 if (hd >= tl) break;
                 if (atomicCAS(&S.ctl->head, hd, hd + 1) == hd) { h = hd; break; }
             }
+            if (h != ~0ull) atomicMax(&S.ctl->last_active_ns, global_ns());
         }
         h = __shfl_sync(kFull, h, 0);
         if (h == ~0ull) {
-            int stop = 0;
-            if (lane == 0) stop = *reinterpret_cast<volatile int *>(&S.ctl->stop);
-            stop = __shfl_sync(kFull, stop, 0);
-            if (stop || global_ns() - idle_since > S.idle_ns) break;
-            __nanosleep(2000);
+            // leave only when the whole server has been idle for idle_ns
+            int leave = 0;
+            if (lane == 0) {
+                const int stop = *reinterpret_cast<volatile int *>(&S.ctl->stop);
+                const long long last = *reinterpret_cast<volatile long long *>(&S.ctl->last_active_ns);
+                leave = stop || (global_ns() - last > S.idle_ns);
+            }
+            if (__shfl_sync(kFull, leave, 0)) break;
+            __nanosleep(1000);
             continue;
         }
         const int e = (int)(h % (unsigned long long)S.ring_cap);
@@ -1095,71 +1116,47 @@ __global__ void __launch_bounds__(128) serve_kernel(const ServeLaunch S)
             for (int w = 0; w < (int)(sizeof(ServeDesc) / sizeof(int)); w++) dst[w] = __ldcg(src + w);
         }
         const GraphView &v = S.views[D.index];
-        SearchLaunch A2;
-        A2.g = v;
-        A2.queries = S.qpool;
-        A2.qstride = S.qstride;
-        A2.entries = nullptr;
-        A2.default_entry = D.entry;
-        A2.nq = S.ring_cap;
-        A2.params = nullptr;
-        A2.per_query = 0;
         const bool rerank = D.p.rerank != 0 && D.precision != kF32;
-        A2.out_ids = rerank ? cand_ids : S.out_ids;
-        A2.out_d = rerank ? cand_d : S.out_d;
-        A2.out_stride = rerank ? S.ef_max : S.out_stride;
-        A2.write_all_ef = rerank ? 1 : 0;
-        A2.out_hops = S.out_hops;
-        A2.out_visited = S.out_visited;
-        A2.work_counter = nullptr;
-        A2.status = S.status;
-        A2.bloom_bits_max = S.bloom_bits_max;
-        A2.ef_max = S.ef_max;
-        A2.mc_max = S.mc_max;
-        A2.mg_max = S.mg_max;
-        A2.channels = 0;
-        A2.cq_max = S.cq_max;
-        A2.bloom_global = S.bloom_global;
-        // per-request output row: the ring entry (rerank candidates: this warp's row 0)
-        const int64_t row = rerank ? 0 : e;
-        if (rerank) {   // hops/visited still go to the ring entry
-            A2.out_hops = S.out_hops + e;
-            A2.out_visited = S.out_visited + e;
-            A2.queries = S.qpool + (int64_t)e * S.qstride;
-        }
-        const int64_t qi = rerank ? 0 : e;
+        QueryIO io;
+        io.query = S.qpool + (int64_t)e * S.qstride;
+        io.entry = D.entry;
+        io.out_ids = rerank ? cand_ids : S.out_ids + (int64_t)e * S.out_stride;
+        io.out_d = rerank ? cand_d : S.out_d + (int64_t)e * S.out_stride;
+        io.out_stride = rerank ? S.ef_max : S.out_stride;
+        io.write_all_ef = rerank ? 1 : 0;
+        io.hops = S.out_hops + e;
+        io.visited = S.out_visited + e;
+        io.status = S.status;
         const int seg_bytes = (D.precision == kF32) ? 4 : (D.precision == kBF16 ? 2 : 1);
         const int vrows = (v.dpad * seg_bytes / 16 + 31) / 32;
         if (D.precision == kF32) {
-            if (vrows == 1) serve_search<kF32, EPL, 1>(A2, D.p, qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-            else if (vrows == 2) serve_search<kF32, EPL, 2>(A2, D.p, qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-            else if (vrows == 3) serve_search<kF32, EPL, 3>(A2, D.p, qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-            else serve_search<kF32, EPL, 4>(A2, D.p, qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            if (vrows <= 1) search_one_inter<kF32, EPL, 1>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            else if (VMAX >= 2 && vrows == 2) search_one_inter<kF32, EPL, (VMAX >= 2 ? 2 : 1)>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            else if (VMAX >= 3 && vrows == 3) search_one_inter<kF32, EPL, (VMAX >= 3 ? 3 : 1)>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            else if (VMAX >= 4) search_one_inter<kF32, EPL, (VMAX >= 4 ? 4 : 1)>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
         } else if (D.precision == kBF16) {
-            if (vrows == 1) serve_search<kBF16, EPL, 1>(A2, D.p, qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-            else serve_search<kBF16, EPL, 2>(A2, D.p, qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            if (vrows <= 1) search_one_inter<kBF16, EPL, 1>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            else if (VMAX >= 3) search_one_inter<kBF16, EPL, (VMAX >= 3 ? 2 : 1)>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
         } else {
-            serve_search<kFP8, EPL, 1>(A2, D.p, qi, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            search_one_inter<kFP8, EPL, 1>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
         }
-        (void)row;
         if (rerank) {
             __syncwarp();
             const int vr32 = (v.dpad * 4 / 16 + 31) / 32;
-            const float *Q = S.qpool + (int64_t)e * S.qstride;
             int32_t *orow = S.out_ids + (int64_t)e * S.out_stride;
             float *drow = S.out_d + (int64_t)e * S.out_stride;
-            if (vr32 == 1) rerank_one<1>(v, D.p, Q, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
-            else if (vr32 == 2) rerank_one<2>(v, D.p, Q, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
-            else if (vr32 == 3) rerank_one<3>(v, D.p, Q, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
-            else rerank_one<4>(v, D.p, Q, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
+            if (vr32 <= 1) rerank_one<1>(v, D.p, io.query, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
+            else if (VMAX >= 2 && vr32 == 2) rerank_one<(VMAX >= 2 ? 2 : 1)>(v, D.p, io.query, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
+            else if (VMAX >= 3 && vr32 == 3) rerank_one<(VMAX >= 3 ? 3 : 1)>(v, D.p, io.query, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
+            else if (VMAX >= 4) rerank_one<(VMAX >= 4 ? 4 : 1)>(v, D.p, io.query, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
         }
         __syncwarp();
         if (lane == 0) {
             __threadfence_system();
             *reinterpret_cast<volatile unsigned long long *>(S.done + e) = D.seq + 1;
+            atomicMax(&S.ctl->last_active_ns, global_ns());
         }
         __syncwarp();
-        idle_since = global_ns();
     }
 }
 
@@ -1318,33 +1315,58 @@ cudaError_t search_bloom_slots(const SearchLaunch &a, int elem, int num_sms, int
     return search_dispatch(a, elem, num_sms, nullptr, slots);
 }
 
-cudaError_t serve_config(const ServeLaunch &sv, int epl, int num_sms, int *grid, size_t *smem)
+template <int EPL, int VMAX>
+static cudaError_t serve_config_t(const ServeLaunch &sv, int num_sms, int *grid, size_t *smem)
 {
-    const int heap_cap = (epl > 8) ? 32 * epl : 0;
+    const int heap_cap = (EPL > 8) ? 32 * EPL : 0;
     *smem = serve_warp_smem_bytes(sv.bloom_bits_max, sv.mc_max, sv.mg_max, heap_cap, sv.ef_max) * 4;
-    cudaError_t e;
+    cudaError_t e = cudaFuncSetAttribute(serve_kernel<EPL, VMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)*smem);
     int per_sm = 0;
-    if (epl == 8) {
-        e = cudaFuncSetAttribute(serve_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel<8>, 128, *smem);
-    } else if (epl == 32) {
-        e = cudaFuncSetAttribute(serve_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel<32>, 128, *smem);
-    } else {
-        return cudaErrorInvalidValue;
-    }
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel<EPL, VMAX>, 128, *smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     *grid = per_sm * num_sms;
     return cudaSuccess;
 }
 
-cudaError_t launch_serve(const ServeLaunch &sv, int epl, int grid, size_t smem, cudaStream_t st)
+template <int EPL>
+static cudaError_t serve_config_v(const ServeLaunch &sv, int vmax, int num_sms, int *grid, size_t *smem)
 {
-    if (epl == 8) serve_kernel<8><<<grid, 128, smem, st>>>(sv);
-    else if (epl == 32) serve_kernel<32><<<grid, 128, smem, st>>>(sv);
-    else return cudaErrorInvalidValue;
+    switch (vmax) {
+        case 1: return serve_config_t<EPL, 1>(sv, num_sms, grid, smem);
+        case 2: return serve_config_t<EPL, 2>(sv, num_sms, grid, smem);
+        case 3: return serve_config_t<EPL, 3>(sv, num_sms, grid, smem);
+        case 4: return serve_config_t<EPL, 4>(sv, num_sms, grid, smem);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t serve_config(const ServeLaunch &sv, int epl, int vmax, int num_sms, int *grid, size_t *smem)
+{
+    if (epl == 8) return serve_config_v<8>(sv, vmax, num_sms, grid, smem);
+    if (epl == 32) return serve_config_v<32>(sv, vmax, num_sms, grid, smem);
+    return cudaErrorInvalidValue;
+}
+
+template <int EPL>
+static cudaError_t launch_serve_v(const ServeLaunch &sv, int vmax, int grid, size_t smem, cudaStream_t st)
+{
+    switch (vmax) {
+        case 1: serve_kernel<EPL, 1><<<grid, 128, smem, st>>>(sv); break;
+        case 2: serve_kernel<EPL, 2><<<grid, 128, smem, st>>>(sv); break;
+        case 3: serve_kernel<EPL, 3><<<grid, 128, smem, st>>>(sv); break;
+        case 4: serve_kernel<EPL, 4><<<grid, 128, smem, st>>>(sv); break;
+        default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
+}
+
+cudaError_t launch_serve(const ServeLaunch &sv, int epl, int vmax, int grid, size_t smem, cudaStream_t st)
+{
+    if (epl == 8) return launch_serve_v<8>(sv, vmax, grid, smem, st);
+    if (epl == 32) return launch_serve_v<32>(sv, vmax, grid, smem, st);
+    return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_rerank(const RerankLaunch &a, int ef_max, int num_sms, cudaStream_t s)

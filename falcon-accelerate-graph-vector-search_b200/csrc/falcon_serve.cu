@@ -37,7 +37,7 @@ int check_search_params(const falcon_search_params &p, const falcon_index *ix, i
 
 struct falcon_server {
     falcon_server_config cfg;
-    int device = 0, num_sms = 0, epl = 8, grid = 0;
+    int device = 0, num_sms = 0, epl = 8, vmax = 1, grid = 0;
     size_t smem = 0;
     int cap = 0;                          // ring entries
     int qstride = 0;                      // floats per query slot
@@ -163,6 +163,7 @@ int falcon_server_create(const falcon_server_config *c, falcon_server **out)
     sv->device = c->device;
     sv->epl = (c->ef_max <= 256 && c->cand_queue_max <= 64) ? 8 : 32;
     sv->qstride = (c->dim_max + 15) / 16 * 16;
+    sv->vmax = (sv->qstride + 127) / 128;   // FP32 16-byte rows per lane for the largest dimension
     cudaError_t e;
     cudaDeviceProp prop;
     if ((e = cudaGetDeviceProperties(&prop, c->device)) != cudaSuccess) { free_server(sv); return cuda_fail(e, "properties"); }
@@ -189,7 +190,7 @@ int falcon_server_create(const falcon_server_config *c, falcon_server **out)
     L.ef_max = c->ef_max;
     L.cq_max = c->cand_queue_max;
     L.idle_ns = (long long)c->idle_exit_us * 1000;
-    if ((e = serve_config(L, sv->epl, sv->num_sms, &sv->grid, &sv->smem)) != cudaSuccess) {
+    if ((e = serve_config(L, sv->epl, sv->vmax, sv->num_sms, &sv->grid, &sv->smem)) != cudaSuccess) {
         free_server(sv);
         return cuda_fail(e, "serve kernel configuration");
     }
@@ -249,7 +250,7 @@ int falcon_server_create(const falcon_server_config *c, falcon_server **out)
     {
         cudaGraph_t g = nullptr;
         SV_ALLOC(cudaStreamBeginCapture(sv->kstream, cudaStreamCaptureModeThreadLocal), "capture");
-        e = launch_serve(L, sv->epl, sv->grid, sv->smem, sv->kstream);
+        e = launch_serve(L, sv->epl, sv->vmax, sv->grid, sv->smem, sv->kstream);
         cudaError_t e2 = cudaStreamEndCapture(sv->kstream, &g);
         if (e == cudaSuccess) e = e2;
         if (e == cudaSuccess) e = cudaGraphInstantiate(&sv->graph, g, 0);

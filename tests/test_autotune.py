@@ -1,0 +1,62 @@
+"""Autotuner: Bloom sizing from visited counts (CPU), profile storage and
+lookup (CPU), and one small measured tune on the GPU."""
+import math
+
+import numpy as np
+import pytest
+
+from helpers import small_graph
+
+
+def test_bloom_bits_for_false_rejection_target():
+    from falcon_b200.autotune import bloom_bits_for
+    prev = 0
+    for v in (100, 2000, 20000, 60000, 500000):
+        b = bloom_bits_for(v, 0.01)
+        assert b >= prev
+        prev = b
+        if b < 24:
+            assert (1 - math.exp(-3 * v / (1 << b))) ** 3 <= 0.01
+        if b > 16:
+            assert (1 - math.exp(-3 * v / (1 << (b - 1)))) ** 3 > 0.01
+    assert bloom_bits_for(2000, 0.01) == 16      # the reference's 2^16 suffices at ef=64 on SIFT-like visits
+
+
+def test_profile_roundtrip_and_pick(tmp_path):
+    from falcon_b200.autotune import load_profile, pick, save_profile, best_for_recall
+    prof = {
+        "D96_R64_ef64": {"throughput": {"params": {"k": 10, "ef": 64, "mc": 1, "mg": 1, "cand_queue_size": 32,
+                                                   "bloom_bits": 16, "mode": "inter"}, "qps": 1.5e6, "recall": 0.3},
+                         "latency": {"threads_per_query": 32, "mode": "inter", "channels": None, "median_ms": {}}},
+        "D96_R64_ef1024": {"throughput": {"params": {"k": 10, "ef": 1024, "mc": 1, "mg": 1, "cand_queue_size": 256,
+                                                     "bloom_bits": 20, "mode": "inter"}, "qps": 7e4, "recall": 0.96},
+                           "latency": {"threads_per_query": 256, "mode": "intra", "channels": 8, "median_ms": {}}},
+    }
+    path = str(tmp_path / "p.json")
+    save_profile(prof, path)
+    got = load_profile(path)
+    assert pick(got, 96, 64, 500)["ef"] == 1024
+    assert pick(got, 96, 64, 1024, objective="latency")["channels"] == 8
+    assert best_for_recall(got, 0.95)[0] == "D96_R64_ef1024"
+    with pytest.raises(KeyError):
+        pick(got, 128, 64, 64)
+
+
+@pytest.mark.gpu
+def test_tune_small_index():
+    from falcon_b200 import FalconIndex
+    from falcon_b200.autotune import tune
+    from falcon_b200.groundtruth import brute_force_f64
+    g, q = small_graph("unit", 6000, 96, 64, 200, seed=41)
+    ix = FalconIndex(g)
+    gt, _ = brute_force_f64(g.vectors, q, 10)
+    prof = tune(ix, q, gt, 96, 64, ef_list=(32, 128), recall_target=0.9, cq_grid=(32, 64),
+                mcmg_grid=((1, 1), (2, 2)), latency_channels=(4,))
+    assert set(prof) == {"D96_R64_ef32", "D96_R64_ef128"}
+    for e in prof.values():
+        t = e["throughput"]
+        assert t["qps"] > 0 and 0 <= t["recall"] <= 1
+        if e["recall_target_met"]:
+            assert t["recall"] >= 0.9
+        assert e["latency"]["mode"] in ("inter", "intra")
+    assert prof["D96_R64_ef128"]["throughput"]["recall"] >= prof["D96_R64_ef32"]["throughput"]["recall"]
