@@ -21,6 +21,8 @@ constexpr int kMaxSmemBloomBits = 18;   // larger filters live in global memory,
 constexpr int kMinBloomBits = 10;
 constexpr int kMaxDimPadded = 512;
 constexpr int kMaxChannels = 8;
+// Neighbour ids staged per warp: a whole adjacency row of up to 64 ids.
+constexpr int kSidsPerWarp = 64;
 
 // Device view of one resident graph.
 struct GraphView {
@@ -132,7 +134,7 @@ __host__ __device__ inline size_t serve_warp_smem_bytes(int bloom_bits_max, int 
     size_t b = (bloom_bits_max <= kMaxSmemBloomBits) ? ((size_t)1 << (bloom_bits_max - 3)) : 0;
     b += (size_t)heap_cap * (sizeof(uint64_t) + sizeof(int));
     if (heap_cap == 0) b += (size_t)ef_max * (sizeof(float) + sizeof(int));   // else the heap is reused
-    b += sizeof(int) * (size_t)(mc_max * mg_max + mg_max + 32);
+    b += sizeof(int) * (size_t)(mc_max * mg_max + mg_max + kSidsPerWarp);
     return (b + 15) & ~(size_t)15;
 }
 

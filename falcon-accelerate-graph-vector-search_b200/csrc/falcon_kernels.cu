@@ -392,6 +392,87 @@ __device__ __forceinline__ bool bloom_chunk(uint32_t *words, uint32_t mask, uint
     return active && !(p0 && p1 && p2);
 }
 
+// Bloom check of a whole adjacency row of up to 64 ids (lane l holds ids l
+// and 32+l), same sequential semantics as bloom_chunk.  The filter bits of
+// all ids are read first and give a provisional answer; the atomics that set
+// the clear bits are issued at once but their old values are only examined by
+// bloom_row_resolve, after the caller has issued its vector gathers, so the
+// atomic round trip overlaps the gathers.  A collision (a bit set first by
+// another id of this row) can only turn a provisional "new" into "seen".
+struct BloomRow {
+    uint32_t h[2][3];
+    bool pre[2][3];
+    uint32_t old[2][3];
+    bool act[2];
+};
+
+__device__ __forceinline__ void bloom_row_begin(BloomRow &B, uint32_t *words, uint32_t mask, uint32_t seed,
+                                                int k0, int k1, bool a0, bool a1, bool &prov0, bool &prov1)
+{
+    B.act[0] = a0;
+    B.act[1] = a1;
+    const int key[2] = {k0, k1};
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            B.h[c][j] = B.act[c] ? (murmur2_keylen4((uint32_t)key[c], seed + (uint32_t)j) & mask) : 0u;
+            B.pre[c][j] = B.act[c] ? (((words[B.h[c][j] >> 5] >> (B.h[c][j] & 31)) & 1u) != 0) : true;
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            B.old[c][j] = 0u;
+            if (B.act[c] && !B.pre[c][j]) B.old[c][j] = atomicOr(&words[B.h[c][j] >> 5], 1u << (B.h[c][j] & 31));
+        }
+    }
+    prov0 = a0 && !(B.pre[0][0] && B.pre[0][1] && B.pre[0][2]);
+    prov1 = a1 && !(B.pre[1][0] && B.pre[1][1] && B.pre[1][2]);
+}
+
+// Exact validity (sequential semantics) of the two ids of this lane.
+__device__ __forceinline__ void bloom_row_resolve(BloomRow &B, int lane, bool &v0, bool &v1)
+{
+    bool coll = false;
+#pragma unroll
+    for (int c = 0; c < 2; c++)
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+            coll |= B.act[c] && !B.pre[c][j] && ((B.old[c][j] >> (B.h[c][j] & 31)) & 1u);
+    bool s[2][3];
+#pragma unroll
+    for (int c = 0; c < 2; c++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) s[c][j] = B.pre[c][j];
+    if (__any_sync(kFull, coll)) {
+        const unsigned am0 = __ballot_sync(kFull, B.act[0]);
+        const unsigned am1 = __ballot_sync(kFull, B.act[1]);
+        for (int src = 0; src < 32; src++) {
+            uint32_t t0[3], t1[3];
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                t0[j] = __shfl_sync(kFull, B.h[0][j], src);
+                t1[j] = __shfl_sync(kFull, B.h[1][j], src);
+            }
+            const bool src0 = (am0 >> src) & 1u, src1 = (am1 >> src) & 1u;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                // first-half id of this lane: earlier ids are first-half ids of lower lanes
+                if (src0 && src < lane) s[0][j] |= (B.h[0][j] == t0[0]) | (B.h[0][j] == t0[1]) | (B.h[0][j] == t0[2]);
+                // second-half id: every first-half id, and second-half ids of lower lanes
+                if (src0) s[1][j] |= (B.h[1][j] == t0[0]) | (B.h[1][j] == t0[1]) | (B.h[1][j] == t0[2]);
+                if (src1 && src < lane) s[1][j] |= (B.h[1][j] == t1[0]) | (B.h[1][j] == t1[1]) | (B.h[1][j] == t1[2]);
+            }
+        }
+    }
+    v0 = B.act[0] && !(s[0][0] && s[0][1] && s[0][2]);
+    v1 = B.act[1] && !(s[1][0] && s[1][1] && s[1][2]);
+    __syncwarp();
+}
+
 // ---------------------------------------------------------------------------
 // One query, inter-query semantics (v1.3).
 // ---------------------------------------------------------------------------
@@ -408,7 +489,12 @@ struct QueryIO {
     int32_t *status;
 };
 
-template <int ELEM, int EPL, int VROWS>
+template <int ELEM, int VROWS>
+constexpr bool kRowBloom = (VROWS == 1 && ELEM != kFP8);
+
+// ROW selects the whole-row Bloom path for degrees <= 64; instances whose
+// vector registers leave no room for it keep the per-32-id path.
+template <int ELEM, int EPL, int VROWS, bool ROW>
 __device__ void search_one_inter(const GraphView &g, const QParams &P, const QueryIO &io, uint32_t *bloom, int *fifo,
                                  int *fifo_len, int *sids, uint64_t *hkey, int *hid, int lane)
 {
@@ -474,6 +560,84 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
         for (int b = 0; b < glen; b++) {
             const int node = fifo[head * mc + b];
             const int32_t *row = g.links + (int64_t)node * g.lstride;
+            if (ROW && g.max_degree <= 64) {
+                // count and ids in one round trip (the row always holds max_degree slots)
+                const int cnt = ld_nc_s32(row);
+                const int n0 = (lane < g.max_degree) ? ld_nc_s32(row + g.ids_off + lane) : -1;
+                const int n1 = (32 + lane < g.max_degree) ? ld_nc_s32(row + g.ids_off + 32 + lane) : -1;
+                const bool a0 = lane < cnt, a1 = 32 + lane < cnt;
+                BloomRow B;
+                bool p0, p1;
+                bloom_row_begin(B, bloom, bmask, P.seed, n0, n1, a0, a1, p0, p1);
+                // provisional candidates in stream order (first half, then second half)
+                const unsigned pm0 = __ballot_sync(kFull, p0), pm1 = __ballot_sync(kFull, p1);
+                const int PV0 = __popc(pm0), PV = PV0 + __popc(pm1);
+                if (p0) sids[__popc(pm0 & ((1u << lane) - 1u))] = n0;
+                if (p1) sids[PV0 + __popc(pm1 & ((1u << lane) - 1u))] = n1;
+                __syncwarp();
+                bool resolved = false, v0 = false, v1 = false;
+                unsigned vm0 = 0, vm1 = 0;
+                for (int b0 = 0; b0 < PV; b0 += NB) {
+                    uint4 raw[NB][VROWS];
+                    float scale[NB];
+#pragma unroll
+                    for (int t = 0; t < NB; t++) {
+                        const bool tv = b0 + t < PV;
+                        const int id = tv ? sids[b0 + t] : 0;
+                        const unsigned char *base = g.vecs + (int64_t)id * g.vstride_bytes;
+                        scale[t] = 1.0f;
+                        if constexpr (ELEM == kFP8) scale[t] = tv ? g.scales[id] : 1.0f;
+#pragma unroll
+                        for (int r = 0; r < VROWS; r++) {
+                            const int seg = lane + 32 * r;
+                            raw[t][r] = (tv && seg < nseg) ? ld_nc_v4(base + 16 * seg) : make_uint4(0, 0, 0, 0);
+                        }
+                    }
+                    if (!resolved) {   // the atomics overlapped the first gathers
+                        bloom_row_resolve(B, lane, v0, v1);
+                        vm0 = __ballot_sync(kFull, v0);
+                        vm1 = __ballot_sync(kFull, v1);
+                        resolved = true;
+                    }
+                    const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane);
+                    const int nt = min(NB, PV - b0);
+                    // provisional slot b0+t is exact-valid iff its id's lane bit survived
+                    bool keep = false;
+                    if (lane < nt) {
+                        const int slot = b0 + lane;
+                        if (slot < PV0) keep = (vm0 >> __fns(pm0, 0, slot + 1)) & 1u;
+                        else keep = (vm1 >> __fns(pm1, 0, slot - PV0 + 1)) & 1u;
+                    }
+                    unsigned m = __ballot_sync(kFull, lane < nt && keep && dist < rmax);
+                    while (m) {
+                        const int t = __ffs(m) - 1;
+                        m &= m - 1;
+                        const float dd = __shfl_sync(kFull, dist, t);
+                        if (dd < rmax) {
+                            const int id = sids[b0 + t];
+                            if constexpr (HEAP) {
+                                heap_replace_root(hkey, hid, P.ef, heap_key(dd, ++age), id, lane);
+                                rmax = __uint_as_float((uint32_t)(hkey[0] >> 32));
+                            } else {
+                                rl_insert<EPL>(rd, ri, lane, dd, id);
+                                rmax = rl_get<EPL>(rd, P.ef - 1);
+                            }
+                            if (dd < cmax) {
+                                cl_insert<CPL>(cd, ci, lane, P.cq, dd, id);
+                                cmax = rl_get<CPL>(cd, P.cq - 1);
+                            }
+                        }
+                    }
+                }
+                if (!resolved) {
+                    bloom_row_resolve(B, lane, v0, v1);
+                    vm0 = __ballot_sync(kFull, v0);
+                    vm1 = __ballot_sync(kFull, v1);
+                }
+                visited += __popc(vm0) + __popc(vm1);
+                __syncwarp();
+                continue;
+            }
             const int cnt = ld_nc_s32(row);
             for (int c0 = 0; c0 < cnt; c0 += 32) {
                 const bool act = c0 + lane < cnt;
@@ -594,12 +758,12 @@ __host__ __device__ __forceinline__ size_t warp_smem_bytes(int bloom_bits_max, i
 {
     size_t b = (bloom_bits_max <= kMaxSmemBloomBits) ? ((size_t)1 << (bloom_bits_max - 3)) : 0;
     b += (size_t)heap_cap * (sizeof(uint64_t) + sizeof(int));
-    b += sizeof(int) * (size_t)(mc_max * mg_max + mg_max + 32);
+    b += sizeof(int) * (size_t)(mc_max * mg_max + mg_max + kSidsPerWarp);
     return (b + 15) & ~(size_t)15;
 }
 
 template <int ELEM, int EPL, int VROWS>
-__global__ void __launch_bounds__(128) inter_kernel(const SearchLaunch A)
+__global__ void __launch_bounds__(128, 4) inter_kernel(const SearchLaunch A)
 {
     extern __shared__ uint4 smem_u4[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -632,7 +796,8 @@ __global__ void __launch_bounds__(128) inter_kernel(const SearchLaunch A)
         io.hops = A.out_hops ? A.out_hops + qi : nullptr;
         io.visited = A.out_visited ? A.out_visited + qi : nullptr;
         io.status = A.status;
-        search_one_inter<ELEM, EPL, VROWS>(A.g, P, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+        search_one_inter<ELEM, EPL, VROWS, kRowBloom<ELEM, VROWS>>(A.g, P, io, bloom, fifo, fifo_len, sids, hkey, hid,
+                                                                   lane);
         __syncwarp();
     }
 }
@@ -1130,15 +1295,15 @@ __global__ void __launch_bounds__(128, 4) serve_kernel(const ServeLaunch S)
         const int seg_bytes = (D.precision == kF32) ? 4 : (D.precision == kBF16 ? 2 : 1);
         const int vrows = (v.dpad * seg_bytes / 16 + 31) / 32;
         if (D.precision == kF32) {
-            if (vrows <= 1) search_one_inter<kF32, EPL, 1>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-            else if (VMAX >= 2 && vrows == 2) search_one_inter<kF32, EPL, (VMAX >= 2 ? 2 : 1)>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-            else if (VMAX >= 3 && vrows == 3) search_one_inter<kF32, EPL, (VMAX >= 3 ? 3 : 1)>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-            else if (VMAX >= 4) search_one_inter<kF32, EPL, (VMAX >= 4 ? 4 : 1)>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            if (vrows <= 1) search_one_inter<kF32, EPL, 1, false>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            else if (VMAX >= 2 && vrows == 2) search_one_inter<kF32, EPL, (VMAX >= 2 ? 2 : 1), false>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            else if (VMAX >= 3 && vrows == 3) search_one_inter<kF32, EPL, (VMAX >= 3 ? 3 : 1), false>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            else if (VMAX >= 4) search_one_inter<kF32, EPL, (VMAX >= 4 ? 4 : 1), false>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
         } else if (D.precision == kBF16) {
-            if (vrows <= 1) search_one_inter<kBF16, EPL, 1>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-            else if (VMAX >= 3) search_one_inter<kBF16, EPL, (VMAX >= 3 ? 2 : 1)>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            if (vrows <= 1) search_one_inter<kBF16, EPL, 1, false>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            else if (VMAX >= 3) search_one_inter<kBF16, EPL, (VMAX >= 3 ? 2 : 1), false>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
         } else {
-            search_one_inter<kFP8, EPL, 1>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            search_one_inter<kFP8, EPL, 1, false>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
         }
         if (rerank) {
             __syncwarp();
