@@ -476,6 +476,28 @@ __device__ __forceinline__ void bloom_row_resolve(BloomRow &B, int lane, bool &v
 // ---------------------------------------------------------------------------
 // One query, inter-query semantics (v1.3).
 // ---------------------------------------------------------------------------
+// Issue the gathers of stream slots b0 .. b0+NB-1 (of n) of the staged ids:
+// lane l loads 16-byte segment l+32r of every vector.  Slots past n load
+// nothing and read as zeros.
+template <int ELEM, int VROWS, int NB>
+__device__ __forceinline__ void gather_batch(const GraphView &g, const int *sids, int b0, int n, int nseg, int lane,
+                                             uint4 (&raw)[NB][VROWS], float (&scale)[NB])
+{
+#pragma unroll
+    for (int t = 0; t < NB; t++) {
+        const bool tv = b0 + t < n;
+        const int id = tv ? sids[b0 + t] : 0;
+        const unsigned char *base = g.vecs + (int64_t)id * g.vstride_bytes;
+        scale[t] = 1.0f;
+        if constexpr (ELEM == kFP8) scale[t] = tv ? g.scales[id] : 1.0f;
+#pragma unroll
+        for (int r = 0; r < VROWS; r++) {
+            const int seg = lane + 32 * r;
+            raw[t][r] = (tv && seg < nseg) ? ld_nc_v4(base + 16 * seg) : make_uint4(0, 0, 0, 0);
+        }
+    }
+}
+
 // Per-query inputs and outputs of search_one_inter.
 struct QueryIO {
     const float *query;             // dim floats
@@ -575,31 +597,17 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                 if (p0) sids[__popc(pm0 & ((1u << lane) - 1u))] = n0;
                 if (p1) sids[PV0 + __popc(pm1 & ((1u << lane) - 1u))] = n1;
                 __syncwarp();
-                bool resolved = false, v0 = false, v1 = false;
-                unsigned vm0 = 0, vm1 = 0;
+                // gathers of batch i+1 are issued as soon as batch i's distances are
+                // formed, so they are in flight while batch i is inserted
+                uint4 raw[NB][VROWS];
+                float scale[NB];
+                if (PV > 0) gather_batch<ELEM, VROWS, NB>(g, sids, 0, PV, nseg, lane, raw, scale);
+                bool v0, v1;
+                bloom_row_resolve(B, lane, v0, v1);   // the atomics overlapped the first gathers
+                const unsigned vm0 = __ballot_sync(kFull, v0), vm1 = __ballot_sync(kFull, v1);
                 for (int b0 = 0; b0 < PV; b0 += NB) {
-                    uint4 raw[NB][VROWS];
-                    float scale[NB];
-#pragma unroll
-                    for (int t = 0; t < NB; t++) {
-                        const bool tv = b0 + t < PV;
-                        const int id = tv ? sids[b0 + t] : 0;
-                        const unsigned char *base = g.vecs + (int64_t)id * g.vstride_bytes;
-                        scale[t] = 1.0f;
-                        if constexpr (ELEM == kFP8) scale[t] = tv ? g.scales[id] : 1.0f;
-#pragma unroll
-                        for (int r = 0; r < VROWS; r++) {
-                            const int seg = lane + 32 * r;
-                            raw[t][r] = (tv && seg < nseg) ? ld_nc_v4(base + 16 * seg) : make_uint4(0, 0, 0, 0);
-                        }
-                    }
-                    if (!resolved) {   // the atomics overlapped the first gathers
-                        bloom_row_resolve(B, lane, v0, v1);
-                        vm0 = __ballot_sync(kFull, v0);
-                        vm1 = __ballot_sync(kFull, v1);
-                        resolved = true;
-                    }
                     const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane);
+                    if (b0 + NB < PV) gather_batch<ELEM, VROWS, NB>(g, sids, b0 + NB, PV, nseg, lane, raw, scale);
                     const int nt = min(NB, PV - b0);
                     // provisional slot b0+t is exact-valid iff its id's lane bit survived
                     bool keep = false;
@@ -629,11 +637,6 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                         }
                     }
                 }
-                if (!resolved) {
-                    bloom_row_resolve(B, lane, v0, v1);
-                    vm0 = __ballot_sync(kFull, v0);
-                    vm1 = __ballot_sync(kFull, v1);
-                }
                 visited += __popc(vm0) + __popc(vm1);
                 __syncwarp();
                 continue;
@@ -648,23 +651,12 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                 visited += V;
                 if (valid) sids[__popc(vm & ((1u << lane) - 1u))] = nb;
                 __syncwarp();
+                uint4 raw[NB][VROWS];
+                float scale[NB];
+                if (V > 0) gather_batch<ELEM, VROWS, NB>(g, sids, 0, V, nseg, lane, raw, scale);
                 for (int b0 = 0; b0 < V; b0 += NB) {
-                    uint4 raw[NB][VROWS];
-                    float scale[NB];
-#pragma unroll
-                    for (int t = 0; t < NB; t++) {
-                        const bool tv = b0 + t < V;
-                        const int id = tv ? sids[b0 + t] : 0;
-                        const unsigned char *base = g.vecs + (int64_t)id * g.vstride_bytes;
-                        scale[t] = 1.0f;
-                        if constexpr (ELEM == kFP8) scale[t] = tv ? g.scales[id] : 1.0f;
-#pragma unroll
-                        for (int r = 0; r < VROWS; r++) {
-                            const int seg = lane + 32 * r;
-                            raw[t][r] = (tv && seg < nseg) ? ld_nc_v4(base + 16 * seg) : make_uint4(0, 0, 0, 0);
-                        }
-                    }
                     const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane);
+                    if (b0 + NB < V) gather_batch<ELEM, VROWS, NB>(g, sids, b0 + NB, V, nseg, lane, raw, scale);
                     const int nt = min(NB, V - b0);
                     // results collection (DRAM_utils.hpp:421-438) in stream order; the
                     // maximum only decreases, so a distance not below it now never will be
@@ -763,7 +755,7 @@ __host__ __device__ __forceinline__ size_t warp_smem_bytes(int bloom_bits_max, i
 }
 
 template <int ELEM, int EPL, int VROWS>
-__global__ void __launch_bounds__(128, 4) inter_kernel(const SearchLaunch A)
+__global__ void __launch_bounds__(128, 3) inter_kernel(const SearchLaunch A)
 {
     extern __shared__ uint4 smem_u4[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
