@@ -129,10 +129,17 @@ __device__ __forceinline__ float seg_tree(const float (&q)[EPS], const float (&x
 // with fewer shuffles.  On return lane l holds the distance of vector l%NB.
 // A pack is 256 leaves; packs are accumulated left to right
 // (compute.hpp:260-267); zero leaves stand for the padding, which is exact.
+//
+// Lane groups: when a vector has at most 16 segments (VROWS == 1) the warp
+// holds 32/G vectors per register row, lanes [gG, gG+G) holding vector g, with
+// G = 2^lg >= NB.  The levels above lane bit lg-1 would only add the zero
+// leaves of the padding (every partial is a sum of squares, >= +0, so x + 0
+// is x exactly), so the tree stops at bit lg-1.  lg = 5 is the plain layout.
+// On return lane l holds the distance of row l%NB of group l>>lg.
 // ---------------------------------------------------------------------------
 template <int ELEM, int VROWS, int NB>
 __device__ __forceinline__ float batch_distances(const float (&q)[VROWS][ET<ELEM>::EPS], const uint4 (&raw)[NB][VROWS],
-                                                 const float (&scale)[NB], int lane)
+                                                 const float (&scale)[NB], int lane, int lg = 5)
 {
     constexpr int EPS = ET<ELEM>::EPS;
     float rowv[VROWS];
@@ -159,10 +166,13 @@ __device__ __forceinline__ float batch_distances(const float (&q)[VROWS][ET<ELEM
         }
         float v = p[0];
         constexpr int kLaneLevels = (ELEM == kFP8) ? 4 : 5;
+        const int top = min(kLaneLevels, lg);
 #pragma unroll
-        for (int lv = level; lv < kLaneLevels; lv++) v = __fadd_rn(v, __shfl_xor_sync(kFull, v, 1 << lv));
+        for (int lv = level; lv < kLaneLevels; lv++)
+            if (lv < top) v = __fadd_rn(v, __shfl_xor_sync(kFull, v, 1 << lv));
         rowv[r] = v;
     }
+    if (VROWS == 1 && lg < 5) return rowv[0];   // one vector per group: the rest of the tree adds zeros
     float dist;
     if constexpr (ELEM == kF32) {
         // one row = 128 leaves = half a pack
@@ -476,26 +486,41 @@ __device__ __forceinline__ void bloom_row_resolve(BloomRow &B, int lane, bool &v
 // ---------------------------------------------------------------------------
 // One query, inter-query semantics (v1.3).
 // ---------------------------------------------------------------------------
-// Issue the gathers of stream slots b0 .. b0+NB-1 (of n) of the staged ids:
-// lane l loads 16-byte segment l+32r of every vector.  Slots past n load
-// nothing and read as zeros.
+// Issue the gathers of stream slots b0 .. b0+(32>>lg)*NB-1 (of n) of the
+// staged ids.  Slot b0 + gNB + t goes to register row t of lane group g (lanes
+// [g<<lg, (g+1)<<lg)), whose lane l loads 16-byte segment (l mod 2^lg)+32r.
+// Slots past n load nothing and read as zeros.
 template <int ELEM, int VROWS, int NB>
 __device__ __forceinline__ void gather_batch(const GraphView &g, const int *sids, int b0, int n, int nseg, int lane,
-                                             uint4 (&raw)[NB][VROWS], float (&scale)[NB])
+                                             int lg, uint4 (&raw)[NB][VROWS], float (&scale)[NB])
 {
+    const int s0 = b0 + (lane >> lg) * NB;
+    const int lseg = lane & ((1 << lg) - 1);
 #pragma unroll
     for (int t = 0; t < NB; t++) {
-        const bool tv = b0 + t < n;
-        const int id = tv ? sids[b0 + t] : 0;
+        const bool tv = s0 + t < n;
+        const int id = tv ? sids[s0 + t] : 0;
         const unsigned char *base = g.vecs + (int64_t)id * g.vstride_bytes;
         scale[t] = 1.0f;
         if constexpr (ELEM == kFP8) scale[t] = tv ? g.scales[id] : 1.0f;
 #pragma unroll
         for (int r = 0; r < VROWS; r++) {
-            const int seg = lane + 32 * r;
+            const int seg = lseg + 32 * r;
             raw[t][r] = (tv && seg < nseg) ? ld_nc_v4(base + 16 * seg) : make_uint4(0, 0, 0, 0);
         }
     }
+}
+
+// Lane-group size (log2) for vectors of nseg 16-byte segments: the smallest
+// power of two >= max(nseg, NB) when one register row holds the vector,
+// otherwise the whole warp.
+template <int VROWS, int NB>
+__device__ __forceinline__ int lane_group_log2(int nseg)
+{
+    if (VROWS > 1) return 5;
+    int lg = 0;
+    while ((1 << lg) < nseg || (1 << lg) < NB) lg++;
+    return lg;
 }
 
 // Per-query inputs and outputs of search_one_inter.
@@ -525,13 +550,20 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
     constexpr int EPS = ET<ELEM>::EPS;
     constexpr int NB = (VROWS == 1) ? 8 : 4;
     const int nseg = g.dpad * ET<ELEM>::BYTES / 16;
+    // lane groups: BS = (32 >> lg) * NB stream slots per gather batch; slot
+    // b0 + s lives in row s mod NB of group s / NB, read back at lane rep(s)
+    const int lg = lane_group_log2<VROWS, NB>(nseg);
+    const int BS = (32 >> lg) * NB;
+    const int gmask = (1 << lg) - 1;
+    const bool rep_lane = (lane & gmask) < NB;              // one lane per slot
+    const int my_slot = (lane >> lg) * NB + (lane & gmask);  // the slot that lane represents
 
     float q[VROWS][EPS];
     {
         const float *Q = io.query;
 #pragma unroll
         for (int r = 0; r < VROWS; r++) {
-            const int seg = lane + 32 * r;
+            const int seg = (lane & gmask) + 32 * r;
 #pragma unroll
             for (int e = 0; e < EPS; e++) {
                 const int j = seg * EPS + e;
@@ -601,28 +633,28 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                 // formed, so they are in flight while batch i is inserted
                 uint4 raw[NB][VROWS];
                 float scale[NB];
-                if (PV > 0) gather_batch<ELEM, VROWS, NB>(g, sids, 0, PV, nseg, lane, raw, scale);
+                if (PV > 0) gather_batch<ELEM, VROWS, NB>(g, sids, 0, PV, nseg, lane, lg, raw, scale);
                 bool v0, v1;
                 bloom_row_resolve(B, lane, v0, v1);   // the atomics overlapped the first gathers
                 const unsigned vm0 = __ballot_sync(kFull, v0), vm1 = __ballot_sync(kFull, v1);
-                for (int b0 = 0; b0 < PV; b0 += NB) {
-                    const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane);
-                    if (b0 + NB < PV) gather_batch<ELEM, VROWS, NB>(g, sids, b0 + NB, PV, nseg, lane, raw, scale);
-                    const int nt = min(NB, PV - b0);
-                    // provisional slot b0+t is exact-valid iff its id's lane bit survived
+                for (int b0 = 0; b0 < PV; b0 += BS) {
+                    const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane, lg);
+                    if (b0 + BS < PV) gather_batch<ELEM, VROWS, NB>(g, sids, b0 + BS, PV, nseg, lane, lg, raw, scale);
+                    const int nt = min(BS, PV - b0);
+                    // provisional slot b0+s is exact-valid iff its id's lane bit survived
                     bool keep = false;
-                    if (lane < nt) {
-                        const int slot = b0 + lane;
+                    if (rep_lane && my_slot < nt) {
+                        const int slot = b0 + my_slot;
                         if (slot < PV0) keep = (vm0 >> __fns(pm0, 0, slot + 1)) & 1u;
                         else keep = (vm1 >> __fns(pm1, 0, slot - PV0 + 1)) & 1u;
                     }
-                    unsigned m = __ballot_sync(kFull, lane < nt && keep && dist < rmax);
-                    while (m) {
+                    unsigned m = __ballot_sync(kFull, keep && dist < rmax);
+                    while (m) {   // representative lanes ascend with the slots
                         const int t = __ffs(m) - 1;
                         m &= m - 1;
                         const float dd = __shfl_sync(kFull, dist, t);
                         if (dd < rmax) {
-                            const int id = sids[b0 + t];
+                            const int id = sids[b0 + (t >> lg) * NB + (t & gmask)];
                             if constexpr (HEAP) {
                                 heap_replace_root(hkey, hid, P.ef, heap_key(dd, ++age), id, lane);
                                 rmax = __uint_as_float((uint32_t)(hkey[0] >> 32));
@@ -653,20 +685,20 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                 __syncwarp();
                 uint4 raw[NB][VROWS];
                 float scale[NB];
-                if (V > 0) gather_batch<ELEM, VROWS, NB>(g, sids, 0, V, nseg, lane, raw, scale);
-                for (int b0 = 0; b0 < V; b0 += NB) {
-                    const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane);
-                    if (b0 + NB < V) gather_batch<ELEM, VROWS, NB>(g, sids, b0 + NB, V, nseg, lane, raw, scale);
-                    const int nt = min(NB, V - b0);
+                if (V > 0) gather_batch<ELEM, VROWS, NB>(g, sids, 0, V, nseg, lane, lg, raw, scale);
+                for (int b0 = 0; b0 < V; b0 += BS) {
+                    const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane, lg);
+                    if (b0 + BS < V) gather_batch<ELEM, VROWS, NB>(g, sids, b0 + BS, V, nseg, lane, lg, raw, scale);
+                    const int nt = min(BS, V - b0);
                     // results collection (DRAM_utils.hpp:421-438) in stream order; the
                     // maximum only decreases, so a distance not below it now never will be
-                    unsigned m = __ballot_sync(kFull, lane < nt && dist < rmax);
-                    while (m) {
+                    unsigned m = __ballot_sync(kFull, rep_lane && my_slot < nt && dist < rmax);
+                    while (m) {   // representative lanes ascend with the slots
                         const int t = __ffs(m) - 1;
                         m &= m - 1;
                         const float dd = __shfl_sync(kFull, dist, t);
                         if (dd < rmax) {
-                            const int id = sids[b0 + t];
+                            const int id = sids[b0 + (t >> lg) * NB + (t & gmask)];
                             if constexpr (HEAP) {
                                 heap_replace_root(hkey, hid, P.ef, heap_key(dd, ++age), id, lane);
                                 rmax = __uint_as_float((uint32_t)(hkey[0] >> 32));
@@ -1213,7 +1245,7 @@ __device__ __forceinline__ long long global_ns()
 // VMAX: FP32 16-byte rows per lane the server's largest dimension needs
 // (ceil(dpad/128)); only the traversal variants up to it are compiled in.
 template <int EPL, int VMAX>
-__global__ void __launch_bounds__(128, 4) serve_kernel(const ServeLaunch S)
+__global__ void __launch_bounds__(128, 3) serve_kernel(const ServeLaunch S)
 {
     extern __shared__ uint4 smem_u4[];
     constexpr int HEAP_CAP = (EPL > 8) ? 32 * EPL : 0;

@@ -48,6 +48,9 @@ CASES = [
     ("unit", 4000, 384, 64, 10, 64, 2, 2, 32, 16),
     ("unit", 4000, 200, 48, 10, 96, 3, 16, 24, 14),
     ("sift", 4000, 50, 20, 5, 33, 1, 5, 31, 13),
+    # vectors of <= 16 segments share a register row with others (lane groups)
+    ("sift", 4000, 32, 32, 10, 128, 2, 2, 32, 15),
+    ("unit", 6000, 64, 64, 10, 600, 1, 2, 128, 20),
     # beyond the reference hardware's ef <= 64 and 32-entry candidate queue
     ("unit", 6000, 96, 64, 10, 512, 1, 2, 64, 16),
     ("unit", 6000, 96, 64, 10, 1024, 2, 4, 256, 17),
@@ -72,19 +75,28 @@ def test_gpu_matches_oracle_f32(oracle_mod, kind, n, dim, md, k, ef, mc, mg, cq,
     assert np.array_equal(r.visited, vis)
 
 
-@pytest.mark.parametrize("prec,dim,rerank", [("bf16", 128, False), ("bf16", 384, True), ("fp8", 96, False),
-                                             ("fp8", 384, True), ("bf16", 96, True)])
-def test_gpu_reduced_precision_matches_oracle(oracle_mod, prec, dim, rerank):
+# (precision, dim, rerank, ef, mc, mg, cand_queue_size, bloom_bits).  Vectors of
+# at most 16 segments are packed several to a register row of the warp
+# (bf16 dim <= 128, fp8 dim <= 256, f32 dim <= 64), larger ones are not.
+RP_CASES = [("bf16", 128, False, 64, 2, 2, 32, 16), ("bf16", 384, True, 64, 2, 2, 32, 16),
+            ("fp8", 96, False, 64, 2, 2, 32, 16), ("fp8", 384, True, 64, 2, 2, 32, 16),
+            ("bf16", 96, True, 64, 2, 2, 32, 16), ("fp8", 32, False, 100, 1, 3, 48, 15),
+            ("bf16", 48, True, 200, 4, 2, 64, 16), ("bf16", 96, True, 1024, 1, 1, 256, 20),
+            ("fp8", 96, True, 512, 2, 2, 128, 19)]
+
+
+@pytest.mark.parametrize("prec,dim,rerank,ef,mc,mg,cq,bits", RP_CASES)
+def test_gpu_reduced_precision_matches_oracle(oracle_mod, prec, dim, rerank, ef, mc, mg, cq, bits):
     g, q = small_graph("unit", 4000, dim, 64, 64, seed=9)
     ix = _index(g, storage=("f32", prec))
-    r = ix.search(q, k=10, ef=64, mc=2, mg=2, precision=prec, rerank=rerank)
+    r = ix.search(q, k=10, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, precision=prec, rerank=rerank)
     if prec == "bf16":
         codes, scales, elem = ix.storage("bf16"), None, oracle_mod.BF16
     else:
         (codes, scales), elem = ix.storage("fp8"), oracle_mod.FP8
     og = oracle_graph(oracle_mod, g, elem=elem, stored=codes, scales=scales)
     ids, d, hops, vis, _ = oracle_mod.search(og, q, g.entry_point, oracle_mod.make_params(
-        k=10, ef=64, mc=2, mg=2, rerank=rerank))
+        k=10, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, rerank=rerank))
     assert _same(r.ids, r.dists, ids, d)
     assert np.array_equal(r.hops, hops) and np.array_equal(r.visited, vis)
 
