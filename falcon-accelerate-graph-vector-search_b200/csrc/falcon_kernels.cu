@@ -62,6 +62,12 @@ __device__ __forceinline__ uint4 ld_nc_v4(const void *p)
     return r;
 }
 
+// Bulk prefetch of a 16-byte aligned range (a multiple of 16 bytes) into L2.
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ int ld_nc_s32(const int32_t *p)
 {
     int r;
@@ -523,6 +529,18 @@ __device__ __forceinline__ int lane_group_log2(int nseg)
     return lg;
 }
 
+// The candidate at the head of the queue is the next one expanded unless a
+// closer one arrives first: its adjacency row goes to L2 when the head changes.
+__device__ __forceinline__ void prefetch_head_row(const GraphView &g, int head_lane0, uint32_t rbytes, int &pf_head,
+                                                  int lane)
+{
+    const int head = __shfl_sync(kFull, head_lane0, 0);
+    if (head != pf_head) {
+        if (lane == 0 && head >= 0 && rbytes) prefetch_l2(g.links + (int64_t)head * g.lstride, rbytes);
+        pf_head = head;
+    }
+}
+
 // Per-query inputs and outputs of search_one_inter.
 struct QueryIO {
     const float *query;             // dim floats
@@ -552,6 +570,10 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
     const int nseg = g.dpad * ET<ELEM>::BYTES / 16;
     // lane groups: BS = (32 >> lg) * NB stream slots per gather batch; slot
     // b0 + s lives in row s mod NB of group s / NB, read back at lane rep(s)
+    const uint32_t vbytes = (uint32_t)nseg * 16u;                       // one stored vector
+    // count word and ids of a row, when rows start on 16-byte boundaries
+    const uint32_t rbytes = (g.lstride % 4 == 0) ? (((uint32_t)(g.ids_off + g.max_degree) * 4u + 15u) & ~15u) : 0u;
+    int pf_head = -1;                                                   // last candidate head prefetched
     const int lg = lane_group_log2<VROWS, NB>(nseg);
     const int BS = (32 >> lg) * NB;
     const int gmask = (1 << lg) - 1;
@@ -628,6 +650,9 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                 const int PV0 = __popc(pm0), PV = PV0 + __popc(pm1);
                 if (p0) sids[__popc(pm0 & ((1u << lane) - 1u))] = n0;
                 if (p1) sids[PV0 + __popc(pm1 & ((1u << lane) - 1u))] = n1;
+                // the row's vectors go to L2 now; the batches below load them from there
+                if (p0) prefetch_l2(g.vecs + (int64_t)n0 * g.vstride_bytes, vbytes);
+                if (p1) prefetch_l2(g.vecs + (int64_t)n1 * g.vstride_bytes, vbytes);
                 __syncwarp();
                 // gathers of batch i+1 are issued as soon as batch i's distances are
                 // formed, so they are in flight while batch i is inserted
@@ -668,6 +693,7 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                             }
                         }
                     }
+                    prefetch_head_row(g, ci[0], rbytes, pf_head, lane);
                 }
                 visited += __popc(vm0) + __popc(vm1);
                 __syncwarp();
@@ -682,6 +708,7 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                 const int V = __popc(vm);
                 visited += V;
                 if (valid) sids[__popc(vm & ((1u << lane) - 1u))] = nb;
+                if (valid) prefetch_l2(g.vecs + (int64_t)nb * g.vstride_bytes, vbytes);
                 __syncwarp();
                 uint4 raw[NB][VROWS];
                 float scale[NB];
@@ -712,6 +739,7 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                             }
                         }
                     }
+                    prefetch_head_row(g, ci[0], rbytes, pf_head, lane);
                 }
                 __syncwarp();
             }
