@@ -228,27 +228,35 @@ __device__ __forceinline__ float batch_distances(const float (&q)[VROWS][ET<ELEM
 // Result list: position p = lane*EPL + e in ascending order; positions >= ef
 // hold evicted entries, which stay above every later insertion because the
 // maximum never increases.
+//
+// Insertion after the entries <= x, decided per entry from local values: an
+// entry <= x stays; an entry > x takes x if its predecessor is <= x (it is the
+// first entry above x), else its predecessor's value.  The predecessor of a
+// lane's first entry is the previous lane's last entry (one shfl_up, which
+// does not depend on x); lane 0's first entry has none.
 // ---------------------------------------------------------------------------
+template <int EPL>
+__device__ __forceinline__ void list_insert(float (&d)[EPL], int (&id)[EPL], int lane, int lim, float x, int xid)
+{
+    float pd = __shfl_up_sync(kFull, d[EPL - 1], 1);
+    const int pi = __shfl_up_sync(kFull, id[EPL - 1], 1);
+    if (lane == 0) pd = -kLarge;
+#pragma unroll
+    for (int e = EPL - 1; e >= 0; e--) {
+        const float prev = (e == 0) ? pd : d[(e > 0) ? e - 1 : 0];
+        const int previ = (e == 0) ? pi : id[(e > 0) ? e - 1 : 0];
+        if (lane * EPL + e < lim && !(d[e] <= x)) {
+            const bool at = prev <= x;
+            d[e] = at ? x : prev;
+            id[e] = at ? xid : previ;
+        }
+    }
+}
+
 template <int EPL>
 __device__ __forceinline__ void rl_insert(float (&d)[EPL], int (&id)[EPL], int lane, float x, int xid)
 {
-    const unsigned full = __ballot_sync(kFull, d[EPL - 1] <= x);   // lanes entirely <= x: a prefix
-    const int f = __popc(full);
-    int c = 0;
-#pragma unroll
-    for (int e = 0; e < EPL; e++) c += (d[e] <= x) ? 1 : 0;
-    const int cf = __shfl_sync(kFull, c, f & 31);
-    const int pos = f * EPL + ((f < 32) ? cf : 0);
-    const float pd = __shfl_up_sync(kFull, d[EPL - 1], 1);
-    const int pi = __shfl_up_sync(kFull, id[EPL - 1], 1);
-#pragma unroll
-    for (int e = EPL - 1; e >= 0; e--) {
-        const int p = lane * EPL + e;
-        const float sd = (e == 0) ? pd : d[(e > 0) ? e - 1 : 0];
-        const int si = (e == 0) ? pi : id[(e > 0) ? e - 1 : 0];
-        if (p > pos) { d[e] = sd; id[e] = si; }
-        else if (p == pos) { d[e] = x; id[e] = xid; }
-    }
+    list_insert<EPL>(d, id, lane, 32 * EPL, x, xid);
 }
 
 // Value at warp-uniform position p of the result list.
@@ -267,25 +275,7 @@ __device__ __forceinline__ float rl_get(const float (&d)[EPL], int p)
 template <int CPL>
 __device__ __forceinline__ void cl_insert(float (&d)[CPL], int (&id)[CPL], int lane, int cq, float x, int xid)
 {
-    const bool lane_le = (lane * CPL + CPL - 1 < cq) && d[CPL - 1] <= x;
-    const int f = __popc(__ballot_sync(kFull, lane_le));
-    int c = 0;
-#pragma unroll
-    for (int e = 0; e < CPL; e++) c += (lane * CPL + e < cq && d[e] <= x) ? 1 : 0;
-    const int cf = __shfl_sync(kFull, c, f & 31);
-    const int pos = f * CPL + ((f < 32) ? cf : 0);
-    const float pd = __shfl_up_sync(kFull, d[CPL - 1], 1);
-    const int pi = __shfl_up_sync(kFull, id[CPL - 1], 1);
-#pragma unroll
-    for (int e = CPL - 1; e >= 0; e--) {
-        const int p = lane * CPL + e;
-        const float sd = (e == 0) ? pd : d[(e > 0) ? e - 1 : 0];
-        const int si = (e == 0) ? pi : id[(e > 0) ? e - 1 : 0];
-        if (p < cq) {
-            if (p > pos) { d[e] = sd; id[e] = si; }
-            else if (p == pos) { d[e] = x; id[e] = xid; }
-        }
-    }
+    list_insert<CPL>(d, id, lane, cq, x, xid);
 }
 
 // pop_top (priority_queue.hpp:131-165): take the best entry, a +large
@@ -309,38 +299,69 @@ __device__ __forceinline__ int cl_pop(float (&d)[CPL], int (&id)[CPL], int lane,
 
 template <int EPL> struct CandPerLane { static constexpr int value = (EPL >= 8) ? EPL / 4 : 1; };
 
-// For ef > 256 the result list is held as a 32-ary max-heap on
-// key = (distance bits, insertion age) in shared memory instead of 32 entries
-// per lane in registers.  The root is the maximum and, among equal maximal
-// distances, the newest entry -- exactly the entry the sorted-list model
-// evicts; a final sort by key gives the list order (ties oldest first).
-// Distances are >= +0, so their bit patterns order like the floats.
+// For ef > 256 the result list is held in shared memory as keys
+// (distance bits, insertion age) instead of 32 entries per lane in registers.
+// Only the maximum matters while searching -- it is the entry the
+// sorted-list model evicts: the largest distance and, among equal distances,
+// the newest -- and a final sort by key gives the list order (ties oldest
+// first).  Distances are >= +0, so their bit patterns order like the floats.
+//
+// The ef slots form 32 buckets of BSZ (= EPL) consecutive slots; lane l keeps
+// bucket l's maximum key and slot in registers and the warp keeps the global
+// maximum.  Replacing the maximum rewrites one slot, re-reduces that bucket
+// (one slot per lane) and then the 32 bucket maxima: a handful of warp
+// reductions instead of a walk down a heap.  Slots at or past ef hold key 0,
+// below every real key (ages start at 1; placeholders carry 1e20).
 __device__ __forceinline__ uint64_t heap_key(float d, uint32_t age)
 {
     return ((uint64_t)__float_as_uint(d) << 32) | age;
 }
 
-__device__ __forceinline__ void heap_replace_root(uint64_t *key, int *id, int n, uint64_t k, int kid, int lane)
+struct BucketMax {
+    uint64_t bmax;      // this lane's bucket maximum
+    int bslot;          // its slot within the bucket
+    uint64_t gmax;      // global maximum (warp-uniform)
+    int gb, gslot;      // its bucket and slot (warp-uniform)
+};
+
+__device__ __forceinline__ void bucket_global(BucketMax &B)
 {
-    int pos = 0;
-    for (;;) {
-        const int c0 = 32 * pos + 1;
-        if (c0 >= n) break;
-        const int c = c0 + lane;
-        const uint64_t ck = (c < n) ? key[c] : 0ull;
-        const uint32_t mhi = __reduce_max_sync(kFull, (uint32_t)(ck >> 32));
-        const uint32_t mlo = __reduce_max_sync(kFull, ((uint32_t)(ck >> 32) == mhi) ? (uint32_t)ck : 0u);
-        const uint64_t mk = ((uint64_t)mhi << 32) | mlo;
-        if (mk <= k) break;
-        const int src = __ffs(__ballot_sync(kFull, c < n && ck == mk)) - 1;
-        const int cidx = c0 + src;
-        const int cid = __shfl_sync(kFull, (c < n) ? id[c] : -1, src);
-        if (lane == 0) { key[pos] = mk; id[pos] = cid; }
-        pos = cidx;
-        __syncwarp();
-    }
-    if (lane == 0) { key[pos] = k; id[pos] = kid; }
+    const uint32_t hi = (uint32_t)(B.bmax >> 32);
+    const uint32_t mhi = __reduce_max_sync(kFull, hi);
+    const uint32_t mlo = __reduce_max_sync(kFull, hi == mhi ? (uint32_t)B.bmax : 0u);
+    B.gmax = ((uint64_t)mhi << 32) | mlo;
+    B.gb = __ffs(__ballot_sync(kFull, B.bmax == B.gmax)) - 1;
+    B.gslot = __shfl_sync(kFull, B.bslot, B.gb);
+}
+
+// ef placeholders (1e20, age 0), slots up to 32*BSZ cleared.
+template <int BSZ>
+__device__ __forceinline__ void bucket_init(BucketMax &B, uint64_t *key, int *id, int ef, int lane)
+{
+    for (int i = lane; i < 32 * BSZ; i += 32) { key[i] = (i < ef) ? heap_key(kLarge, 0u) : 0ull; id[i] = -1; }
+    B.bmax = (BSZ * lane < ef) ? heap_key(kLarge, 0u) : 0ull;
+    B.bslot = 0;
     __syncwarp();
+    bucket_global(B);
+}
+
+// Replace the maximum by k < maximum; returns the new maximum's distance.
+template <int BSZ>
+__device__ __forceinline__ float bucket_replace_max(BucketMax &B, uint64_t *key, int *id, uint64_t k, int kid, int lane)
+{
+    const int slot = BSZ * B.gb + lane;
+    const uint64_t old = (lane < BSZ) ? key[slot] : 0ull;
+    const uint64_t ck = (lane == B.gslot) ? k : old;
+    if (lane == B.gslot) { key[slot] = k; id[slot] = kid; }
+    const uint32_t hi = (uint32_t)(ck >> 32);
+    const uint32_t mhi = __reduce_max_sync(kFull, hi);
+    const uint32_t mlo = __reduce_max_sync(kFull, hi == mhi ? (uint32_t)ck : 0u);
+    const uint64_t mk = ((uint64_t)mhi << 32) | mlo;
+    const int src = __ffs(__ballot_sync(kFull, ck == mk)) - 1;
+    if (lane == B.gb) { B.bmax = mk; B.bslot = src; }
+    bucket_global(B);
+    __syncwarp();
+    return __uint_as_float((uint32_t)(B.gmax >> 32));
 }
 
 // Ascending bitonic sort of the first n2 (a power of two) keys, ids alongside.
@@ -495,7 +516,8 @@ __device__ __forceinline__ void bloom_row_resolve(BloomRow &B, int lane, bool &v
 // Issue the gathers of stream slots b0 .. b0+(32>>lg)*NB-1 (of n) of the
 // staged ids.  Slot b0 + gNB + t goes to register row t of lane group g (lanes
 // [g<<lg, (g+1)<<lg)), whose lane l loads 16-byte segment (l mod 2^lg)+32r.
-// Slots past n load nothing and read as zeros.
+// Slots past n, and slots whose id was withdrawn (stored as ~id < 0), load
+// nothing and read as zeros.
 template <int ELEM, int VROWS, int NB>
 __device__ __forceinline__ void gather_batch(const GraphView &g, const int *sids, int b0, int n, int nseg, int lane,
                                              int lg, uint4 (&raw)[NB][VROWS], float (&scale)[NB])
@@ -504,8 +526,9 @@ __device__ __forceinline__ void gather_batch(const GraphView &g, const int *sids
     const int lseg = lane & ((1 << lg) - 1);
 #pragma unroll
     for (int t = 0; t < NB; t++) {
-        const bool tv = s0 + t < n;
-        const int id = tv ? sids[s0 + t] : 0;
+        const int sid = (s0 + t < n) ? sids[s0 + t] : -1;
+        const bool tv = sid >= 0;
+        const int id = tv ? sid : 0;
         const unsigned char *base = g.vecs + (int64_t)id * g.vstride_bytes;
         scale[t] = 1.0f;
         if constexpr (ELEM == kFP8) scale[t] = tv ? g.scales[id] : 1.0f;
@@ -608,9 +631,8 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
         ri[e] = -1;
     }
     uint32_t age = 0;
-    if constexpr (HEAP) {
-        for (int i = lane; i < P.ef; i += 32) { hkey[i] = heap_key(kLarge, 0u); hid[i] = -1; }
-    }
+    BucketMax BM;
+    if constexpr (HEAP) bucket_init<EPL>(BM, hkey, hid, P.ef, lane);
     constexpr int CPL = CandPerLane<EPL>::value;
     float cd[CPL];
     int ci[CPL];
@@ -648,8 +670,9 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                 // provisional candidates in stream order (first half, then second half)
                 const unsigned pm0 = __ballot_sync(kFull, p0), pm1 = __ballot_sync(kFull, p1);
                 const int PV0 = __popc(pm0), PV = PV0 + __popc(pm1);
-                if (p0) sids[__popc(pm0 & ((1u << lane) - 1u))] = n0;
-                if (p1) sids[PV0 + __popc(pm1 & ((1u << lane) - 1u))] = n1;
+                const int ps0 = __popc(pm0 & ((1u << lane) - 1u)), ps1 = PV0 + __popc(pm1 & ((1u << lane) - 1u));
+                if (p0) sids[ps0] = n0;
+                if (p1) sids[ps1] = n1;
                 // the row's vectors go to L2 now; the batches below load them from there
                 if (p0) prefetch_l2(g.vecs + (int64_t)n0 * g.vstride_bytes, vbytes);
                 if (p1) prefetch_l2(g.vecs + (int64_t)n1 * g.vstride_bytes, vbytes);
@@ -662,17 +685,15 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                 bool v0, v1;
                 bloom_row_resolve(B, lane, v0, v1);   // the atomics overlapped the first gathers
                 const unsigned vm0 = __ballot_sync(kFull, v0), vm1 = __ballot_sync(kFull, v1);
+                // a provisional id that turned out seen is withdrawn from the stream
+                if (p0 && !v0) sids[ps0] = ~n0;
+                if (p1 && !v1) sids[ps1] = ~n1;
+                __syncwarp();
                 for (int b0 = 0; b0 < PV; b0 += BS) {
                     const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane, lg);
                     if (b0 + BS < PV) gather_batch<ELEM, VROWS, NB>(g, sids, b0 + BS, PV, nseg, lane, lg, raw, scale);
                     const int nt = min(BS, PV - b0);
-                    // provisional slot b0+s is exact-valid iff its id's lane bit survived
-                    bool keep = false;
-                    if (rep_lane && my_slot < nt) {
-                        const int slot = b0 + my_slot;
-                        if (slot < PV0) keep = (vm0 >> __fns(pm0, 0, slot + 1)) & 1u;
-                        else keep = (vm1 >> __fns(pm1, 0, slot - PV0 + 1)) & 1u;
-                    }
+                    const bool keep = rep_lane && my_slot < nt && sids[b0 + my_slot] >= 0;
                     unsigned m = __ballot_sync(kFull, keep && dist < rmax);
                     while (m) {   // representative lanes ascend with the slots
                         const int t = __ffs(m) - 1;
@@ -681,8 +702,7 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                         if (dd < rmax) {
                             const int id = sids[b0 + (t >> lg) * NB + (t & gmask)];
                             if constexpr (HEAP) {
-                                heap_replace_root(hkey, hid, P.ef, heap_key(dd, ++age), id, lane);
-                                rmax = __uint_as_float((uint32_t)(hkey[0] >> 32));
+                                rmax = bucket_replace_max<EPL>(BM, hkey, hid, heap_key(dd, ++age), id, lane);
                             } else {
                                 rl_insert<EPL>(rd, ri, lane, dd, id);
                                 rmax = rl_get<EPL>(rd, P.ef - 1);
@@ -727,8 +747,7 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                         if (dd < rmax) {
                             const int id = sids[b0 + (t >> lg) * NB + (t & gmask)];
                             if constexpr (HEAP) {
-                                heap_replace_root(hkey, hid, P.ef, heap_key(dd, ++age), id, lane);
-                                rmax = __uint_as_float((uint32_t)(hkey[0] >> 32));
+                                rmax = bucket_replace_max<EPL>(BM, hkey, hid, heap_key(dd, ++age), id, lane);
                             } else {
                                 rl_insert<EPL>(rd, ri, lane, dd, id);
                                 rmax = rl_get<EPL>(rd, P.ef - 1);
@@ -949,9 +968,9 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
             ri[e] = -1;
         }
         uint32_t age = 0;
+        BucketMax BM;
         if constexpr (HEAP) {
-            if (warp == 0)
-                for (int i = lane; i < P.ef; i += 32) { hkey[i] = heap_key(kLarge, 0u); hid[i] = -1; }
+            if (warp == 0) bucket_init<EPL>(BM, hkey, hid, P.ef, lane);
         }
         constexpr int CPL = CandPerLane<EPL>::value;
         float cd[CPL];
@@ -1060,8 +1079,7 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
                             if (dd < rmax) {
                                 const int id = list_id[o + j0 + t];
                                 if constexpr (HEAP) {
-                                    heap_replace_root(hkey, hid, P.ef, heap_key(dd, ++age), id, lane);
-                                    rmax = __uint_as_float((uint32_t)(hkey[0] >> 32));
+                                    rmax = bucket_replace_max<EPL>(BM, hkey, hid, heap_key(dd, ++age), id, lane);
                                 } else {
                                     rl_insert<EPL>(rd, ri, lane, dd, id);
                                     rmax = rl_get<EPL>(rd, P.ef - 1);
