@@ -62,10 +62,12 @@ __device__ __forceinline__ uint4 ld_nc_v4(const void *p)
     return r;
 }
 
-// Bulk prefetch of a 16-byte aligned range (a multiple of 16 bytes) into L2.
+// Prefetch the 128-byte lines of [p, p + bytes) into L2 (one instruction per
+// line from this lane; cheaper to issue than a bulk prefetch per range).
 __device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes)
 {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+    const char *c = reinterpret_cast<const char *>(p);
+    for (uint32_t o = 0; o < bytes; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(c + o) : "memory");
 }
 
 __device__ __forceinline__ int ld_nc_s32(const int32_t *p)
@@ -594,8 +596,7 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
     // lane groups: BS = (32 >> lg) * NB stream slots per gather batch; slot
     // b0 + s lives in row s mod NB of group s / NB, read back at lane rep(s)
     const uint32_t vbytes = (uint32_t)nseg * 16u;                       // one stored vector
-    // count word and ids of a row, when rows start on 16-byte boundaries
-    const uint32_t rbytes = (g.lstride % 4 == 0) ? (((uint32_t)(g.ids_off + g.max_degree) * 4u + 15u) & ~15u) : 0u;
+    const uint32_t rbytes = (uint32_t)(g.ids_off + g.max_degree) * 4u;  // count word and ids of a row
     int pf_head = -1;                                                   // last candidate head prefetched
     const int lg = lane_group_log2<VROWS, NB>(nseg);
     const int BS = (32 >> lg) * NB;
@@ -890,8 +891,6 @@ __global__ void __launch_bounds__(128, 3) inter_kernel(const SearchLaunch A)
 struct IntraSmem {
     unsigned long long qi;
     int inflight, head, hops, truncated, done;
-    int chan_cnt[kMaxChannels];
-    int chan_off[kMaxChannels + 1];
     int chan_valid[kMaxChannels];
     int chan_visited[kMaxChannels];
 };
@@ -917,11 +916,13 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
     uint32_t *bloom = smem_bloom ? reinterpret_cast<uint32_t *>(base_ptr + off + bloom_bytes * warp)
                                  : A.bloom_global + ((size_t)blockIdx.x * C + warp) * (bloom_bytes / 4);
     if (smem_bloom) off += bloom_bytes * C;
+    // channel c's ids (then its surviving ids and distances) of the current
+    // group: lcap slots at c * lcap
     const int lcap = A.mc_max * g.max_degree;
     int *list_id = reinterpret_cast<int *>(base_ptr + off);
-    off += sizeof(int) * (size_t)lcap;
+    off += sizeof(int) * (size_t)lcap * C;
     float *list_d = reinterpret_cast<float *>(base_ptr + off);
-    off += sizeof(float) * (size_t)lcap;
+    off += sizeof(float) * (size_t)lcap * C;
     int *fifo = reinterpret_cast<int *>(base_ptr + off);
     off += sizeof(int) * (size_t)(A.mc_max * A.mg_max);
     int *fifo_len = reinterpret_cast<int *>(base_ptr + off);
@@ -931,6 +932,15 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
     off = (off + 15) & ~(size_t)15;
     uint64_t *hkey = reinterpret_cast<uint64_t *>(base_ptr + off);
     int *hid = reinterpret_cast<int *>(base_ptr + off + sizeof(uint64_t) * HEAP_CAP);
+    // lane groups and gather batches as in search_one_inter
+    const uint32_t vbytes = (uint32_t)nseg * 16u;
+    const int lg = lane_group_log2<VROWS, NB>(nseg);
+    const int BS = (32 >> lg) * NB;
+    const int gmask = (1 << lg) - 1;
+    const bool rep_lane = (lane & gmask) < NB;
+    const int my_slot = (lane >> lg) * NB + (lane & gmask);
+    int *my_ids = list_id + (size_t)lcap * warp;
+    float *my_d = list_d + (size_t)lcap * warp;
 
     for (;;) {
         if (threadIdx.x == 0) S->qi = atomicAdd(reinterpret_cast<unsigned long long *>(A.work_counter), 1ull);
@@ -944,7 +954,7 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
             const float *Q = A.queries + qi * A.qstride;
 #pragma unroll
             for (int r = 0; r < VROWS; r++) {
-                const int seg = lane + 32 * r;
+                const int seg = (lane & gmask) + 32 * r;
 #pragma unroll
                 for (int e = 0; e < EPS; e++) {
                     const int j = seg * EPS + e;
@@ -997,32 +1007,17 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
         while (S->inflight > 0) {
             const int head = S->head;
             const int glen = fifo_len[head];
-            // 1. route: count, then place this channel's ids in stream order
+            // 1. route: this channel's ids of the group's rows, in stream order
             int count = 0;
             for (int b = 0; b < glen; b++) {
                 const int32_t *row = g.links + (int64_t)fifo[head * mc + b] * g.lstride;
-                const int cnt = row[0];
+                const int cnt = ld_nc_s32(row);
                 for (int c0 = 0; c0 < cnt; c0 += 32) {
-                    const int nb = (c0 + lane < cnt) ? row[g.ids_off + c0 + lane] : -1;
-                    count += __popc(__ballot_sync(kFull, nb >= 0 && (nb & (C - 1)) == warp));
-                }
-            }
-            if (lane == 0) S->chan_cnt[warp] = count;
-            __syncthreads();
-            int my_off = 0;
-            for (int c = 0; c < warp; c++) my_off += S->chan_cnt[c];
-            {
-                int w = my_off;
-                for (int b = 0; b < glen; b++) {
-                    const int32_t *row = g.links + (int64_t)fifo[head * mc + b] * g.lstride;
-                    const int cnt = row[0];
-                    for (int c0 = 0; c0 < cnt; c0 += 32) {
-                        const int nb = (c0 + lane < cnt) ? row[g.ids_off + c0 + lane] : -1;
-                        const bool mine = nb >= 0 && (nb & (C - 1)) == warp;
-                        const unsigned mm = __ballot_sync(kFull, mine);
-                        if (mine) list_id[w + __popc(mm & ((1u << lane) - 1u))] = nb;
-                        w += __popc(mm);
-                    }
+                    const int nb = (c0 + lane < cnt) ? ld_nc_s32(row + g.ids_off + c0 + lane) : -1;
+                    const bool mine = nb >= 0 && (nb & (C - 1)) == warp;
+                    const unsigned mm = __ballot_sync(kFull, mine);
+                    if (mine) my_ids[count + __popc(mm & ((1u << lane) - 1u))] = nb;
+                    count += __popc(mm);
                 }
             }
             __syncwarp();
@@ -1030,34 +1025,23 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
             int nvalid = 0;
             for (int c0 = 0; c0 < count; c0 += 32) {
                 const bool act = c0 + lane < count;
-                const int nb = act ? list_id[my_off + c0 + lane] : -1;
+                const int nb = act ? my_ids[c0 + lane] : -1;
                 const bool valid = bloom_chunk(bloom, bmask, P.seed, nb, act, lane);
                 const unsigned vm = __ballot_sync(kFull, valid);
                 const int V = __popc(vm);
                 visited += V;
                 if (valid) sids[__popc(vm & ((1u << lane) - 1u))] = nb;
+                if (valid) prefetch_l2(g.vecs + (int64_t)nb * g.vstride_bytes, vbytes);
                 __syncwarp();
-                for (int b0 = 0; b0 < V; b0 += NB) {
-                    uint4 raw[NB][VROWS];
-                    float scale[NB];
-#pragma unroll
-                    for (int t = 0; t < NB; t++) {
-                        const bool tv = b0 + t < V;
-                        const int id = tv ? sids[b0 + t] : 0;
-                        const unsigned char *vb = g.vecs + (int64_t)id * g.vstride_bytes;
-                        scale[t] = 1.0f;
-                        if constexpr (ELEM == kFP8) scale[t] = tv ? g.scales[id] : 1.0f;
-#pragma unroll
-                        for (int r = 0; r < VROWS; r++) {
-                            const int seg = lane + 32 * r;
-                            raw[t][r] = (tv && seg < nseg) ? ld_nc_v4(vb + 16 * seg) : make_uint4(0, 0, 0, 0);
-                        }
-                    }
-                    const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane);
-                    const int nt = min(NB, V - b0);
-                    if (lane < nt) {
-                        list_id[my_off + nvalid + b0 + lane] = sids[b0 + lane];
-                        list_d[my_off + nvalid + b0 + lane] = dist;
+                uint4 raw[NB][VROWS];
+                float scale[NB];
+                if (V > 0) gather_batch<ELEM, VROWS, NB>(g, sids, 0, V, nseg, lane, lg, raw, scale);
+                for (int b0 = 0; b0 < V; b0 += BS) {
+                    const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane, lg);
+                    if (b0 + BS < V) gather_batch<ELEM, VROWS, NB>(g, sids, b0 + BS, V, nseg, lane, lg, raw, scale);
+                    if (rep_lane && b0 + my_slot < V) {
+                        my_ids[nvalid + b0 + my_slot] = sids[b0 + my_slot];
+                        my_d[nvalid + b0 + my_slot] = dist;
                     }
                 }
                 nvalid += V;
@@ -1067,7 +1051,8 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
             __syncthreads();
             // 3. warp 0 merges channels in order and runs the scheduler
             if (warp == 0) {
-                for (int c = 0, o = 0; c < C; o += S->chan_cnt[c], c++) {
+                for (int c = 0; c < C; c++) {
+                    const int o = c * lcap;
                     const int nv = S->chan_valid[c];
                     for (int j0 = 0; j0 < nv; j0 += 32) {
                         const float dl = (j0 + lane < nv) ? list_d[o + j0 + lane] : kLarge;
@@ -1172,7 +1157,7 @@ size_t intra_smem_bytes(const SearchLaunch &a, int channels, int heap_cap)
 {
     size_t b = (sizeof(IntraSmem) + 15) & ~(size_t)15;
     if (a.bloom_bits_max <= kMaxSmemBloomBits) b += ((size_t)1 << (a.bloom_bits_max - 3)) * channels;
-    b += 2 * sizeof(int) * (size_t)a.mc_max * a.g.max_degree;
+    b += 2 * sizeof(int) * (size_t)a.mc_max * a.g.max_degree * channels;
     b += sizeof(int) * (size_t)(a.mc_max * a.mg_max + a.mg_max);
     b += sizeof(int) * 32 * channels;
     b = (b + 15) & ~(size_t)15;
