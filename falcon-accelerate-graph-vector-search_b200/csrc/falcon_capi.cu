@@ -29,6 +29,12 @@ struct falcon_index {
     int32_t *d_links = nullptr;    // n x link_stride
     int32_t *d_labels = nullptr;   // n or null
     int64_t device_bytes = 0;
+    // HNSW upper layers (falcon_index_set_upper_layers); max_level 0 = none
+    int32_t *d_upper_rows = nullptr;
+    int64_t *d_upper_start = nullptr;
+    int32_t *d_upper_levels = nullptr;
+    int64_t upper_stride = 0;
+    int upper_max_level = 0, upper_max_degree = 0, upper_entry = 0;
 };
 
 namespace {
@@ -72,6 +78,37 @@ struct DeviceGuard {
 
 int pad16(int d) { return (d + 15) / 16 * 16; }
 
+void free_upper(falcon_index *ix)
+{
+    cudaFree(ix->d_upper_rows);
+    cudaFree(ix->d_upper_start);
+    cudaFree(ix->d_upper_levels);
+    ix->d_upper_rows = nullptr; ix->d_upper_start = nullptr; ix->d_upper_levels = nullptr;
+    ix->upper_max_level = 0;
+}
+
+// Device view of the upper layers and the FP32 vectors for the descent.
+DescendLaunch descend_launch(const falcon_index *ix)
+{
+    DescendLaunch a;
+    memset(&a, 0, sizeof(a));
+    a.g.vecs = reinterpret_cast<const unsigned char *>(ix->d_f32);
+    a.g.vstride_bytes = (int64_t)ix->dpad * 4;
+    a.g.vecs32 = a.g.vecs;
+    a.g.vstride32_bytes = a.g.vstride_bytes;
+    a.g.dim = ix->dim;
+    a.g.dpad = ix->dpad;
+    a.g.n = ix->n;
+    a.u.rows = ix->d_upper_rows;
+    a.u.stride = ix->upper_stride;
+    a.u.row_start = ix->d_upper_start;
+    a.u.levels = ix->d_upper_levels;
+    a.u.max_level = ix->upper_max_level;
+    a.u.max_degree = ix->upper_max_degree;
+    a.u.entry = ix->upper_entry;
+    return a;
+}
+
 void free_index_buffers(falcon_index *ix)
 {
     cudaFree(ix->d_f32);
@@ -82,6 +119,7 @@ void free_index_buffers(falcon_index *ix)
     cudaFree(ix->d_labels);
     ix->d_f32 = nullptr; ix->d_bf16 = nullptr; ix->d_fp8 = nullptr;
     ix->d_scales = nullptr; ix->d_links = nullptr; ix->d_labels = nullptr;
+    free_upper(ix);
 }
 
 // Host-side validation of the adjacency rows: count in [0, max_degree], ids in [0, n).
@@ -354,6 +392,123 @@ int falcon_index_load_fpga(const char *index_dir, const char *graph_type, int32_
     return falcon_index_create(&d, out);
 }
 
+int falcon_index_set_upper_layers(falcon_index *ix, const falcon_upper_layers_desc *d)
+{
+    if (!ix || !d || !d->levels || !d->row_start || (d->num_rows > 0 && !d->rows))
+        return set_error(FALCON_ERR_ARG, "null argument");
+    if (d->max_level < 1 || d->max_degree < 1 || d->max_degree > kMaxDegree || d->ids_offset < 1 ||
+        d->row_stride < d->ids_offset + d->max_degree || d->num_rows < 0)
+        return set_error(FALCON_ERR_ARG, "bad upper-layer shape (max_level=%d, max_degree=%d, ids_offset=%d, "
+                         "row_stride=%lld)", d->max_level, d->max_degree, d->ids_offset, (long long)d->row_stride);
+    const int64_t n = ix->n;
+    if (d->entry_point < 0 || d->entry_point >= n || d->levels[d->entry_point] != d->max_level)
+        return set_error(FALCON_ERR_GRAPH, "upper-layer entry point %d is not on level %d", d->entry_point,
+                         d->max_level);
+    for (int64_t v = 0; v < n; v++) {
+        const int lv = d->levels[v];
+        if (lv < 0 || lv > d->max_level)
+            return set_error(FALCON_ERR_GRAPH, "node %lld: level %d outside [0, %d]", (long long)v, lv, d->max_level);
+        if (lv == 0) continue;
+        const int64_t r0 = d->row_start[v];
+        if (r0 < 0 || r0 + lv > d->num_rows)
+            return set_error(FALCON_ERR_GRAPH, "node %lld: rows [%lld, %lld) outside %lld rows", (long long)v,
+                             (long long)r0, (long long)(r0 + lv), (long long)d->num_rows);
+        for (int l = 1; l <= lv; l++) {
+            const int32_t *row = d->rows + (r0 + l - 1) * d->row_stride;
+            const int c = row[0];
+            if (c < 0 || c > d->max_degree)
+                return set_error(FALCON_ERR_GRAPH, "node %lld level %d: count %d outside [0, %d]", (long long)v, l, c,
+                                 d->max_degree);
+            for (int j = 0; j < c; j++) {
+                const int32_t u = row[d->ids_offset + j];
+                if (u < 0 || u >= n || d->levels[u] < l)
+                    return set_error(FALCON_ERR_GRAPH, "node %lld level %d: neighbour %d is not on that level",
+                                     (long long)v, l, u);
+            }
+        }
+    }
+    // device layout: rows of 16 * (1 + ceil(max_degree / 16)) int32, count at 0, ids at 16; rows of a node consecutive
+    const int64_t stride = 16LL * (1 + (d->max_degree + 15) / 16);
+    std::vector<int64_t> start((size_t)n, 0);
+    int64_t nrows = 0;
+    for (int64_t v = 0; v < n; v++) {
+        start[(size_t)v] = nrows;
+        nrows += d->levels[v];
+    }
+    std::vector<int32_t> rows((size_t)(nrows > 0 ? nrows : 1) * stride, 0);
+    for (int64_t v = 0; v < n; v++)
+        for (int l = 1; l <= d->levels[v]; l++) {
+            const int32_t *src = d->rows + (d->row_start[v] + l - 1) * d->row_stride;
+            int32_t *dst = rows.data() + (start[(size_t)v] + l - 1) * stride;
+            dst[0] = src[0];
+            for (int j = 0; j < src[0]; j++) dst[16 + j] = src[d->ids_offset + j];
+        }
+    DeviceGuard guard(ix->device);
+    if (!guard.ok) return set_error(FALCON_ERR_CUDA, "cannot select device %d", ix->device);
+    free_upper(ix);
+    int rc = FALCON_OK;
+    cudaStream_t s = nullptr;
+    FALCON_CUDA(cudaMalloc((void **)&ix->d_upper_rows, rows.size() * sizeof(int32_t)));
+    FALCON_CUDA(cudaMalloc((void **)&ix->d_upper_start, (size_t)n * sizeof(int64_t)));
+    FALCON_CUDA(cudaMalloc((void **)&ix->d_upper_levels, (size_t)n * sizeof(int32_t)));
+    FALCON_CUDA(cudaMemcpyAsync(ix->d_upper_rows, rows.data(), rows.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    FALCON_CUDA(cudaMemcpyAsync(ix->d_upper_start, start.data(), (size_t)n * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    FALCON_CUDA(cudaMemcpyAsync(ix->d_upper_levels, d->levels, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    FALCON_CUDA(cudaStreamSynchronize(s));
+    ix->upper_stride = stride;
+    ix->upper_max_level = d->max_level;
+    ix->upper_max_degree = d->max_degree;
+    ix->upper_entry = d->entry_point;
+done:
+    if (rc != FALCON_OK) free_upper(ix);
+    return rc;
+}
+
+int falcon_descend(falcon_index *ix, const float *queries, int64_t nq, int64_t query_stride,
+                   int32_t *out_entry_points, int32_t *out_upper_hops, int32_t memory, void *stream_v)
+{
+    if (!ix || !out_entry_points || (nq > 0 && !queries)) return set_error(FALCON_ERR_ARG, "null argument");
+    if (query_stride < ix->dim) return set_error(FALCON_ERR_ARG, "query_stride %lld < dim %d", (long long)query_stride, ix->dim);
+    if (memory != FALCON_MEM_HOST && memory != FALCON_MEM_DEVICE) return set_error(FALCON_ERR_ARG, "bad memory flag");
+    if (ix->upper_max_level < 1) return set_error(FALCON_ERR_ARG, "the index has no upper layers");
+    if (!ix->d_f32) return set_error(FALCON_ERR_UNSUPPORTED, "the descent needs FP32 storage");
+    if (nq < 0) return set_error(FALCON_ERR_ARG, "nq < 0");
+    if (nq == 0) return FALCON_OK;
+    DeviceGuard guard(ix->device);
+    if (!guard.ok) return set_error(FALCON_ERR_CUDA, "cannot select device %d", ix->device);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream_v);
+    const bool host = memory == FALCON_MEM_HOST;
+    int rc = FALCON_OK;
+    float *d_q = nullptr;
+    int32_t *d_e = nullptr, *d_h = nullptr;
+    DescendLaunch a = descend_launch(ix);
+    if (host) {
+        FALCON_CUDA(cudaMallocAsync((void **)&d_q, (size_t)nq * query_stride * sizeof(float), s));
+        FALCON_CUDA(cudaMemcpyAsync(d_q, queries, (size_t)nq * query_stride * sizeof(float), cudaMemcpyHostToDevice, s));
+        FALCON_CUDA(cudaMallocAsync((void **)&d_e, (size_t)nq * sizeof(int32_t), s));
+        if (out_upper_hops) FALCON_CUDA(cudaMallocAsync((void **)&d_h, (size_t)nq * sizeof(int32_t), s));
+    }
+    a.queries = host ? d_q : queries;
+    a.qstride = query_stride;
+    a.nq = nq;
+    a.out_entry = host ? d_e : out_entry_points;
+    a.out_hops = host ? d_h : out_upper_hops;
+    FALCON_CUDA(launch_descend(a, ix->num_sms, s));
+    if (host) {
+        FALCON_CUDA(cudaMemcpyAsync(out_entry_points, d_e, (size_t)nq * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        if (out_upper_hops)
+            FALCON_CUDA(cudaMemcpyAsync(out_upper_hops, d_h, (size_t)nq * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    }
+done:
+    for (void *p : {(void *)d_q, (void *)d_e, (void *)d_h})
+        if (p) cudaFreeAsync(p, s);
+    if (rc == FALCON_OK && host) {
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return set_error(FALCON_ERR_CUDA, "descend: %s", cudaGetErrorString(e));
+    }
+    return rc;
+}
+
 int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t query_stride,
                   const int32_t *entry_points, const falcon_search_params *params, int32_t per_query_params,
                   int32_t *out_ids, float *out_dists, int32_t out_stride, int32_t *out_hops, int32_t *out_visited,
@@ -496,6 +651,17 @@ int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t qu
             FALCON_CUDA(cudaMallocAsync((void **)&d_bloom, (size_t)slots << (bits_max - 3), s));
             a.bloom_global = d_bloom;
         }
+        if (!entry_points && ix->upper_max_level > 0) {   // entries from the upper-layer descent
+            if (!ix->d_f32) { rc = set_error(FALCON_ERR_UNSUPPORTED, "the upper-layer descent needs FP32 storage"); goto done; }
+            FALCON_CUDA(cudaMallocAsync((void **)&d_entries, nq * sizeof(int32_t), s));
+            DescendLaunch dl = descend_launch(ix);
+            dl.queries = a.queries;
+            dl.qstride = query_stride;
+            dl.nq = nq;
+            dl.out_entry = d_entries;
+            FALCON_CUDA(launch_descend(dl, ix->num_sms, s));
+            a.entries = d_entries;
+        }
         FALCON_CUDA(launch_search(a, elem, ix->num_sms, s));
         if (any_rerank) {
             RerankLaunch r;
@@ -630,6 +796,7 @@ int index_graph_view(const falcon_index *ix, int precision, GraphView *v, int *d
 }
 
 int index_device(const falcon_index *ix) { return ix->device; }
+bool index_has_upper(const falcon_index *ix) { return ix->upper_max_level > 0; }
 
 // Validates a no-allocation request; needs ef >= k in every struct so the
 // caller's structs can be copied to the device unchanged (the kernels'
@@ -692,7 +859,7 @@ int prepare_search(const falcon_index *ix, int64_t nq, const falcon_search_param
 int run_search_plan(const falcon_index *ix, const SearchPlan &plan, int64_t nq, const float *queries,
                     int64_t query_stride, const int32_t *entry_points, QParams *d_params, int32_t *d_scratch,
                     int32_t *d_cand_ids, float *d_cand_d, int32_t *out_ids, float *out_dists, int32_t out_stride,
-                    int32_t *out_hops, int32_t *out_visited, cudaStream_t s)
+                    int32_t *out_hops, int32_t *out_visited, int32_t *d_entry_scratch, cudaStream_t s)
 {
     if (query_stride < ix->dim)
         return set_error(FALCON_ERR_ARG, "query_stride %lld < dim %d", (long long)query_stride, ix->dim);
@@ -740,7 +907,20 @@ int run_search_plan(const falcon_index *ix, const SearchPlan &plan, int64_t nq, 
     a.channels = plan.channels;
     a.cq_max = plan.cq_max;
     const int elem = plan.prec == FALCON_PREC_BF16 ? kBF16 : (plan.prec == FALCON_PREC_FP8 ? kFP8 : kF32);
-    cudaError_t e = launch_search(a, elem, ix->num_sms, s);
+    cudaError_t e;
+    if (!entry_points && ix->upper_max_level > 0) {   // entries from the upper-layer descent
+        if (!ix->d_f32 || !d_entry_scratch)
+            return set_error(FALCON_ERR_UNSUPPORTED, "the upper-layer descent needs FP32 storage and entry scratch");
+        DescendLaunch dl = descend_launch(ix);
+        dl.queries = queries;
+        dl.qstride = query_stride;
+        dl.nq = nq;
+        dl.out_entry = d_entry_scratch;
+        e = launch_descend(dl, ix->num_sms, s);
+        if (e != cudaSuccess) return set_error(FALCON_ERR_CUDA, "descend launch: %s", cudaGetErrorString(e));
+        a.entries = d_entry_scratch;
+    }
+    e = launch_search(a, elem, ix->num_sms, s);
     if (e != cudaSuccess) return set_error(FALCON_ERR_CUDA, "search launch: %s", cudaGetErrorString(e));
     if (plan.any_rerank) {
         RerankLaunch r;

@@ -41,6 +41,30 @@ struct GraphView {
     const int32_t *labels;          // may be null
 };
 
+// HNSW upper layers on the device: node v's level-l row (1 <= l <= levels[v])
+// is rows + (row_start[v] + l - 1) * stride, count at [0], ids from [16].
+struct UpperView {
+    const int32_t *rows;
+    int64_t stride;                 // int32 per row (16 * (1 + ceil(max_degree / 16)))
+    const int64_t *row_start;       // per node
+    const int32_t *levels;          // per node (0 = base layer only)
+    int32_t max_level;              // top level (>= 1)
+    int32_t max_degree;             // ids per upper row
+    int32_t entry;                  // top-level entry node
+};
+
+// Greedy descent of the upper layers for nq queries: the base-layer entry of
+// each query (and the number of upper rows expanded).
+struct DescendLaunch {
+    GraphView g;                    // FP32 vectors (vecs = vecs32)
+    UpperView u;
+    const float *queries;
+    int64_t qstride;
+    int64_t nq;
+    int32_t *out_entry;
+    int32_t *out_hops;              // may be null
+};
+
 // Per-query search parameters as the kernels read them.
 struct QParams {
     int32_t k, ef, mc, mg, cq, bloom_bits;
@@ -161,6 +185,7 @@ cudaError_t launch_encode_bf16(const float *src, int64_t src_stride, int64_t n, 
                                cudaStream_t s);
 cudaError_t launch_encode_fp8(const float *src, int64_t src_stride, int64_t n, int dim, int dpad, uint8_t *dst,
                               float *scales, cudaStream_t s);
+cudaError_t launch_descend(const DescendLaunch &a, int num_sms, cudaStream_t s);
 // Number of kernel launches the last launch_search issued (for accounting).
 int search_kernel_count();
 

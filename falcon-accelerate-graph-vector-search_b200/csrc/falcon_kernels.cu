@@ -1166,6 +1166,99 @@ size_t intra_smem_bytes(const SearchLaunch &a, int channels, int heap_cap)
 }
 
 // ---------------------------------------------------------------------------
+// HNSW upper-layer greedy descent (hnswalg.h:514-541 of the reference's
+// vendored hnswlib; the FPGA multi-layer scheduler, FPGA_single_DDR/
+// FPGA_single_DDR_multi_layer_v2.2_async/src/scheduler.hpp:116-144): from the
+// top entry, at every level from the top down to 1, expand the current node's
+// row and move to a neighbour whenever its distance is strictly below the
+// current one, scanning the row in order, until a row brings no improvement.
+// The result of one row scan is the first neighbour with the smallest
+// distance, if that is below the current distance.  No visited filter; FP32
+// distances in the adder-tree order of the base-layer search.  One warp per
+// query; its row's ids are staged in shared memory.
+// ---------------------------------------------------------------------------
+template <int VROWS>
+__global__ void __launch_bounds__(128) descend_kernel(const DescendLaunch A)
+{
+    __shared__ int s_ids[4][kMaxDegree];
+    constexpr int NB = (VROWS == 1) ? 8 : 4;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int *sids = s_ids[warp];
+    const GraphView &g = A.g;
+    const UpperView &u = A.u;
+    const int nseg = g.dpad * 4 / 16;
+    const int lg = lane_group_log2<VROWS, NB>(nseg);
+    const int BS = (32 >> lg) * NB;
+    const int gmask = (1 << lg) - 1;
+    const bool rep_lane = (lane & gmask) < NB;
+    const int my_slot = (lane >> lg) * NB + (lane & gmask);
+    const int64_t nwarps = (int64_t)gridDim.x * 4;
+    for (int64_t qi = (int64_t)blockIdx.x * 4 + warp; qi < A.nq; qi += nwarps) {
+        float q[VROWS][4];
+        const float *Q = A.queries + qi * A.qstride;
+#pragma unroll
+        for (int r = 0; r < VROWS; r++) {
+            const int seg = (lane & gmask) + 32 * r;
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int j = seg * 4 + e;
+                q[r][e] = (seg < nseg && j < g.dim) ? __ldg(Q + j) : 0.0f;
+            }
+        }
+        int cur = u.entry, hops = 0;
+        float curd;
+        {   // distance to the top entry
+            if (lane == 0) sids[0] = cur;
+            __syncwarp();
+            uint4 raw[NB][VROWS];
+            float scale[NB];
+            gather_batch<kF32, VROWS, NB>(g, sids, 0, 1, nseg, lane, lg, raw, scale);
+            curd = __shfl_sync(kFull, batch_distances<kF32, VROWS, NB>(q, raw, scale, lane, lg), 0);
+            __syncwarp();
+        }
+        for (int level = u.max_level; level > 0; level--) {
+            for (;;) {
+                int cnt = 0;
+                const int32_t *row = nullptr;
+                if (__ldg(u.levels + cur) >= level) {
+                    row = u.rows + (__ldg(u.row_start + cur) + level - 1) * u.stride;
+                    cnt = __ldg(row);
+                }
+                hops++;
+                for (int i = lane; i < cnt; i += 32) sids[i] = __ldg(row + 16 + i);
+                __syncwarp();
+                float bestd = curd;
+                int best = -1;   // first slot with the smallest distance below curd
+                uint4 raw[NB][VROWS];
+                float scale[NB];
+                if (cnt > 0) gather_batch<kF32, VROWS, NB>(g, sids, 0, cnt, nseg, lane, lg, raw, scale);
+                for (int b0 = 0; b0 < cnt; b0 += BS) {
+                    const float dist = batch_distances<kF32, VROWS, NB>(q, raw, scale, lane, lg);
+                    if (b0 + BS < cnt) gather_batch<kF32, VROWS, NB>(g, sids, b0 + BS, cnt, nseg, lane, lg, raw, scale);
+                    const bool in = rep_lane && b0 + my_slot < cnt;
+                    // distances are >= +0: their bit patterns order like the floats
+                    const uint32_t mb = __reduce_min_sync(kFull, in ? __float_as_uint(dist) : 0xffffffffu);
+                    const float md = __uint_as_float(mb);
+                    if (md < bestd) {   // strictly better than every earlier slot
+                        const unsigned at = __ballot_sync(kFull, in && __float_as_uint(dist) == mb);
+                        const int t = __ffs(at) - 1;   // representative lanes ascend with the slots
+                        bestd = md;
+                        best = b0 + (t >> lg) * NB + (t & gmask);
+                    }
+                }
+                if (best >= 0) { cur = sids[best]; curd = bestd; }
+                __syncwarp();
+                if (best < 0) break;
+            }
+        }
+        if (lane == 0) {
+            A.out_entry[qi] = cur;
+            if (A.out_hops) A.out_hops[qi] = hops;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Exact FP32 rerank of the final ef candidates of a reduced-precision
 // traversal (extension beyond the reference): one warp per query, the same
 // adder tree on the FP32 vectors, stable ascending order (ties keep the
@@ -1523,6 +1616,23 @@ static cudaError_t search_dispatch(const SearchLaunch &a, int elem, int num_sms,
         if (vrows == 1) return dispatch_epl<kFP8, 1>(a, smem_block, num_sms, s, slots);
     }
     return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_descend(const DescendLaunch &a, int num_sms, cudaStream_t s)
+{
+    if (a.nq <= 0) return cudaSuccess;
+    const int vrows = (a.g.dpad * 4 / 16 + 31) / 32;
+    int64_t blocks = (a.nq + 3) / 4;
+    const int64_t cap = (int64_t)num_sms * 8;
+    if (blocks > cap) blocks = cap;
+    switch (vrows) {
+        case 1: descend_kernel<1><<<(unsigned)blocks, 128, 0, s>>>(a); break;
+        case 2: descend_kernel<2><<<(unsigned)blocks, 128, 0, s>>>(a); break;
+        case 3: descend_kernel<3><<<(unsigned)blocks, 128, 0, s>>>(a); break;
+        case 4: descend_kernel<4><<<(unsigned)blocks, 128, 0, s>>>(a); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_search(const SearchLaunch &a, int elem, int num_sms, cudaStream_t s)

@@ -20,8 +20,10 @@
 //    scratch array, so every struct must have ef >= k.
 //  - The scratch needed by one call is 256 bytes of header, plus 48 bytes per
 //    parameter struct, plus 8 * nq * ef_max bytes when a reduced-precision
-//    search asks for the FP32 rerank; a call needing more than 4 MiB is
-//    rejected with FALCON_ERR_ARG before any device work.
+//    search asks for the FP32 rerank, plus 4 * nq bytes for the upper-layer
+//    descent's entries when the index has HNSW upper layers and no entry
+//    points are given; a call needing more than 4 MiB is rejected with
+//    FALCON_ERR_ARG before any device work.
 //  - The first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (with that device current) and caches it; make that
 //    first call before any stream capture.
@@ -85,9 +87,10 @@ int prepare_search(const falcon_index *ix, int64_t nq, const falcon_search_param
 int run_search_plan(const falcon_index *ix, const SearchPlan &plan, int64_t nq, const float *queries,
                     int64_t query_stride, const int32_t *entry_points, QParams *d_params, int32_t *d_scratch,
                     int32_t *d_cand_ids, float *d_cand_d, int32_t *out_ids, float *out_dists, int32_t out_stride,
-                    int32_t *out_hops, int32_t *out_visited, cudaStream_t s);
+                    int32_t *out_hops, int32_t *out_visited, int32_t *d_entry_scratch, cudaStream_t s);
 int set_error_code(int code, const char *msg);
 int index_device(const falcon_index *ix);
+bool index_has_upper(const falcon_index *ix);
 }  // namespace falcon
 
 extern "C" int falcon_search_noalloc(falcon_index *ix, const float *queries, int64_t nq, int64_t query_stride,
@@ -105,11 +108,14 @@ extern "C" int falcon_search_noalloc(falcon_index *ix, const float *queries, int
     const size_t param_off = kHeaderBytes;
     const size_t cand_off = (param_off + param_bytes + 255) & ~(size_t)255;
     const size_t cand_bytes = plan.any_rerank ? (size_t)nq * plan.ef_max * (sizeof(int32_t) + sizeof(float)) : 0;
-    if (cand_off + cand_bytes > kNoAllocScratchBytes)
+    // per-query entries of the upper-layer descent, when the index has upper layers and none are given
+    const size_t entry_off = (cand_off + cand_bytes + 255) & ~(size_t)255;
+    const size_t entry_bytes = (!entry_points && index_has_upper(ix)) ? (size_t)nq * sizeof(int32_t) : 0;
+    if (entry_off + entry_bytes > kNoAllocScratchBytes)
         return set_error_code(FALCON_ERR_ARG,
                               "falcon_search_noalloc: this call needs more than the 4 MiB static scratch "
-                              "(48 B per parameter struct + 8 B per query per ef with rerank); "
-                              "split the batch or use falcon_search");
+                              "(48 B per parameter struct + 8 B per query per ef with rerank + 4 B per query "
+                              "for upper-layer entries); split the batch or use falcon_search");
     const int device = index_device(ix);
     int prev = -1;
     if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
@@ -130,13 +136,14 @@ extern "C" int falcon_search_noalloc(falcon_index *ix, const float *queries, int
         d_cand_ids = reinterpret_cast<int32_t *>(base + cand_off);
         d_cand_d = reinterpret_cast<float *>(base + cand_off + (size_t)nq * plan.ef_max * sizeof(int32_t));
     }
+    int32_t *d_entry = entry_bytes ? reinterpret_cast<int32_t *>(base + entry_off) : nullptr;
     rc = FALCON_OK;
     if (cudaMemsetAsync(d_header, 0, 16, s) != cudaSuccess ||
         cudaMemcpyAsync(d_params, params, param_bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
         rc = set_error_code(FALCON_ERR_CUDA, "falcon_search_noalloc: scratch initialisation failed");
     if (rc == FALCON_OK)
         rc = run_search_plan(ix, plan, nq, queries, query_stride, entry_points, d_params, d_header, d_cand_ids,
-                             d_cand_d, out_ids, out_dists, out_stride, out_hops, out_visited, s);
+                             d_cand_d, out_ids, out_dists, out_stride, out_hops, out_visited, d_entry, s);
     if (prev >= 0) cudaSetDevice(prev);
     return rc;
 }

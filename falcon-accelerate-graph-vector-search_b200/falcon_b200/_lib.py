@@ -60,6 +60,20 @@ class IndexInfo(ctypes.Structure):
     ]
 
 
+class UpperLayersDesc(ctypes.Structure):
+    _fields_ = [
+        ("max_level", ctypes.c_int32),
+        ("max_degree", ctypes.c_int32),
+        ("entry_point", ctypes.c_int32),
+        ("ids_offset", ctypes.c_int32),
+        ("num_rows", ctypes.c_int64),
+        ("row_stride", ctypes.c_int64),
+        ("levels", ctypes.c_void_p),
+        ("row_start", ctypes.c_void_p),
+        ("rows", ctypes.c_void_p),
+    ]
+
+
 class SearchParams(ctypes.Structure):
     _fields_ = [
         ("k", ctypes.c_int32),
@@ -109,6 +123,8 @@ SIGNATURES = {
     "falcon_index_info_get": (_I32, [_VP, ctypes.POINTER(IndexInfo)]),
     "falcon_index_free": (_I32, [_VP]),
     "falcon_index_copy_storage": (_I32, [_VP, _I32, _VP, _I64]),
+    "falcon_index_set_upper_layers": (_I32, [_VP, ctypes.POINTER(UpperLayersDesc)]),
+    "falcon_descend": (_I32, [_VP, _VP, _I64, _I64, _VP, _VP, _I32, _VP]),
     "falcon_search": (_I32, [_VP, _VP, _I64, _I64, _VP, ctypes.POINTER(SearchParams), _I32,
                              _VP, _VP, _I32, _VP, _VP, _I32, _VP]),
     "falcon_search_noalloc": (_I32, [_VP, _VP, _I64, _I64, _VP, ctypes.POINTER(SearchParams), _I32,

@@ -70,13 +70,17 @@ class Graph:
 # Reference FPGA index files (hnsw.py:264-377 / nsg_to_FPGA.py:56-137)
 # ---------------------------------------------------------------------------
 
-def write_fpga_index(out_dir, graph, graph_type="HNSW", max_level=0, max_m=None):
+def write_fpga_index(out_dir, graph, graph_type="HNSW", max_level=0, max_m=None, upper=None):
     """Write meta.bin, ground_links_1_chan_0.bin, ground_vectors_1_chan_0.bin
-    and ground_labels.bin in the reference layout (single channel)."""
+    and ground_labels.bin in the reference layout (single channel), and with
+    `upper` (HNSW) also upper_links.bin and upper_links_pointers.bin."""
     os.makedirs(out_dir, exist_ok=True)
     n, md, dim = graph.n, graph.max_degree, graph.dim
+    if upper is not None:
+        max_level, max_m = upper.max_level, upper.max_degree
     if graph_type == "HNSW":
-        meta = np.array([n, max_level, graph.entry_point, max_m if max_m else md // 2, md], dtype=np.int32)
+        entry = upper.entry if upper is not None else graph.entry_point
+        meta = np.array([n, max_level, entry, max_m if max_m else md // 2, md], dtype=np.int32)
     elif graph_type == "NSG":
         meta = np.array([n, graph.entry_point, md], dtype=np.int32)
     else:
@@ -93,6 +97,8 @@ def write_fpga_index(out_dir, graph, graph_type="HNSW", max_level=0, max_m=None)
     vec.tofile(os.path.join(out_dir, "ground_vectors_1_chan_0.bin"))
     labels = graph.labels if graph.labels is not None else np.arange(n, dtype=np.int32)
     labels.astype(np.int32).tofile(os.path.join(out_dir, "ground_labels.bin"))
+    if upper is not None:
+        write_fpga_upper(out_dir, upper)
 
 
 def read_fpga_index(index_dir, graph_type, dim):
@@ -116,3 +122,190 @@ def reference_vector_rows(vectors):
     out[:, :dim] = vectors
     out[:, pad16(dim)] = np.frombuffer(np.int32(-1).tobytes(), dtype=np.float32)[0]
     return out
+
+
+# ---------------------------------------------------------------------------
+# HNSW upper layers
+# ---------------------------------------------------------------------------
+
+class UpperLayers:
+    """HNSW levels >= 1 in hnswlib's arrangement: node v is on levels
+    0..levels[v]; for 1 <= l <= levels[v] its level-l list is row
+    row_start[v] + l - 1 of `rows` ([num_rows, 1 + max_degree] int32: the
+    count, then the ids; hnswalg.h:379-381, size_links_per_element_)."""
+
+    def __init__(self, max_level, max_degree, entry, levels, row_start, rows):
+        self.max_level = int(max_level)
+        self.max_degree = int(max_degree)
+        self.entry = int(entry)
+        self.levels = np.ascontiguousarray(levels, dtype=np.int32)
+        self.row_start = np.ascontiguousarray(row_start, dtype=np.int64)
+        self.rows = np.ascontiguousarray(rows, dtype=np.int32).reshape(-1, 1 + self.max_degree)
+
+    def row(self, v, level):
+        """Neighbour ids of node v on `level` (>= 1)."""
+        r = self.rows[self.row_start[v] + level - 1]
+        return r[1:1 + r[0]].copy()
+
+    @classmethod
+    def from_lists(cls, max_degree, entry, lists):
+        """lists[v] = [ids on level 1, ids on level 2, ...] (empty for base-only nodes)."""
+        n = len(lists)
+        levels = np.array([len(x) for x in lists], dtype=np.int32)
+        row_start = np.zeros(n, dtype=np.int64)
+        row_start[1:] = np.cumsum(levels)[:-1]
+        rows = np.zeros((max(int(levels.sum()), 1), 1 + max_degree), dtype=np.int32)
+        for v, per_level in enumerate(lists):
+            for l, ids in enumerate(per_level):
+                r = rows[row_start[v] + l]
+                r[0] = len(ids)
+                r[1:1 + len(ids)] = ids
+        return cls(int(levels.max()) if n else 0, max_degree, entry, levels, row_start, rows)
+
+
+# hnswlib save files (hnswalg.h:588-616 of the reference's vendored hnswlib;
+# hnsw.py:139-262 reads the same layout): a 96-byte header, then per element
+# (in internal-id order) the level-0 record [count u32 (low 16 bits), maxM0 ids
+# u32, dim floats, label u64], then per element [bytes u32, levels x (count u32,
+# maxM ids u32)].
+_HNSW_HEADER = np.dtype([("offsetLevel0", "<u8"), ("max_elements", "<u8"), ("cur_element_count", "<u8"),
+                         ("size_data_per_element", "<u8"), ("label_offset", "<u8"), ("offsetData", "<u8"),
+                         ("maxlevel", "<i4"), ("enterpoint_node", "<u4"), ("maxM", "<u8"), ("maxM0", "<u8"),
+                         ("M", "<u8"), ("mult", "<f8"), ("ef_construction", "<u8")])
+
+
+def read_hnswlib_index(path):
+    """Read an hnswlib save file.  Returns (Graph of the base layer with the
+    file's labels, UpperLayers or None when the index has one level, header
+    dict)."""
+    raw = np.fromfile(path, dtype=np.uint8)
+    hdr = np.frombuffer(raw[:_HNSW_HEADER.itemsize].tobytes(), dtype=_HNSW_HEADER)[0]
+    n = int(hdr["cur_element_count"])
+    size = int(hdr["size_data_per_element"])
+    m0, m = int(hdr["maxM0"]), int(hdr["maxM"])
+    off_data, off_label = int(hdr["offsetData"]), int(hdr["label_offset"])
+    if int(hdr["offsetLevel0"]) != 0 or off_data != 4 + 4 * m0:
+        raise ValueError("unsupported hnswlib layout (offsetLevel0=%d, offsetData=%d)" % (hdr["offsetLevel0"], off_data))
+    dim = (off_label - off_data) // 4
+    pos = _HNSW_HEADER.itemsize
+    rec = raw[pos:pos + n * size].reshape(n, size)
+    pos += n * size
+    counts = rec[:, 0:4].copy().view("<u4")[:, 0] & 0xffff
+    ids = rec[:, 4:off_data].copy().view("<u4").astype(np.int64)
+    vectors = rec[:, off_data:off_label].copy().view("<f4")
+    labels = rec[:, off_label:off_label + 8].copy().view("<u8")[:, 0]
+    adj = np.where(np.arange(m0)[None, :] < counts[:, None], ids, -1).astype(np.int32)
+    levels = np.zeros(n, dtype=np.int32)
+    row_start = np.zeros(n, dtype=np.int64)
+    chunks = []
+    row_bytes = 4 * (1 + m)
+    nrows = 0
+    for v in range(n):
+        nb = int(np.frombuffer(raw[pos:pos + 4].tobytes(), dtype="<u4")[0])
+        pos += 4
+        row_start[v] = nrows
+        if nb:
+            lv = nb // row_bytes
+            levels[v] = lv
+            block = raw[pos:pos + nb].copy().view("<u4").reshape(lv, 1 + m).astype(np.int64)
+            block[:, 0] &= 0xffff
+            # slots past the count may hold stale ids: clear them
+            block[:, 1:][np.arange(m)[None, :] >= block[:, :1]] = 0
+            chunks.append(block.astype(np.int32))
+            nrows += lv
+            pos += nb
+    if pos != raw.size:
+        raise ValueError("trailing bytes in %s" % path)
+    entry = int(hdr["enterpoint_node"])
+    g = Graph.from_adjacency(vectors, adj, entry, labels=labels.astype(np.int32))
+    upper = None
+    if int(hdr["maxlevel"]) > 0:
+        rows = np.concatenate(chunks) if chunks else np.zeros((1, 1 + m), dtype=np.int32)
+        upper = UpperLayers(int(hdr["maxlevel"]), m, entry, levels, row_start, rows)
+    info = {k: (float(hdr[k]) if k == "mult" else int(hdr[k])) for k in _HNSW_HEADER.names}
+    info["dim"] = dim
+    return g, upper, info
+
+
+def write_hnswlib_index(path, graph, upper, M, ef_construction=200, labels=None):
+    """Write `graph` (base layer, max_degree = maxM0) and `upper` (or None) as
+    an hnswlib save file that hnswlib's loadIndex reads."""
+    n, dim, m0 = graph.n, graph.dim, graph.max_degree
+    m = upper.max_degree if upper is not None else M
+    size = 4 + 4 * m0 + 4 * dim + 8
+    hdr = np.zeros(1, dtype=_HNSW_HEADER)
+    hdr["offsetLevel0"], hdr["max_elements"], hdr["cur_element_count"] = 0, n, n
+    hdr["size_data_per_element"], hdr["label_offset"], hdr["offsetData"] = size, 4 + 4 * m0 + 4 * dim, 4 + 4 * m0
+    hdr["maxlevel"] = upper.max_level if upper is not None else 0
+    hdr["enterpoint_node"] = upper.entry if upper is not None else graph.entry_point
+    hdr["maxM"], hdr["maxM0"], hdr["M"] = m, m0, M
+    hdr["mult"] = 1.0 / np.log(float(M))
+    hdr["ef_construction"] = ef_construction
+    rec = np.zeros((n, size), dtype=np.uint8)
+    adj = graph.adjacency()
+    rec[:, 0:4] = graph.counts().astype("<u4").view(np.uint8).reshape(n, 4)
+    rec[:, 4:4 + 4 * m0] = np.where(adj >= 0, adj, 0).astype("<u4").view(np.uint8).reshape(n, 4 * m0)
+    rec[:, 4 + 4 * m0:4 + 4 * m0 + 4 * dim] = graph.vectors.astype("<f4").view(np.uint8).reshape(n, 4 * dim)
+    lab = labels if labels is not None else (graph.labels if graph.labels is not None else np.arange(n))
+    rec[:, size - 8:] = np.asarray(lab, dtype="<u8").view(np.uint8).reshape(n, 8)
+    with open(path, "wb") as f:
+        f.write(hdr.tobytes())
+        f.write(rec.tobytes())
+        for v in range(n):
+            lv = int(upper.levels[v]) if upper is not None else 0
+            f.write(np.uint32(lv * 4 * (1 + m)).tobytes())
+            if lv:
+                f.write(upper.rows[upper.row_start[v]:upper.row_start[v] + lv].astype("<u4").tobytes())
+
+
+# Reference multi-layer FPGA files (hnsw.py:264-377; read by FPGA_single_DDR/
+# FPGA_single_DDR_multi_layer_v2.2_async/src/host.cpp:66-161): upper_links.bin
+# holds, per node and level, a 64-byte header line (count + 60 bytes of zeros)
+# and then maxM ids padded to 64 bytes; upper_links_pointers.bin holds one
+# 8-byte byte offset per node.
+
+def _fpga_upper_row_words(max_m):
+    return 16 * (1 + (4 * max_m + 63) // 64)
+
+
+def write_fpga_upper(out_dir, upper):
+    n = upper.levels.shape[0]
+    rw = _fpga_upper_row_words(upper.max_degree)
+    ptr = np.zeros(n, dtype="<u8")
+    blocks = []
+    off = 0
+    for v in range(n):
+        ptr[v] = off
+        for l in range(1, int(upper.levels[v]) + 1):
+            r = upper.rows[upper.row_start[v] + l - 1]
+            row = np.zeros(rw, dtype="<u4")
+            row[0] = r[0]
+            row[16:16 + upper.max_degree] = np.where(np.arange(upper.max_degree) < r[0], r[1:], 0)
+            blocks.append(row)
+            off += 4 * rw
+    data = np.concatenate(blocks) if blocks else np.zeros(0, dtype="<u4")
+    data.tofile(os.path.join(out_dir, "upper_links.bin"))
+    ptr.tofile(os.path.join(out_dir, "upper_links_pointers.bin"))
+
+
+def read_fpga_upper(index_dir):
+    """UpperLayers from meta.bin (n, max_level, entry, maxM, maxM0) and the
+    upper-link files, or None when max_level is 0 or the files are absent."""
+    meta = np.fromfile(os.path.join(index_dir, "meta.bin"), dtype=np.int32)
+    n, max_level, entry, max_m = int(meta[0]), int(meta[1]), int(meta[2]), int(meta[3])
+    lp, pp = os.path.join(index_dir, "upper_links.bin"), os.path.join(index_dir, "upper_links_pointers.bin")
+    if max_level < 1 or not (os.path.exists(lp) and os.path.exists(pp)):
+        return None
+    rw = _fpga_upper_row_words(max_m)
+    data = np.fromfile(lp, dtype="<u4").reshape(-1, rw).astype(np.int64)
+    ptr = np.fromfile(pp, dtype="<u8").astype(np.int64)
+    if ptr.shape[0] != n:
+        raise ValueError("upper_links_pointers.bin holds %d pointers for %d nodes" % (ptr.shape[0], n))
+    ends = np.append(ptr[1:], data.shape[0] * 4 * rw)
+    levels = ((ends - ptr) // (4 * rw)).astype(np.int32)
+    row_start = (ptr // (4 * rw)).astype(np.int64)
+    rows = np.zeros((max(data.shape[0], 1), 1 + max_m), dtype=np.int32)
+    if data.shape[0]:
+        rows[:data.shape[0], 0] = data[:, 0]
+        rows[:data.shape[0], 1:] = data[:, 16:16 + max_m]
+    return UpperLayers(max_level, max_m, entry, levels, row_start, rows)

@@ -121,3 +121,38 @@ def build_graph(vectors, max_degree, knn_k=None, device=None, batch=2048, verbos
     entry = int(torch.argmin(((x - mean) ** 2).sum(1)).item())
     adj = out.to(torch.int32).cpu().numpy()
     return Graph.from_adjacency(xs, adj, entry)
+
+
+def build_upper_layers(vectors, M, seed=0, device=None):
+    """HNSW upper layers for a base graph over `vectors`: node levels drawn as
+    hnswlib draws them (floor(-ln U * mult), mult = 1/ln M; hnswalg.h:148-153,
+    here from a seeded numpy generator), and on every level l >= 1 a graph of
+    max degree M over the nodes with level >= l, built like the base layer
+    (k nearest neighbours, hnswlib's heuristic, reverse edges).  The entry is
+    the medoid of the top level.  Returns formats.UpperLayers."""
+    from .formats import UpperLayers
+    xs = np.ascontiguousarray(vectors, dtype=np.float32)
+    n = xs.shape[0]
+    rng = np.random.default_rng(seed)
+    mult = 1.0 / np.log(float(M))
+    u = rng.random(n)
+    levels = np.floor(-np.log(np.maximum(u, 1e-300)) * mult).astype(np.int32)
+    max_level = int(levels.max())
+    if max_level < 1:   # make sure there is one upper level with one node
+        levels[int(rng.integers(0, n))] = 1
+        max_level = 1
+    lists = [[] for _ in range(n)]
+    entry = -1
+    for lvl in range(1, max_level + 1):
+        nodes = np.nonzero(levels >= lvl)[0]
+        if nodes.size == 1:
+            lists[int(nodes[0])].append(np.zeros(0, dtype=np.int32))
+            entry = int(nodes[0])
+            continue
+        sub = build_graph(xs[nodes], min(M, nodes.size - 1), device=device)
+        adj = sub.adjacency()
+        for j, v in enumerate(nodes):
+            row = adj[j]
+            lists[int(v)].append(nodes[row[row >= 0]].astype(np.int32))
+        entry = int(nodes[sub.entry_point])
+    return UpperLayers.from_lists(M, entry, lists)

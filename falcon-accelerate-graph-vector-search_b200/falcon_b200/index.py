@@ -113,6 +113,39 @@ class FalconIndex:
             return out[:n * dp].reshape(n, dp), out[n * dp:].view(np.float32).copy()
         return out
 
+    def set_upper_layers(self, upper):
+        """Attach HNSW upper layers (formats.UpperLayers); afterwards searches
+        without entry points start from the greedy descent's entry."""
+        rows = np.ascontiguousarray(upper.rows, dtype=np.int32)
+        levels = np.ascontiguousarray(upper.levels, dtype=np.int32)
+        starts = np.ascontiguousarray(upper.row_start, dtype=np.int64)
+        d = _lib.UpperLayersDesc()
+        d.max_level, d.max_degree, d.entry_point, d.ids_offset = upper.max_level, upper.max_degree, upper.entry, 1
+        d.num_rows, d.row_stride = rows.shape[0], rows.shape[1]
+        d.levels, d.row_start, d.rows = levels.ctypes.data, starts.ctypes.data, rows.ctypes.data
+        _lib.check(_lib.load().falcon_index_set_upper_layers(self._h, ctypes.byref(d)))
+
+    def descend(self, queries, stream=None):
+        """Base-layer entry point per query from the upper-layer descent, and
+        the number of upper rows expanded: (entries, hops), numpy for host
+        queries, torch for device queries."""
+        lib = _lib.load()
+        if _is_torch_cuda(queries):
+            import torch
+            q = queries.contiguous().float()
+            ent = torch.empty(q.shape[0], dtype=torch.int32, device=q.device)
+            hops = torch.empty(q.shape[0], dtype=torch.int32, device=q.device)
+            s = stream if stream is not None else torch.cuda.current_stream(q.device).cuda_stream
+            _lib.check(lib.falcon_descend(self._h, q.data_ptr(), q.shape[0], q.stride(0), ent.data_ptr(),
+                                          hops.data_ptr(), _lib.MEM_DEVICE, ctypes.c_void_p(s)))
+            return ent, hops
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        ent = np.empty(q.shape[0], dtype=np.int32)
+        hops = np.empty(q.shape[0], dtype=np.int32)
+        _lib.check(lib.falcon_descend(self._h, q.ctypes.data, q.shape[0], q.shape[1], ent.ctypes.data,
+                                      hops.ctypes.data, _lib.MEM_HOST, stream))
+        return ent, hops
+
     def close(self):
         if getattr(self, "_h", None):
             _lib.load().falcon_index_free(self._h)

@@ -138,12 +138,57 @@ int falcon_index_copy_storage(const falcon_index *ix, int32_t which, void *dst, 
 int falcon_index_free(falcon_index *ix);
 
 /*
+ * HNSW upper layers (levels >= 1) for an index whose graph is an HNSW base
+ * layer, in hnswlib's own arrangement (hnswalg.h:371-384, 588-616 of the
+ * reference's vendored hnswlib; hnsw.py:230-262): node v lives on levels
+ * 0..levels[v]; for 1 <= l <= levels[v] its level-l list is row
+ * row_start[v] + l - 1 of `rows`, a row being row_stride int32: the count at
+ * [0], the ids at [ids_offset ..].  Host arrays; copied to the device.
+ * Replaces the reference multi-layer FPGA inputs meta.bin (max_level, entry),
+ * upper_links.bin and upper_links_pointers.bin (FPGA_single_DDR/
+ * FPGA_single_DDR_multi_layer_v2.2_async/src/host.cpp:66-161,
+ * vadd.cpp ptr_to_upper_links/links_upper).
+ *   max_level:   hnswlib maxlevel_ (>= 1)
+ *   max_degree:  hnswlib maxM_ (ids per upper row, <= 128)
+ *   entry_point: hnswlib enterpoint_node_ (a node with levels[v] == max_level)
+ * Every id on level l must itself be on level l.  Errors: FALCON_ERR_GRAPH.
+ */
+typedef struct falcon_upper_layers_desc {
+    int32_t max_level;
+    int32_t max_degree;
+    int32_t entry_point;
+    int32_t ids_offset;
+    int64_t num_rows;
+    int64_t row_stride;
+    const int32_t *levels;          /* num_vectors */
+    const int64_t *row_start;       /* num_vectors (ignored where levels[v] == 0) */
+    const int32_t *rows;            /* num_rows x row_stride */
+} falcon_upper_layers_desc;
+
+int falcon_index_set_upper_layers(falcon_index *ix, const falcon_upper_layers_desc *desc);
+
+/*
+ * Greedy descent of the upper layers (hnswalg.h:514-541; the multi-layer
+ * scheduler FPGA_single_DDR_multi_layer_v2.2_async/src/scheduler.hpp:116-144):
+ * for each query, the base-layer entry point (mem_debug[2q] of the
+ * multi-layer kernel) and the number of upper rows expanded.  FP32 distances
+ * in the base search's order; requires FP32 storage and upper layers.
+ * falcon_search and falcon_search_noalloc run this descent themselves when
+ * the index has upper layers and entry_points is NULL.
+ * memory as for falcon_search.
+ */
+int falcon_descend(falcon_index *ix, const float *queries, int64_t nq, int64_t query_stride,
+                   int32_t *out_entry_points, int32_t *out_upper_hops, int32_t memory, void *stream);
+
+/*
  * Search nq queries.  Replaces the kernel launch + result migration of the
  * reference host (host.cpp:852-993, vadd.cpp:11-95).
  *   queries:      nq rows of `dim` floats, row stride query_stride floats
- *   entry_points: per-query entry ids, or NULL for the index entry point
- *                 (the reference sets every query to the global entry,
- *                 host.cpp:711-713)
+ *   entry_points: per-query entry ids, or NULL: the upper-layer descent's
+ *                 entry when the index has HNSW upper layers
+ *                 (falcon_index_set_upper_layers), else the index entry
+ *                 point (the reference's multi-DDR host sets every query to
+ *                 the global entry, host.cpp:711-713)
  *   params:       one falcon_search_params, or nq of them when
  *                 per_query_params != 0 (mixed k/ef/mc in one launch)
  *   out_ids/out_dists: nq rows of out_stride (>= every k); the first k of a
@@ -174,8 +219,8 @@ int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t qu
  * a device pointer on the index's device and `params` are host structs, each
  * with ef >= k.  Scratch lives in one static 4 MiB device array per GPU (held
  * until the process exits); a call needing more (256 B + 48 B per params
- * struct + 8 B x nq x ef_max for a reduced-precision search with rerank) fails
- * with FALCON_ERR_ARG.  The first call on a device looks the array up with
+ * struct + 8 B x nq x ef_max for a reduced-precision search with rerank
+ * + 4 B x nq for upper-layer entries) fails with FALCON_ERR_ARG.  The first call on a device looks the array up with
  * cudaGetSymbolAddress and should come before any stream capture.  All calls
  * share the array: calls whose kernels overlap on the GPU race and must be
  * serialised by the caller.  Nothing is allocated by this call.

@@ -541,3 +541,62 @@ void fo_l2_batch(const fo_graph *g, const float *query, const int32_t *ids, int 
     for (int i = 0; i < n; i++) out[i] = dist_to(g, qpad, ids[i], scratch);
     free(qpad); free(scratch);
 }
+
+/* -------------------------------------------------------------------------- */
+/* HNSW upper-layer greedy descent (hnswalg.h:514-541 of the vendored hnswlib; */
+/* FPGA_single_DDR/FPGA_single_DDR_multi_layer_v2.2_async/src/                  */
+/* scheduler.hpp:116-144).  From the top entry, for level = max_level .. 1:     */
+/* repeat { scan the current node's level row in order, moving to every       */
+/* neighbour whose distance is strictly below the current one } until a scan  */
+/* moves nowhere.  No visited filter.  Distances use the same adder-tree order */
+/* as the base search (the FPGA computes upper and base distances in the same */
+/* compute units).  The v2.2 scheduler starts one level lower (max_level - 1) */
+/* because its indexes keep only the entry point on the top level, whose row  */
+/* is then empty: both starts give the same entry there.                      */
+/* -------------------------------------------------------------------------- */
+typedef struct {
+    const int32_t *rows;      /* row r at rows + r * row_stride: count, ids from ids_offset */
+    int64_t row_stride;
+    int ids_offset;
+    const int64_t *row_start; /* node v's level-l row is row_start[v] + l - 1 */
+    const int32_t *levels;    /* per node */
+    int max_level;
+    int entry;
+} fo_upper;
+
+int fo_descend(const fo_graph *g, const fo_upper *u, const float *queries, int64_t nq, int64_t qstride,
+               int32_t *out_entry, int32_t *out_hops)
+{
+    float *qpad = malloc(sizeof(float) * g->dpad), *scratch = malloc(sizeof(float) * g->dpad);
+    if (!qpad || !scratch) { free(qpad); free(scratch); return -1; }
+    for (int64_t qi = 0; qi < nq; qi++) {
+        const float *q = queries + qi * qstride;
+        for (int j = 0; j < g->dpad; j++) qpad[j] = (j < g->dim) ? q[j] : 0.0f;
+        int cur = u->entry, hops = 0;
+        float curdist = dist_to(g, qpad, cur, scratch);
+        for (int level = u->max_level; level > 0; level--) {
+            int changed = 1;
+            while (changed) {
+                changed = 0;
+                hops++;
+                if (u->levels[cur] < level) break;
+                const int32_t *row = u->rows + (u->row_start[cur] + level - 1) * u->row_stride;
+                const int size = row[0];
+                for (int i = 0; i < size; i++) {
+                    const int cand = row[u->ids_offset + i];
+                    const float d = dist_to(g, qpad, cand, scratch);
+                    if (d < curdist) {
+                        curdist = d;
+                        cur = cand;
+                        changed = 1;
+                    }
+                }
+            }
+        }
+        out_entry[qi] = cur;
+        if (out_hops) out_hops[qi] = hops;
+    }
+    free(qpad);
+    free(scratch);
+    return 0;
+}

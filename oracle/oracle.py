@@ -37,6 +37,18 @@ class FoGraph(ctypes.Structure):
     ]
 
 
+class FoUpper(ctypes.Structure):
+    _fields_ = [
+        ("rows", ctypes.c_void_p),
+        ("row_stride", ctypes.c_int64),
+        ("ids_offset", ctypes.c_int),
+        ("row_start", ctypes.c_void_p),
+        ("levels", ctypes.c_void_p),
+        ("max_level", ctypes.c_int),
+        ("entry", ctypes.c_int),
+    ]
+
+
 class FoParams(ctypes.Structure):
     _fields_ = [
         ("k", ctypes.c_int), ("ef", ctypes.c_int), ("mc", ctypes.c_int), ("mg", ctypes.c_int),
@@ -69,6 +81,9 @@ def lib():
         _lib.fo_bloom_stream.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p]
         _lib.fo_l2_batch.argtypes = [ctypes.POINTER(FoGraph), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                      ctypes.c_void_p]
+        _lib.fo_descend.restype = ctypes.c_int
+        _lib.fo_descend.argtypes = [ctypes.POINTER(FoGraph), ctypes.POINTER(FoUpper), ctypes.c_void_p,
+                                    ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
     return _lib
 
 
@@ -143,6 +158,33 @@ def search(og, queries, entries, params, out_stride=None, threads=None):
     if rc < 0:
         raise ValueError("oracle rejected arguments: %d" % rc)
     return ids, d, hops, vis, rc
+
+
+def descend(og, upper, queries):
+    """HNSW upper-layer greedy descent (fo_descend).  upper: an object with
+    max_level, entry, levels [n] int32, row_start [n] int64 and rows
+    [num_rows, 1 + max_degree] int32 (count, then ids), as
+    falcon_b200.formats.UpperLayers.  Returns (entries, upper hops)."""
+    q = np.ascontiguousarray(queries, dtype=np.float32)
+    rows = np.ascontiguousarray(upper.rows, dtype=np.int32)
+    starts = np.ascontiguousarray(upper.row_start, dtype=np.int64)
+    levels = np.ascontiguousarray(upper.levels, dtype=np.int32)
+    u = FoUpper()
+    u.rows = rows.ctypes.data
+    u.row_stride = rows.shape[1]
+    u.ids_offset = 1
+    u.row_start = starts.ctypes.data
+    u.levels = levels.ctypes.data
+    u.max_level = int(upper.max_level)
+    u.entry = int(upper.entry)
+    nq = q.shape[0]
+    ent = np.empty(nq, dtype=np.int32)
+    hops = np.empty(nq, dtype=np.int32)
+    rc = lib().fo_descend(ctypes.byref(og.g), ctypes.byref(u), q.ctypes.data, nq, q.shape[1], ent.ctypes.data,
+                          hops.ctypes.data)
+    if rc < 0:
+        raise MemoryError("oracle descent failed")
+    return ent, hops
 
 
 def murmur2(key, seed):
@@ -246,6 +288,11 @@ class Hnsw:
         L.hnsw_search.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         L.hnsw_free.argtypes = [ctypes.c_void_p]
+        L.hnsw_save.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        L.hnsw_upper_rows.restype = ctypes.c_int64
+        L.hnsw_upper_rows.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.hnsw_export_upper.argtypes = [ctypes.c_void_p] * 4
+        L.hnsw_descend.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p]
         return L
 
     @classmethod
@@ -283,6 +330,31 @@ class Hnsw:
         labels = np.empty(n.value, dtype=np.int32)
         L.hnsw_export_level0(self.h, links.ctypes.data, counts.ctypes.data, labels.ctypes.data)
         return links, counts, labels, ep.value, ml.value
+
+    def save(self, path):
+        """hnswlib's own saveIndex."""
+        self._L().hnsw_save(self.h, path.encode())
+
+    def upper(self):
+        """(max_level, entry, max_m, levels [n], row_start [n], rows [num_rows, 1 + max_m]) through
+        hnswlib's accessors."""
+        L = self._L()
+        links, counts, labels, ep, ml = self.level0()
+        n = links.shape[0]
+        mm = ctypes.c_int()
+        nrows = L.hnsw_upper_rows(self.h, ctypes.byref(mm))
+        levels = np.empty(n, dtype=np.int32)
+        starts = np.empty(n, dtype=np.int64)
+        rows = np.zeros((max(nrows, 1), 1 + mm.value), dtype=np.int32)
+        L.hnsw_export_upper(self.h, levels.ctypes.data, starts.ctypes.data, rows.ctypes.data)
+        return ml, ep, mm.value, levels, starts, rows
+
+    def descend(self, queries):
+        """Base-layer entry per query from hnswlib's greedy upper-layer search."""
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        out = np.empty(len(q), dtype=np.int32)
+        self._L().hnsw_descend(self.h, q.ctypes.data, len(q), self.dim, out.ctypes.data)
+        return out
 
     def search(self, queries, k, ef, threads):
         q = np.ascontiguousarray(queries, dtype=np.float32)

@@ -12,7 +12,10 @@
  *     loaded into the GPU index and the oracle;
  *   - the reference CPU search baseline: searchKnn with setEf(ef) over
  *     std::threads (hnswalg.h:1115-1160, 241-325), on any graph loaded through
- *     hnsw_from_graph (single layer, given entry point).
+ *     hnsw_from_graph (single layer, given entry point);
+ *   - checking the hnswlib file reader (saveIndex, hnswalg.h:588-616, and the
+ *     upper layers read through get_linklist) and the upper-layer descent
+ *     (searchKnn's greedy part, hnswalg.h:514-541, with hnswlib's distance).
  */
 #include <algorithm>
 #include <atomic>
@@ -124,6 +127,80 @@ extern "C" int hnsw_search(void *hp, const float *queries, int64_t nq, int dim, 
     std::vector<std::thread> th;
     for (int t = 0; t < threads; t++) th.emplace_back(work);
     for (auto &t : th) t.join();
+    return 0;
+}
+
+/* hnswlib's own saveIndex (hnswalg.h:588-616). */
+extern "C" int hnsw_save(void *hp, const char *path)
+{
+    hnsw_handle *h = (hnsw_handle *)hp;
+    h->index->saveIndex(std::string(path));
+    return 0;
+}
+
+/* Upper layers: number of level rows (sum of element levels) and maxM. */
+extern "C" int64_t hnsw_upper_rows(void *hp, int *max_m)
+{
+    hnsw_handle *h = (hnsw_handle *)hp;
+    auto *ix = h->index;
+    int64_t rows = 0;
+    for (size_t i = 0; i < ix->cur_element_count; i++) rows += ix->element_levels_[i];
+    *max_m = (int)ix->maxM_;
+    return rows;
+}
+
+/* Export levels [n], row_start [n] and rows [num_rows x (1 + maxM)] (count,
+   ids) read through hnswlib's own accessors (get_linklist, getListCount). */
+extern "C" int hnsw_export_upper(void *hp, int32_t *levels, int64_t *row_start, int32_t *rows)
+{
+    hnsw_handle *h = (hnsw_handle *)hp;
+    auto *ix = h->index;
+    const int m = (int)ix->maxM_;
+    int64_t r = 0;
+    for (size_t i = 0; i < ix->cur_element_count; i++) {
+        const int lv = ix->element_levels_[i];
+        levels[i] = lv;
+        row_start[i] = r;
+        for (int l = 1; l <= lv; l++, r++) {
+            hnswlib::linklistsizeint *ll = ix->get_linklist((hnswlib::tableint)i, l);
+            const int c = ix->getListCount(ll);
+            const hnswlib::tableint *src = (const hnswlib::tableint *)(ll + 1);
+            rows[r * (1 + m)] = c;
+            for (int j = 0; j < m; j++) rows[r * (1 + m) + 1 + j] = (j < c) ? (int32_t)src[j] : 0;
+        }
+    }
+    return 0;
+}
+
+/* The upper-layer part of searchKnn (hnswalg.h:514-541) with hnswlib's own
+   distance function: the base-layer entry point of each query. */
+extern "C" int hnsw_descend(void *hp, const float *queries, int64_t nq, int dim, int32_t *out_entry)
+{
+    hnsw_handle *h = (hnsw_handle *)hp;
+    auto *ix = h->index;
+    for (int64_t q = 0; q < nq; q++) {
+        const void *qd = (const void *)(queries + q * dim);
+        hnswlib::tableint cur = ix->enterpoint_node_;
+        float curdist = ix->fstdistfunc_(qd, ix->getDataByInternalId(cur), ix->dist_func_param_);
+        for (int level = ix->maxlevel_; level > 0; level--) {
+            bool changed = true;
+            while (changed) {
+                changed = false;
+                hnswlib::linklistsizeint *ll = ix->get_linklist(cur, level);
+                const int size = ix->getListCount(ll);
+                const hnswlib::tableint *datal = (const hnswlib::tableint *)(ll + 1);
+                for (int i = 0; i < size; i++) {
+                    const float d = ix->fstdistfunc_(qd, ix->getDataByInternalId(datal[i]), ix->dist_func_param_);
+                    if (d < curdist) {
+                        curdist = d;
+                        cur = datal[i];
+                        changed = true;
+                    }
+                }
+            }
+        }
+        out_entry[q] = (int32_t)cur;
+    }
     return 0;
 }
 
