@@ -32,7 +32,9 @@ N_QUERIES = 10_000
 MAX_DEGREE = 64
 K = 10
 RECALL_TARGET = 0.95
-WORKLOAD = "deep1m_hnsw_m32: 1M x 96 unit-normal base, 10k queries, degree-64 single-layer graph, k=10"
+WORKLOAD = ("deep1m_hnsw_m32: 1M x 96 unit-normal base, 10k queries, HNSW M=32 (degree-64 base layer + upper "
+            "layers), k=10")
+HNSW_M = 32
 # (ef, mc, mg, cand_queue_size, bloom_bits): the configuration's ef values with
 # the reference's 32-entry candidate queue and 2^16-bit Bloom filter, then
 # larger ef, queues and filters (a query here visits 10^4-10^5 nodes, which
@@ -52,8 +54,8 @@ def dist_env():
     return ws, rank, local
 
 
-def make_workload(rank, device):
-    from falcon_b200.graph import build_graph
+def make_workload(rank, device, upper_layers=False):
+    from falcon_b200.graph import build_graph, build_upper_layers
     from falcon_b200.groundtruth import shortlist_f64
     from falcon_b200.synthetic import unit_normal
     t = time.time()
@@ -63,9 +65,17 @@ def make_workload(rank, device):
     t = time.time()
     g = build_graph(x, MAX_DEGREE, device=device)
     log("graph %.1fs (mean degree %.1f)" % (time.time() - t, g.counts().mean()))
+    upper = None
+    if upper_layers:
+        t = time.time()
+        upper = build_upper_layers(x, HNSW_M, seed=0, device=device)
+        log("upper layers %.1fs (levels %d, %d nodes above the base)" % (time.time() - t, upper.max_level,
+                                                                          int((upper.levels > 0).sum())))
     t = time.time()
     gt, _ = shortlist_f64(x, q, K, device=device)
     log("ground truth %.1fs" % (time.time() - t))
+    if upper_layers:
+        return x, q, g, gt, upper
     return x, q, g, gt
 
 
@@ -286,8 +296,9 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from falcon_b200 import FalconIndex
     from falcon_b200.groundtruth import recall_at_k
-    x, q, g, gt = make_workload(rank, dev)
+    x, q, g, gt, upper = make_workload(rank, dev, upper_layers=True)
     ix = FalconIndex(g, storage=("f32", "bf16"), device=local)
+    ix.set_upper_layers(upper)   # every search descends the upper layers, then searches the base layer
     if args.fixed:
         ef_, mc_, mg_, cq_, bits_ = [int(v) for v in args.fixed.split(",")]
         best, reached, table = dict(ef=ef_, mc=mc_, mg=mg_, cq=cq_, bits=bits_), None, []
@@ -421,7 +432,7 @@ def run_ours(args):
                 "h2d_bytes_per_step": int(q.nbytes), "d2h_bytes_per_step": int(N_QUERIES * K * 8 + N_QUERIES * 8)},
         "bf16_rerank": {"value": N_QUERIES / (bf_ms / 1e3), "unit": "queries/s", "recall@10": bf_recall},
         "served": served,
-        "gpu_launches": args.steps,
+        "gpu_launches": 2 * args.steps,   # per step: the upper-layer descent and the base-layer search
         "clocks": clk.summary(),
         "roofline": roof,
         "cpu_baseline": cpu,
