@@ -509,10 +509,52 @@ done:
     return rc;
 }
 
+// Trace outputs of falcon_search_trace (caller memory, host or device).
+struct TraceOut {
+    float *cand_d;
+    int32_t *cand_n;
+    int32_t cand_cap;
+    float *d;
+    int32_t *ids;
+    int32_t cap;
+    int32_t *counts;
+};
+
+static int search_impl(falcon_index *ix, const float *queries, int64_t nq, int64_t query_stride,
+                       const int32_t *entry_points, const falcon_search_params *params, int32_t per_query_params,
+                       int32_t *out_ids, float *out_dists, int32_t out_stride, int32_t *out_hops,
+                       int32_t *out_visited, int32_t memory, void *stream_v, const TraceOut *tro);
+
 int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t query_stride,
                   const int32_t *entry_points, const falcon_search_params *params, int32_t per_query_params,
                   int32_t *out_ids, float *out_dists, int32_t out_stride, int32_t *out_hops, int32_t *out_visited,
                   int32_t memory, void *stream_v)
+{
+    return search_impl(ix, queries, nq, query_stride, entry_points, params, per_query_params, out_ids, out_dists,
+                       out_stride, out_hops, out_visited, memory, stream_v, nullptr);
+}
+
+int falcon_search_trace(falcon_index *ix, const float *queries, int64_t nq, int64_t query_stride,
+                        const int32_t *entry_points, const falcon_search_params *params, int32_t *out_ids,
+                        float *out_dists, int32_t out_stride, int32_t *out_hops, int32_t *out_visited,
+                        float *trace_cand_dists, int32_t *trace_cand_counts, int32_t cand_capacity,
+                        float *trace_dists, int32_t *trace_ids, int32_t capacity, int32_t *trace_counts,
+                        int32_t memory, void *stream)
+{
+    if (!params || !trace_counts || cand_capacity < 0 || capacity < 0 ||
+        (cand_capacity > 0 && (!trace_cand_dists || !trace_cand_counts)) || (capacity > 0 && (!trace_dists || !trace_ids)))
+        return set_error(FALCON_ERR_ARG, "falcon_search_trace: bad trace buffers");
+    if (params->mode != FALCON_MODE_INTER || params->precision != FALCON_PREC_F32 || params->rerank)
+        return set_error(FALCON_ERR_UNSUPPORTED, "falcon_search_trace: FP32 inter-query searches only");
+    TraceOut t = {trace_cand_dists, trace_cand_counts, cand_capacity, trace_dists, trace_ids, capacity, trace_counts};
+    return search_impl(ix, queries, nq, query_stride, entry_points, params, 0, out_ids, out_dists, out_stride,
+                       out_hops, out_visited, memory, stream, &t);
+}
+
+static int search_impl(falcon_index *ix, const float *queries, int64_t nq, int64_t query_stride,
+                       const int32_t *entry_points, const falcon_search_params *params, int32_t per_query_params,
+                       int32_t *out_ids, float *out_dists, int32_t out_stride, int32_t *out_hops,
+                       int32_t *out_visited, int32_t memory, void *stream_v, const TraceOut *tro)
 {
     if (!ix || !params || !out_ids || !out_dists) return set_error(FALCON_ERR_ARG, "null argument");
     if (nq < 0 || (nq > 0 && !queries) || query_stride < ix->dim)
@@ -571,6 +613,8 @@ int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t qu
     QParams *d_params = nullptr;
     int32_t *d_scratch = nullptr;   // [0..1] work counter (u64), [2] status
     uint32_t *d_bloom = nullptr;    // global Bloom filters when bloom_bits > kMaxSmemBloomBits
+    float *d_tcd = nullptr, *d_td = nullptr;      // trace buffers (host-memory calls)
+    int32_t *d_tcn = nullptr, *d_tid = nullptr, *d_tcnt = nullptr;
     int32_t status_h = 0;
     SearchLaunch a;
     memset(&a, 0, sizeof(a));
@@ -634,6 +678,23 @@ int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t qu
         a.mg_max = mg_max;
         a.channels = (mode == FALCON_MODE_INTRA) ? qp[0].channels : 0;
         a.cq_max = cq_max;
+        if (tro) {
+            const size_t ncd = (size_t)nq * tro->cand_cap, nd = (size_t)nq * tro->cap;
+            if (host) {
+                if (ncd) FALCON_CUDA(cudaMallocAsync((void **)&d_tcd, ncd * sizeof(float), s));
+                if (ncd) FALCON_CUDA(cudaMallocAsync((void **)&d_tcn, ncd * sizeof(int32_t), s));
+                if (nd) FALCON_CUDA(cudaMallocAsync((void **)&d_td, nd * sizeof(float), s));
+                if (nd) FALCON_CUDA(cudaMallocAsync((void **)&d_tid, nd * sizeof(int32_t), s));
+                FALCON_CUDA(cudaMallocAsync((void **)&d_tcnt, (size_t)nq * 3 * sizeof(int32_t), s));
+            }
+            a.trace_cand_d = host ? d_tcd : tro->cand_d;
+            a.trace_cand_n = host ? d_tcn : tro->cand_n;
+            a.trace_cand_cap = tro->cand_cap;
+            a.trace_d = host ? d_td : tro->d;
+            a.trace_id = host ? d_tid : tro->ids;
+            a.trace_cap = tro->cap;
+            a.trace_counts = host ? d_tcnt : tro->counts;
+        }
         int32_t *final_ids = a.out_ids;
         float *final_d = a.out_d;
         if (any_rerank) {
@@ -685,11 +746,25 @@ int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t qu
             if (out_hops) FALCON_CUDA(cudaMemcpyAsync(out_hops, d_hops, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
             if (out_visited) FALCON_CUDA(cudaMemcpyAsync(out_visited, d_vis, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
             FALCON_CUDA(cudaMemcpyAsync(&status_h, d_scratch + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            if (tro) {
+                const size_t ncd = (size_t)nq * tro->cand_cap, nd = (size_t)nq * tro->cap;
+                if (ncd) {
+                    FALCON_CUDA(cudaMemcpyAsync(tro->cand_d, d_tcd, ncd * sizeof(float), cudaMemcpyDeviceToHost, s));
+                    FALCON_CUDA(cudaMemcpyAsync(tro->cand_n, d_tcn, ncd * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+                }
+                if (nd) {
+                    FALCON_CUDA(cudaMemcpyAsync(tro->d, d_td, nd * sizeof(float), cudaMemcpyDeviceToHost, s));
+                    FALCON_CUDA(cudaMemcpyAsync(tro->ids, d_tid, nd * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+                }
+                FALCON_CUDA(cudaMemcpyAsync(tro->counts, d_tcnt, (size_t)nq * 3 * sizeof(int32_t),
+                                            cudaMemcpyDeviceToHost, s));
+            }
         }
     }
 done:
     for (void *p : {(void *)d_q, (void *)d_entries, (void *)d_ids, (void *)d_d, (void *)d_hops, (void *)d_vis,
-                    (void *)d_params, (void *)d_scratch, (void *)d_cand, (void *)d_cand_d, (void *)d_bloom})
+                    (void *)d_params, (void *)d_scratch, (void *)d_cand, (void *)d_cand_d, (void *)d_bloom,
+                    (void *)d_tcd, (void *)d_tcn, (void *)d_td, (void *)d_tid, (void *)d_tcnt})
         if (p) cudaFreeAsync(p, s);
     if (rc == FALCON_OK && host) {
         cudaError_t e = cudaStreamSynchronize(s);

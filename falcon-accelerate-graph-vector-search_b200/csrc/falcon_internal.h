@@ -96,6 +96,15 @@ struct SearchLaunch {
     int32_t channels;               // 0: inter-query (warp per query); else intra-query block of `channels` warps
     int32_t cq_max;                 // largest candidate queue of the call
     uint32_t *bloom_global;         // bloom_bits_max > kMaxSmemBloomBits: per-warp filters in global memory
+    // traversal trace (FP32 inter-query only; null = off): per query trace_cand_cap
+    // (distance, computed count) and trace_cap (distance, id) entries, 3 counts
+    float *trace_cand_d;
+    int32_t *trace_cand_n;
+    int32_t trace_cand_cap;
+    float *trace_d;
+    int32_t *trace_id;
+    int32_t trace_cap;
+    int32_t *trace_counts;
 };
 
 struct RerankLaunch {

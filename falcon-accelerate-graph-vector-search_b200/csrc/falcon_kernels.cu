@@ -582,11 +582,41 @@ struct QueryIO {
 template <int ELEM, int VROWS>
 constexpr bool kRowBloom = (VROWS == 1 && ELEM != kFP8);
 
+// Traversal trace of one query (the reference's trace kernel,
+// FPGA_multi_DDR/eval_trace_FPGA_inter_query_v1.3/src/DRAM_utils.hpp:389-474,
+// scheduler.hpp:84): per expanded candidate in FIFO order its distance (1e20
+// for the entry point, which is not distance-computed) and the number of
+// distances computed for its row; per computed distance in stream order the
+// distance and the id.  counts = {popped incl. the entry, expanded, computed};
+// entries past a capacity are counted, not written.
+struct TraceIO {
+    float *cand_d;
+    int32_t *cand_n;
+    int32_t cand_cap;
+    float *d;
+    int32_t *id;
+    int32_t cap;
+    int32_t *counts;
+};
+
+// Record the computed distances of one batch (lanes with `rec`, whose slots
+// ascend with the lanes) at trace positions n.. in stream order.
+__device__ __forceinline__ void trace_batch(const TraceIO *tr, int &n, bool rec, float dist, int id, int lane)
+{
+    const unsigned m = __ballot_sync(kFull, rec);
+    if (rec) {
+        const int pos = n + __popc(m & ((1u << lane) - 1u));
+        if (pos < tr->cap) { tr->d[pos] = dist; tr->id[pos] = id; }
+    }
+    n += __popc(m);
+}
+
 // ROW selects the whole-row Bloom path for degrees <= 64; instances whose
 // vector registers leave no room for it keep the per-32-id path.
-template <int ELEM, int EPL, int VROWS, bool ROW>
+template <int ELEM, int EPL, int VROWS, bool ROW, bool TRACE = false>
 __device__ void search_one_inter(const GraphView &g, const QParams &P, const QueryIO &io, uint32_t *bloom, int *fifo,
-                                 int *fifo_len, int *sids, uint64_t *hkey, int *hid, int lane)
+                                 int *fifo_len, int *sids, uint64_t *hkey, int *hid, int lane,
+                                 const TraceIO *tr = nullptr)
 {
     constexpr bool HEAP = EPL > 8;            // result list as a shared-memory heap
     constexpr int REPL = HEAP ? 1 : EPL;      // register entries per lane
@@ -653,6 +683,10 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
     if (lane == 0) { fifo[0] = entry; fifo_len[0] = 1; }
     __syncwarp();
     bool truncated = false;
+    int t_pop = 1, t_exp = 0, t_dist = 0;   // trace counters
+    if constexpr (TRACE) {
+        if (lane == 0 && tr->cand_cap > 0) tr->cand_d[0] = kLarge;
+    }
 
     while (inflight > 0) {
         const int glen = fifo_len[head];
@@ -695,6 +729,7 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                     if (b0 + BS < PV) gather_batch<ELEM, VROWS, NB>(g, sids, b0 + BS, PV, nseg, lane, lg, raw, scale);
                     const int nt = min(BS, PV - b0);
                     const bool keep = rep_lane && my_slot < nt && sids[b0 + my_slot] >= 0;
+                    if constexpr (TRACE) trace_batch(tr, t_dist, keep, dist, keep ? sids[b0 + my_slot] : 0, lane);
                     unsigned m = __ballot_sync(kFull, keep && dist < rmax);
                     while (m) {   // representative lanes ascend with the slots
                         const int t = __ffs(m) - 1;
@@ -717,10 +752,15 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                     prefetch_head_row(g, ci[0], rbytes, pf_head, lane);
                 }
                 visited += __popc(vm0) + __popc(vm1);
+                if constexpr (TRACE) {
+                    if (lane == 0 && t_exp < tr->cand_cap) tr->cand_n[t_exp] = __popc(vm0) + __popc(vm1);
+                    t_exp++;
+                }
                 __syncwarp();
                 continue;
             }
             const int cnt = ld_nc_s32(row);
+            int row_valid = 0;
             for (int c0 = 0; c0 < cnt; c0 += 32) {
                 const bool act = c0 + lane < cnt;
                 const int nb = act ? ld_nc_s32(row + g.ids_off + c0 + lane) : -1;
@@ -728,6 +768,7 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                 const unsigned vm = __ballot_sync(kFull, valid);
                 const int V = __popc(vm);
                 visited += V;
+                row_valid += V;
                 if (valid) sids[__popc(vm & ((1u << lane) - 1u))] = nb;
                 if (valid) prefetch_l2(g.vecs + (int64_t)nb * g.vstride_bytes, vbytes);
                 __syncwarp();
@@ -738,6 +779,9 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                     const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane, lg);
                     if (b0 + BS < V) gather_batch<ELEM, VROWS, NB>(g, sids, b0 + BS, V, nseg, lane, lg, raw, scale);
                     const int nt = min(BS, V - b0);
+                    if constexpr (TRACE)
+                        trace_batch(tr, t_dist, rep_lane && my_slot < nt, dist,
+                                    (rep_lane && my_slot < nt) ? sids[b0 + my_slot] : 0, lane);
                     // results collection (DRAM_utils.hpp:421-438) in stream order; the
                     // maximum only decreases, so a distance not below it now never will be
                     unsigned m = __ballot_sync(kFull, rep_lane && my_slot < nt && dist < rmax);
@@ -763,6 +807,10 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                 }
                 __syncwarp();
             }
+            if constexpr (TRACE) {
+                if (lane == 0 && t_exp < tr->cand_cap) tr->cand_n[t_exp] = row_valid;
+                t_exp++;
+            }
         }
         // the oldest group is retired (scheduler.hpp:112-155): threshold = worst result
         const float thr = rmax;
@@ -776,6 +824,10 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                 const float best = __shfl_sync(kFull, cd[0], 0);
                 if (!(best <= thr && best < kLarge)) break;
                 if (P.max_hops > 0 && hops >= P.max_hops) { truncated = true; break; }
+                if constexpr (TRACE) {
+                    if (lane == 0 && t_pop < tr->cand_cap) tr->cand_d[t_pop] = best;
+                    t_pop++;
+                }
                 const int pid = cl_pop<CPL>(cd, ci, lane, P.cq);
                 if (lane == 0) fifo[slot * mc + n] = pid;
                 n++;
@@ -787,6 +839,9 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
         }
         cmax = rl_get<CPL>(cd, P.cq - 1);
         __syncwarp();
+    }
+    if constexpr (TRACE) {
+        if (lane == 0) { tr->counts[0] = t_pop; tr->counts[1] = t_exp; tr->counts[2] = t_dist; }
     }
 
     // results best-first (DRAM_utils.hpp:460-464): list position i is result i
@@ -834,7 +889,7 @@ __host__ __device__ __forceinline__ size_t warp_smem_bytes(int bloom_bits_max, i
     return (b + 15) & ~(size_t)15;
 }
 
-template <int ELEM, int EPL, int VROWS>
+template <int ELEM, int EPL, int VROWS, bool TRACE>
 __global__ void __launch_bounds__(128, 3) inter_kernel(const SearchLaunch A)
 {
     extern __shared__ uint4 smem_u4[];
@@ -868,8 +923,21 @@ __global__ void __launch_bounds__(128, 3) inter_kernel(const SearchLaunch A)
         io.hops = A.out_hops ? A.out_hops + qi : nullptr;
         io.visited = A.out_visited ? A.out_visited + qi : nullptr;
         io.status = A.status;
-        search_one_inter<ELEM, EPL, VROWS, kRowBloom<ELEM, VROWS>>(A.g, P, io, bloom, fifo, fifo_len, sids, hkey, hid,
-                                                                   lane);
+        if constexpr (TRACE) {
+            TraceIO tio;
+            tio.cand_d = A.trace_cand_d + (int64_t)qi * A.trace_cand_cap;
+            tio.cand_n = A.trace_cand_n + (int64_t)qi * A.trace_cand_cap;
+            tio.cand_cap = A.trace_cand_cap;
+            tio.d = A.trace_d + (int64_t)qi * A.trace_cap;
+            tio.id = A.trace_id + (int64_t)qi * A.trace_cap;
+            tio.cap = A.trace_cap;
+            tio.counts = A.trace_counts + 3 * (int64_t)qi;
+            search_one_inter<ELEM, EPL, VROWS, kRowBloom<ELEM, VROWS>, true>(A.g, P, io, bloom, fifo, fifo_len, sids,
+                                                                             hkey, hid, lane, &tio);
+        } else {
+            search_one_inter<ELEM, EPL, VROWS, kRowBloom<ELEM, VROWS>>(A.g, P, io, bloom, fifo, fifo_len, sids, hkey,
+                                                                       hid, lane);
+        }
         __syncwarp();
     }
 }
@@ -1511,7 +1579,10 @@ __global__ void encode_fp8_kernel(const float *src, int64_t src_stride, int64_t 
 template <int ELEM, int EPL, int VROWS>
 cudaError_t launch_inter(const SearchLaunch &a, size_t, int num_sms, cudaStream_t s, int64_t *slots)
 {
-    auto kern = inter_kernel<ELEM, EPL, VROWS>;
+    // the trace variant (a.trace_counts set) exists for FP32 only
+    constexpr bool kTrace = (ELEM == kF32);
+    auto kern = (kTrace && a.trace_counts) ? inter_kernel<ELEM, EPL, VROWS, kTrace> : inter_kernel<ELEM, EPL, VROWS, false>;
+    if (a.trace_counts && !kTrace) return cudaErrorInvalidValue;
     const size_t smem_block = warp_smem_bytes(a.bloom_bits_max, a.mc_max, a.mg_max, (EPL > 8) ? 32 * EPL : 0) * 4;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_block);
     if (e != cudaSuccess) return e;

@@ -127,6 +127,8 @@ SIGNATURES = {
     "falcon_descend": (_I32, [_VP, _VP, _I64, _I64, _VP, _VP, _I32, _VP]),
     "falcon_search": (_I32, [_VP, _VP, _I64, _I64, _VP, ctypes.POINTER(SearchParams), _I32,
                              _VP, _VP, _I32, _VP, _VP, _I32, _VP]),
+    "falcon_search_trace": (_I32, [_VP, _VP, _I64, _I64, _VP, ctypes.POINTER(SearchParams), _VP, _VP, _I32, _VP,
+                                   _VP, _VP, _VP, _I32, _VP, _VP, _I32, _VP, _I32, _VP]),
     "falcon_search_noalloc": (_I32, [_VP, _VP, _I64, _I64, _VP, ctypes.POINTER(SearchParams), _I32,
                                      _VP, _VP, _I32, _VP, _VP, _VP]),
     "falcon_vadd": (_I32, [_I32, _I32, _I32, _I32, _I32, _I32, _I32, ctypes.c_uint32, _I32, _I32, _I32, _I64,

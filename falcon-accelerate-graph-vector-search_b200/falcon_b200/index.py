@@ -49,6 +49,36 @@ class SearchResult:
         return iter((self.ids, self.dists, self.hops, self.visited))
 
 
+class Trace:
+    """Per-query traversal trace: cand_d/cand_n [nq, cand_capacity] (distance
+    of each expanded candidate, 1e20 for the entry, and the distances computed
+    for its row), d/ids [nq, capacity] (each computed distance and its id, in
+    traversal order), counts [nq, 3] (popped incl. entry, expanded, computed)."""
+
+    def __init__(self, cand_d, cand_n, d, ids, counts):
+        self.cand_d, self.cand_n, self.d, self.ids, self.counts = cand_d, cand_n, d, ids, counts
+
+    def query(self, i):
+        """(cand_d, cand_n, d, ids) of query i, cut to what was written."""
+        ne = min(int(self.counts[i, 1]), self.cand_d.shape[1])
+        nd = min(int(self.counts[i, 2]), self.d.shape[1])
+        return self.cand_d[i, :ne], self.cand_n[i, :ne], self.d[i, :nd], self.ids[i, :nd]
+
+    def reference_streams(self):
+        """The reference trace kernel's flat outputs (debug_out_per_query_*,
+        eval_trace_FPGA_inter_query_v1.3 DRAM_utils.hpp:389-404): per query -1,
+        the entries, then -2; returns (cand_dists, cand_num_neighbors, dists, ids)."""
+        cds, cns, ds, ids = [], [], [], []
+        for i in range(self.counts.shape[0]):
+            c_d, c_n, d, di = self.query(i)
+            cds += [-1.0] + c_d.tolist() + [-2.0]
+            cns += [-1] + c_n.tolist() + [-2]
+            ds += [-1.0] + d.tolist() + [-2.0]
+            ids += [-1] + di.tolist() + [-2]
+        return (np.array(cds, dtype=np.float32), np.array(cns, dtype=np.int32), np.array(ds, dtype=np.float32),
+                np.array(ids, dtype=np.int32))
+
+
 class FalconIndex:
     """A device-resident graph index (one GPU)."""
 
@@ -196,6 +226,32 @@ class FalconIndex:
                                vis.ctypes.data, _lib.MEM_HOST, stream)
         _lib.check(rc)
         return SearchResult(ids, dists, hops, vis, rc)
+
+    def search_trace(self, queries, cand_capacity=4096, capacity=65536, k=10, ef=64, mc=1, mg=1,
+                     cand_queue_size=32, bloom_bits=16, hash_seed=1, max_hops=0, entry_points=None, stream=None):
+        """FP32 inter-query search with the traversal trace (falcon_search_trace)
+        on host queries.  Returns (SearchResult, Trace)."""
+        lib = _lib.load()
+        params = make_params(k, ef, mc, mg, cand_queue_size, bloom_bits, hash_seed, "inter", 4, "f32", False,
+                             max_hops)
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        nq = q.shape[0]
+        ids = np.empty((nq, k), dtype=np.int32)
+        dists = np.empty((nq, k), dtype=np.float32)
+        hops = np.empty(nq, dtype=np.int32)
+        vis = np.empty(nq, dtype=np.int32)
+        cd = np.zeros((nq, cand_capacity), dtype=np.float32)
+        cn = np.zeros((nq, cand_capacity), dtype=np.int32)
+        td = np.zeros((nq, capacity), dtype=np.float32)
+        ti = np.zeros((nq, capacity), dtype=np.int32)
+        cnt = np.zeros((nq, 3), dtype=np.int32)
+        ep = None if entry_points is None else np.ascontiguousarray(entry_points, dtype=np.int32)
+        rc = lib.falcon_search_trace(self._h, q.ctypes.data, nq, q.shape[1], ep.ctypes.data if ep is not None else None,
+                                     ctypes.byref(params), ids.ctypes.data, dists.ctypes.data, k, hops.ctypes.data,
+                                     vis.ctypes.data, cd.ctypes.data, cn.ctypes.data, cand_capacity, td.ctypes.data,
+                                     ti.ctypes.data, capacity, cnt.ctypes.data, _lib.MEM_HOST, stream)
+        _lib.check(rc)
+        return SearchResult(ids, dists, hops, vis, rc), Trace(cd, cn, td, ti, cnt)
 
     def _search_device(self, queries, params, pq, ostride, entry_points, stream):
         import torch

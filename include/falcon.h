@@ -209,6 +209,30 @@ int falcon_search(falcon_index *ix, const float *queries, int64_t nq, int64_t qu
                   int32_t *out_visited, int32_t memory, void *stream);
 
 /*
+ * Search with the traversal trace: the reference's trace kernel
+ * (FPGA_multi_DDR/eval_trace_FPGA_inter_query_v1.3: vadd's
+ * debug_out_per_query_{cand_dists, cand_num_neighbors, dists, ids}, written by
+ * DRAM_utils.hpp:389-474) as per-query arrays instead of -1/-2-delimited
+ * streams.  Results as falcon_search (one params struct: FP32, inter-query
+ * mode, no rerank).  Per query q:
+ *   trace_cand_dists/counts [q * cand_capacity + i]: the i-th expanded
+ *       candidate's distance (1e20 for the entry point, which is not
+ *       distance-computed) and the number of distances computed for its row;
+ *   trace_dists/ids [q * capacity + j]: the j-th computed distance and its id,
+ *       in the order the traversal computed them;
+ *   trace_counts[3q .. 3q+2]: popped candidates including the entry,
+ *       expanded candidates, computed distances (= hops, hops, visited).
+ * Entries past a capacity are counted but not written; array slots past a
+ * query's counts are unspecified.  memory/stream as for falcon_search.
+ */
+int falcon_search_trace(falcon_index *ix, const float *queries, int64_t nq, int64_t query_stride,
+                        const int32_t *entry_points, const falcon_search_params *params, int32_t *out_ids,
+                        float *out_dists, int32_t out_stride, int32_t *out_hops, int32_t *out_visited,
+                        float *trace_cand_dists, int32_t *trace_cand_counts, int32_t cand_capacity,
+                        float *trace_dists, int32_t *trace_ids, int32_t capacity, int32_t *trace_counts,
+                        int32_t memory, void *stream);
+
+/*
  * Search without allocating: for callers that cannot allocate device memory
  * on their query path -- serving threads with a fixed, pre-reserved
  * device-memory budget, hosts embedding this library inside a runtime that

@@ -5,6 +5,9 @@ Outputs:
   oracle/_ref/libfalcon_ref_d{D}.so the reference's own v1.3 HLS kernel headers
                                     compiled as plain C++ through the harness
                                     in oracle/ref_harness/ (one per dimension D)
+  oracle/_ref/libfalcon_ref_trace_d128.so
+                                    the same harness over the reference's trace
+                                    variant (eval_trace_FPGA_inter_query_v1.3)
   oracle/_ref/libhnswlib_ref.so     the reference's vendored hnswlib (graph
                                     builder + CPU search baseline)
   oracle/_ref/murmur_golden,
@@ -28,6 +31,7 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_ROOT = "/root/reference"
 REF_V13 = os.path.join(REF_ROOT, "FPGA_multi_DDR", "FPGA_inter_query_v1.3_longer_FIFO_alt_PR", "src")
+REF_TRACE = os.path.join(REF_ROOT, "FPGA_multi_DDR", "eval_trace_FPGA_inter_query_v1.3", "src")
 REF_HNSWLIB = os.path.join(REF_ROOT, "networked_FPGA", "CPU_programs_oldest", "hnswlib")
 REF_MURMUR = os.path.join(REF_ROOT, "unit_tests", "bloom_and_hash", "sw_murmur2", "murmur2.cpp")
 REF_SWBLOOM = os.path.join(REF_ROOT, "unit_tests", "bloom_and_hash", "sw_bloom")
@@ -70,11 +74,11 @@ _EDITS = [
 ]
 
 
-def _patched_v13_copy(dst, dim):
+def _patched_v13_copy(dst, dim, src=None):
     names = ["constants.hpp", "types.hpp", "utils.hpp", "priority_queue.hpp", "bloom_filter.hpp",
              "compute.hpp", "DRAM_utils.hpp", "scheduler.hpp"]
     for n in names:
-        shutil.copy(os.path.join(REF_V13, n), os.path.join(dst, n))
+        shutil.copy(os.path.join(src or REF_V13, n), os.path.join(dst, n))
     for fname, pat, rep in _EDITS:
         p = os.path.join(dst, fname)
         s = open(p).read()
@@ -107,6 +111,16 @@ def build_ref(force=False):
             _patched_v13_copy(td, dim)
             _run(["g++", "-O1", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math",
                   "-Wno-unknown-pragmas", "-pthread", "-I", shim, "-I", td, harness, "-o", out + ".tmp"])
+        os.replace(out + ".tmp", out)
+    # the trace variant of the same kernel (eval_trace_FPGA_inter_query_v1.3), D = 128
+    out = os.path.join(REF_OUT, "libfalcon_ref_trace_d128.so")
+    srcs = [harness] + [os.path.join(shim, f) for f in os.listdir(shim)] + [os.path.abspath(__file__)]
+    if force or _stale(out, srcs):
+        with tempfile.TemporaryDirectory() as td:
+            _patched_v13_copy(td, 128, REF_TRACE)
+            _run(["g++", "-O1", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math",
+                  "-Wno-unknown-pragmas", "-pthread", "-DFALCON_REF_TRACE", "-I", shim, "-I", td, harness,
+                  "-o", out + ".tmp"])
         os.replace(out + ".tmp", out)
     out = os.path.join(REF_OUT, "libhnswlib_ref.so")
     src = os.path.join(HERE, "ref_harness", "hnswlib_ref.cpp")

@@ -271,6 +271,18 @@ typedef struct {
     int *ins_ids; float *ins_d; /* items forwarded to the candidate queue */
 } fo_work;
 
+/* Trace of one inter-query traversal (FPGA_multi_DDR/
+   eval_trace_FPGA_inter_query_v1.3/src/DRAM_utils.hpp:389-474 and
+   scheduler.hpp:84): per expanded candidate in FIFO order its distance (1e20
+   for the entry point, which is not distance-computed) and the number of
+   distances computed for its row; per computed distance in stream order the
+   distance and the id.  Entries past a capacity are counted, not written. */
+typedef struct {
+    float *cand_d; int *cand_n; int cand_cap;
+    float *d; int *id; int cap;
+    int n_pop, n_exp, n_dist;
+} fo_trace;
+
 static int row_count(const fo_graph *g, int node)
 {
     return g->links[(int64_t)node * g->link_stride];
@@ -282,7 +294,7 @@ static int row_id(const fo_graph *g, int node, int j)
 
 /* Returns 0 on success, 1 when max_hops cut the traversal short. */
 static int search_one(const fo_graph *g, const fo_params *p, const float *query, int entry,
-                      fo_work *w, int *out_id, float *out_d, int *out_hops, int *out_visited)
+                      fo_work *w, int *out_id, float *out_d, int *out_hops, int *out_visited, fo_trace *tr)
 {
     const int ef = p->ef, mc = p->mc, mg = p->mg;
     fo_queue rq = { w->d, w->id, ef };
@@ -302,6 +314,10 @@ static int search_one(const fo_graph *g, const fo_params *p, const float *query,
     int head = 0, inflight = 1;
     w->fifo[0] = entry; w->fifo_len[0] = 1;
     int hops = 1, visited = 0, truncated = 0;
+    if (tr) {
+        tr->n_pop = 1; tr->n_exp = 0; tr->n_dist = 0;
+        if (tr->cand_cap > 0) tr->cand_d[0] = FO_LARGE;
+    }
 
     while (inflight > 0) {
         const int *grp = w->fifo + head * mc;
@@ -313,12 +329,17 @@ static int search_one(const fo_graph *g, const fo_params *p, const float *query,
             for (int b = 0; b < glen; b++) {
                 const int node = grp[b];
                 const int cnt = row_count(g, node);
-                int nins = 0;
+                int nins = 0, nval = 0;
                 for (int j = 0; j < cnt; j++) {
                     const int nb = row_id(g, node, j);
                     if (!bloom_check_update(&bl[0], (uint32_t)nb)) continue;
                     visited++;
+                    nval++;
                     const float dd = dist_to(g, w->qpad, nb, w->scratch);
+                    if (tr) {
+                        if (tr->n_dist < tr->cap) { tr->d[tr->n_dist] = dd; tr->id[tr->n_dist] = nb; }
+                        tr->n_dist++;
+                    }
                     if (dd < rq.d[0]) {
                         rq.d[0] = dd; rq.id[0] = nb;
                         w->ins_ids[nins] = nb; w->ins_d[nins] = dd; nins++;
@@ -326,6 +347,10 @@ static int search_one(const fo_graph *g, const fo_params *p, const float *query,
                     q_step(&rq);
                 }
                 for (int i = 0; i < nins; i++) q_insert_v13(&cq, w->ins_ids[i], w->ins_d[i]);
+                if (tr) {
+                    if (tr->n_exp < tr->cand_cap) tr->cand_n[tr->n_exp] = nval;
+                    tr->n_exp++;
+                }
             }
             q_sort(&rq);
         } else {
@@ -378,6 +403,10 @@ static int search_one(const fo_graph *g, const fo_params *p, const float *query,
                 const float best = cq.d[cq.n - 1];
                 if (best <= thr && best < FO_LARGE) {
                     if (p->max_hops > 0 && hops >= p->max_hops) { truncated = 1; break; }
+                    if (tr) {
+                        if (tr->n_pop < tr->cand_cap) tr->cand_d[tr->n_pop] = best;
+                        tr->n_pop++;
+                    }
                     q_pop(&cq, &w->fifo[slot * mc + n]);
                     n++;
                     hops++;
@@ -428,6 +457,10 @@ typedef struct {
     int64_t next;
     pthread_mutex_t mu;
     int any_truncated;
+    /* trace (inter-query mode; NULL = off): per query cand_cap / cap entries, counts [3] */
+    float *tr_cand_d; int32_t *tr_cand_n; int tr_cand_cap;
+    float *tr_d; int32_t *tr_id; int tr_cap;
+    int32_t *tr_counts;
 } fo_batch;
 
 static void *batch_worker(void *arg)
@@ -465,7 +498,19 @@ static void *batch_worker(void *arg)
             fo_params p = bt->params[qi * bt->param_stride];
             if (p.ef < p.k) p.ef = p.k;
             int hops, vis;
-            int tr = search_one(g, &p, bt->queries + qi * bt->q_stride, bt->entries[qi], &w, tid, td, &hops, &vis);
+            fo_trace trace, *tp = NULL;
+            if (bt->tr_counts) {
+                trace.cand_d = bt->tr_cand_d + qi * bt->tr_cand_cap; trace.cand_n = bt->tr_cand_n + qi * bt->tr_cand_cap;
+                trace.cand_cap = bt->tr_cand_cap;
+                trace.d = bt->tr_d + qi * bt->tr_cap; trace.id = bt->tr_id + qi * bt->tr_cap; trace.cap = bt->tr_cap;
+                tp = &trace;
+            }
+            int tr = search_one(g, &p, bt->queries + qi * bt->q_stride, bt->entries[qi], &w, tid, td, &hops, &vis, tp);
+            if (tp) {
+                bt->tr_counts[3 * qi] = trace.n_pop;
+                bt->tr_counts[3 * qi + 1] = trace.n_exp;
+                bt->tr_counts[3 * qi + 2] = trace.n_dist;
+            }
             if (tr) { pthread_mutex_lock(&bt->mu); bt->any_truncated = 1; pthread_mutex_unlock(&bt->mu); }
             if (p.rerank && g->elem != FO_F32 && g->vectors_f32) rerank_f32(g, w.qpad, p.ef, tid, td, w.scratch);
             for (int i = 0; i < bt->out_stride; i++) {
@@ -500,6 +545,8 @@ int fo_search(const fo_graph *g, const fo_params *params, int param_stride,
     bt.queries = queries; bt.q_stride = q_stride; bt.entries = entries; bt.nq = nq;
     bt.out_stride = out_stride; bt.out_ids = out_ids; bt.out_d = out_d;
     bt.out_hops = out_hops; bt.out_visited = out_visited; bt.next = 0; bt.any_truncated = 0;
+    bt.tr_cand_d = NULL; bt.tr_cand_n = NULL; bt.tr_cand_cap = 0;
+    bt.tr_d = NULL; bt.tr_id = NULL; bt.tr_cap = 0; bt.tr_counts = NULL;
     pthread_mutex_init(&bt.mu, NULL);
     if (threads < 1) threads = 1;
     if (threads > 256) threads = 256;
@@ -599,4 +646,35 @@ int fo_descend(const fo_graph *g, const fo_upper *u, const float *queries, int64
     free(qpad);
     free(scratch);
     return 0;
+}
+
+/* Inter-query search with the traversal trace (see fo_trace): per query
+   cand_cap candidate entries (distance, computed count) and cap distance
+   entries (distance, id); counts[3q..3q+2] = popped candidates incl. the entry,
+   expanded candidates, computed distances (entries past a capacity are counted,
+   not written). */
+int fo_search_trace(const fo_graph *g, const fo_params *params, const float *queries, int64_t q_stride,
+                    const int32_t *entries, int64_t nq, int out_stride, int32_t *out_ids, float *out_d,
+                    int32_t *out_hops, int32_t *out_visited, float *tr_cand_d, int32_t *tr_cand_n, int cand_cap,
+                    float *tr_d, int32_t *tr_id, int cap, int32_t *tr_counts, int threads)
+{
+    if (!g || !params || nq < 0 || g->dpad % 16 || g->dpad < g->dim || params->mode != 0 || !tr_counts) return -1;
+    if (params->ef < 1 || params->k < 1 || params->k > out_stride || params->mc < 1 || params->mg < 1 ||
+        params->cand_queue_size < 1 || params->bloom_bits < 10 || params->bloom_bits > 30 || cand_cap < 0 || cap < 0)
+        return -2;
+    fo_batch bt;
+    bt.g = g; bt.params = params; bt.param_stride = 0;
+    bt.queries = queries; bt.q_stride = q_stride; bt.entries = entries; bt.nq = nq;
+    bt.out_stride = out_stride; bt.out_ids = out_ids; bt.out_d = out_d;
+    bt.out_hops = out_hops; bt.out_visited = out_visited; bt.next = 0; bt.any_truncated = 0;
+    bt.tr_cand_d = tr_cand_d; bt.tr_cand_n = tr_cand_n; bt.tr_cand_cap = cand_cap;
+    bt.tr_d = tr_d; bt.tr_id = tr_id; bt.tr_cap = cap; bt.tr_counts = tr_counts;
+    pthread_mutex_init(&bt.mu, NULL);
+    if (threads < 1) threads = 1;
+    if (threads > 256) threads = 256;
+    pthread_t th[256];
+    for (int t = 0; t < threads; t++) pthread_create(&th[t], NULL, batch_worker, &bt);
+    for (int t = 0; t < threads; t++) pthread_join(th[t], NULL);
+    pthread_mutex_destroy(&bt.mu);
+    return bt.any_truncated;
 }

@@ -81,6 +81,11 @@ def lib():
         _lib.fo_bloom_stream.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p]
         _lib.fo_l2_batch.argtypes = [ctypes.POINTER(FoGraph), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                      ctypes.c_void_p]
+        _lib.fo_search_trace.restype = ctypes.c_int
+        _lib.fo_search_trace.argtypes = [ctypes.POINTER(FoGraph), ctypes.POINTER(FoParams), ctypes.c_void_p,
+                                         ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int] + \
+            [ctypes.c_void_p] * 6 + [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                     ctypes.c_int]
         _lib.fo_descend.restype = ctypes.c_int
         _lib.fo_descend.argtypes = [ctypes.POINTER(FoGraph), ctypes.POINTER(FoUpper), ctypes.c_void_p,
                                     ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
@@ -187,6 +192,33 @@ def descend(og, upper, queries):
     return ent, hops
 
 
+def search_trace(og, queries, entries, params, cand_cap, cap, threads=None):
+    """Inter-query search with the traversal trace (fo_search_trace).  Returns
+    ids, dists, hops, visited, and the trace: cand_d [nq, cand_cap],
+    cand_n [nq, cand_cap], d [nq, cap], id [nq, cap], counts [nq, 3]
+    (popped incl. entry, expanded, computed distances)."""
+    q = np.ascontiguousarray(queries, dtype=np.float32)
+    nq = q.shape[0]
+    e = np.ascontiguousarray(np.broadcast_to(np.asarray(entries, dtype=np.int32), (nq,)))
+    k = params.k
+    ids = np.empty((nq, k), dtype=np.int32)
+    d = np.empty((nq, k), dtype=np.float32)
+    hops = np.empty(nq, dtype=np.int32)
+    vis = np.empty(nq, dtype=np.int32)
+    cd = np.zeros((nq, cand_cap), dtype=np.float32)
+    cn = np.zeros((nq, cand_cap), dtype=np.int32)
+    td = np.zeros((nq, cap), dtype=np.float32)
+    ti = np.zeros((nq, cap), dtype=np.int32)
+    cnt = np.zeros((nq, 3), dtype=np.int32)
+    threads = threads or min(32, os.cpu_count() or 1)
+    rc = lib().fo_search_trace(ctypes.byref(og.g), ctypes.byref(params), q.ctypes.data, q.shape[1], e.ctypes.data, nq,
+                               k, ids.ctypes.data, d.ctypes.data, hops.ctypes.data, vis.ctypes.data, cd.ctypes.data,
+                               cn.ctypes.data, cand_cap, td.ctypes.data, ti.ctypes.data, cap, cnt.ctypes.data, threads)
+    if rc < 0:
+        raise ValueError("oracle rejected arguments: %d" % rc)
+    return ids, d, hops, vis, (cd, cn, td, ti, cnt)
+
+
 def murmur2(key, seed):
     return int(lib().fo_murmur2_keylen4(key & 0xffffffff, seed & 0xffffffff))
 
@@ -241,6 +273,60 @@ def _ref_lib(dim):
             [ctypes.c_void_p] * 7
         _ref_libs[dim] = L
     return _ref_libs[dim]
+
+
+def ref_trace_available():
+    return os.path.exists(os.path.join(REF_DIR, "libfalcon_ref_trace_d128.so"))
+
+
+def ref_inter_search_trace(vectors, links_ref, max_degree, queries, entries, ef=64, cand_queue_size=32, mc=1, mg=1,
+                           bloom_bits=16, hash_seed=1, burst=16):
+    """The reference's trace kernel (eval_trace_FPGA_inter_query_v1.3, D = 128)
+    on reference-layout data.  Returns ids, dists, hops, visited and per query
+    the lists (cand_d, cand_n, d, ids) cut from its flat -1 ... -2 streams."""
+    n, dim = vectors.shape
+    if dim != 128:
+        raise ValueError("the trace harness is built for D = 128")
+    p = os.path.join(REF_DIR, "libfalcon_ref_trace_d128.so")
+    L = ctypes.CDLL(p)
+    L.ref_inter_search_trace.restype = ctypes.c_int
+    L.ref_inter_search_trace.argtypes = [ctypes.c_int] * 6 + [ctypes.c_uint, ctypes.c_int, ctypes.c_int] + \
+        [ctypes.c_void_p] * 11
+    db = np.zeros((n, 128 + 16), dtype=np.float32)
+    db[:, :dim] = vectors
+    q = np.ascontiguousarray(queries, dtype=np.float32)
+    nq = len(q)
+    e = np.ascontiguousarray(np.broadcast_to(np.asarray(entries, dtype=np.int32), (nq,)))
+    lk = np.ascontiguousarray(links_ref, dtype=np.int32)
+    oid = np.empty((nq, ef), dtype=np.int32)
+    od = np.empty((nq, ef), dtype=np.float32)
+    dbg = np.empty((nq, 2), dtype=np.int32)
+    cap = nq * (n + 2)          # visited <= n and hops <= visited + 1 per query
+    cd = np.zeros(cap, dtype=np.float32)
+    cn = np.zeros(cap, dtype=np.int32)
+    td = np.zeros(cap, dtype=np.float32)
+    ti = np.zeros(cap, dtype=np.int32)
+    rc = L.ref_inter_search_trace(nq, ef, cand_queue_size, mc, mg, bloom_bits, hash_seed, burst, max_degree,
+                                  e.ctypes.data, q.ctypes.data, db.ctypes.data, lk.ctypes.data, oid.ctypes.data,
+                                  od.ctypes.data, dbg.ctypes.data, cd.ctypes.data, cn.ctypes.data, td.ctypes.data,
+                                  ti.ctypes.data)
+    if rc != 0:
+        raise ValueError("reference harness rejected arguments")
+
+    def split(a, b):
+        out, i = [], 0
+        for _ in range(nq):
+            assert a[i] == -1 and b[i] == -1
+            j = i + 1
+            while not (a[j] == -2 and b[j] == -2):
+                j += 1
+            out.append((a[i + 1:j].copy(), b[i + 1:j].copy()))
+            i = j + 1
+        return out
+    cand = split(cd, cn)
+    dist = split(td, ti)
+    trace = [(c[0], c[1], d_[0], d_[1]) for c, d_ in zip(cand, dist)]
+    return oid, od, dbg[:, 0].copy(), dbg[:, 1].copy(), trace
 
 
 def ref_inter_search(vectors, links_ref, max_degree, queries, entries, ef=64, cand_queue_size=32, mc=1, mg=1,

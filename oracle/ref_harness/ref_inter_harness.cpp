@@ -46,11 +46,30 @@ extern "C" int ref_max_bloom_bits(void) { return bloom_num_bucket_addr_bits; }
  * db_vectors: reference vector layout, one row = vec lines + 1 pad line
  * links:     reference link layout, one row = 1 header line + ceil(MD/16) lines
  */
+/*
+ * Built twice: from the v1.3 kernel sources (ref_inter_search), and with
+ * FALCON_REF_TRACE from eval_trace_FPGA_inter_query_v1.3/src, whose
+ * scheduler sends the popped candidate with its distance and whose
+ * results_collection also writes the traversal trace (DRAM_utils.hpp:389-474):
+ * trace_cand_d/n and trace_d/ids are flat streams, -1 before and -2 after each
+ * query; each must hold, per query, 2 markers + hops (cand) or + visited (dist).
+ */
+#ifdef FALCON_REF_TRACE
+typedef result_t top_cand_t;
+extern "C" int ref_inter_search_trace(int nq, int ef, int cand_queue_size, int mc, int mg,
+                                      int bloom_bits, unsigned hash_seed, int max_bloom_out_burst_size,
+                                      int max_link_num_base, const int *entry_ids, const float *queries,
+                                      const void *db_vectors, const void *links,
+                                      int *out_id, float *out_dist, int *mem_debug,
+                                      float *trace_cand_d, int *trace_cand_n, float *trace_d, int *trace_ids)
+#else
+typedef cand_t top_cand_t;
 extern "C" int ref_inter_search(int nq, int ef, int cand_queue_size, int mc, int mg,
                                 int bloom_bits, unsigned hash_seed, int max_bloom_out_burst_size,
                                 int max_link_num_base, const int *entry_ids, const float *queries,
                                 const void *db_vectors, const void *links,
                                 int *out_id, float *out_dist, int *mem_debug)
+#endif
 {
     if (ef > hardware_result_queue_size || cand_queue_size > hardware_candidate_queue_size ||
         bloom_bits > bloom_num_bucket_addr_bits || bloom_bits < 10)
@@ -73,14 +92,23 @@ extern "C" int ref_inter_search(int nq, int ef, int cand_queue_size, int mc, int
     hls::stream<int> s_finish_query_task_scheduler, s_finish_query_results_collection;
     hls::stream<ap_uint<512>> s_query_vectors;
     hls::stream<int> s_cand_batch_size;
-    hls::stream<cand_t> s_top_candidates;
+    hls::stream<top_cand_t> s_top_candidates;
     hls::stream<int> s_num_inserted_candidates;
     hls::stream<result_t> s_inserted_candidates;
     hls::stream<int> s_num_valid_candidates_base_level_total;
     hls::stream<result_t> s_distances_base_level;
     hls::stream<float> s_largest_result_queue_elements;
     hls::stream<int> s_debug_num_vec_base_layer;
-    hls::stream<int> s_qbs_rep[4];
+#ifdef FALCON_REF_TRACE
+    constexpr int kQbsRep = 5;   // one more for the top-candidate replication
+#else
+    constexpr int kQbsRep = 4;
+#endif
+    hls::stream<int> s_qbs_rep[kQbsRep];
+#ifdef FALCON_REF_TRACE
+    hls::stream<top_cand_t> s_top_candidates_rep[2];
+    hls::stream<int> s_finish_replicate_s_top_candidates;
+#endif
     hls::stream<int> s_num_neighbors_base_level;
     hls::stream<cand_t> s_fetched_neighbor_ids;
     hls::stream<int> s_finish_query_fetch_neighbor_ids;
@@ -120,7 +148,13 @@ extern "C" int ref_inter_search(int nq, int ef, int cand_queue_size, int mc, int
     BloomFilter<bloom_num_hash_funs, bloom_num_bucket_addr_bits> bloom(bloom_bits);
 
     std::vector<std::thread> th;
-    th.emplace_back([&] { replicate_s_query_batch_size<4>(s_query_batch_size, s_qbs_rep); });
+    th.emplace_back([&] { replicate_s_query_batch_size<kQbsRep>(s_query_batch_size, s_qbs_rep); });
+#ifdef FALCON_REF_TRACE
+    th.emplace_back([&] {
+        replicate_s_control<2, top_cand_t>(s_qbs_rep[4], s_top_candidates, s_finish_query_task_scheduler,
+                                           s_top_candidates_rep, s_finish_replicate_s_top_candidates);
+    });
+#endif
     th.emplace_back([&] {
         task_scheduler(cand_queue_size, mc, mg, s_qbs_rep[0], s_query_vectors_in, s_entry_point_ids,
                        s_num_inserted_candidates, s_inserted_candidates, s_largest_result_queue_elements,
@@ -128,8 +162,14 @@ extern "C" int ref_inter_search(int nq, int ef, int cand_queue_size, int mc, int
                        s_cand_batch_size, s_top_candidates, s_debug_signals, s_finish_query_task_scheduler);
     });
     th.emplace_back([&] {
+#ifdef FALCON_REF_TRACE
+        fetch_neighbor_ids(max_link_num_base, lk, s_qbs_rep[1], s_top_candidates_rep[0],
+                           s_finish_replicate_s_top_candidates, s_num_neighbors_base_level, s_fetched_neighbor_ids,
+                           s_finish_query_fetch_neighbor_ids);
+#else
         fetch_neighbor_ids(max_link_num_base, lk, s_qbs_rep[1], s_top_candidates, s_finish_query_task_scheduler,
                            s_num_neighbors_base_level, s_fetched_neighbor_ids, s_finish_query_fetch_neighbor_ids);
+#endif
     });
     /* bloom_fetch_compute */
     th.emplace_back([&] { replicate_s_query_batch_size<4>(s_qbs_rep[2], bfc_qbs); });
@@ -190,10 +230,18 @@ extern "C" int ref_inter_search(int nq, int ef, int cand_queue_size, int mc, int
                                    s_finish_pack, s_distances_base_level, s_finish_query_bloom_fetch_compute);
     });
     th.emplace_back([&] {
+#ifdef FALCON_REF_TRACE
+        results_collection(ef, s_qbs_rep[3], s_cand_batch_size, s_top_candidates_rep[1],
+                           s_num_valid_candidates_base_level_total, s_distances_base_level,
+                           s_finish_query_bloom_fetch_compute, trace_cand_d, trace_cand_n, trace_d, trace_ids,
+                           s_inserted_candidates, s_num_inserted_candidates, s_largest_result_queue_elements,
+                           s_debug_num_vec_base_layer, s_finish_query_results_collection, s_out_ids, s_out_dists);
+#else
         results_collection(ef, s_qbs_rep[3], s_cand_batch_size, s_num_valid_candidates_base_level_total,
                            s_distances_base_level, s_finish_query_bloom_fetch_compute, s_inserted_candidates,
                            s_num_inserted_candidates, s_largest_result_queue_elements, s_debug_num_vec_base_layer,
                            s_finish_query_results_collection, s_out_ids, s_out_dists);
+#endif
     });
 
     /* feed one batch of nq queries, then the stop token (read_queries) */
