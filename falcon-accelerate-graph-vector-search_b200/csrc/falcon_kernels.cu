@@ -1436,6 +1436,17 @@ __device__ __forceinline__ long long global_ns()
 
 // VMAX: FP32 16-byte rows per lane the server's largest dimension needs
 // (ceil(dpad/128)); only the traversal variants up to it are compiled in.
+// One request's traversal in the serving kernel.  Kept out of line so that
+// each (precision, row count) instance gets its own register allocation: the
+// serving kernel holds all of them, and inlined together they would leave no
+// room for the whole-row Bloom path.
+template <int ELEM, int EPL, int VROWS>
+__device__ __noinline__ void serve_search(const GraphView &g, const QParams &P, const QueryIO &io, uint32_t *bloom,
+                                          int *fifo, int *fifo_len, int *sids, uint64_t *hkey, int *hid, int lane)
+{
+    search_one_inter<ELEM, EPL, VROWS, kRowBloom<ELEM, VROWS>>(g, P, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+}
+
 template <int EPL, int VMAX>
 __global__ void __launch_bounds__(128, 3) serve_kernel(const ServeLaunch S)
 {
@@ -1511,15 +1522,15 @@ __global__ void __launch_bounds__(128, 3) serve_kernel(const ServeLaunch S)
         const int seg_bytes = (D.precision == kF32) ? 4 : (D.precision == kBF16 ? 2 : 1);
         const int vrows = (v.dpad * seg_bytes / 16 + 31) / 32;
         if (D.precision == kF32) {
-            if (vrows <= 1) search_one_inter<kF32, EPL, 1, false>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-            else if (VMAX >= 2 && vrows == 2) search_one_inter<kF32, EPL, (VMAX >= 2 ? 2 : 1), false>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-            else if (VMAX >= 3 && vrows == 3) search_one_inter<kF32, EPL, (VMAX >= 3 ? 3 : 1), false>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-            else if (VMAX >= 4) search_one_inter<kF32, EPL, (VMAX >= 4 ? 4 : 1), false>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            if (vrows <= 1) serve_search<kF32, EPL, 1>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            else if (VMAX >= 2 && vrows == 2) serve_search<kF32, EPL, (VMAX >= 2 ? 2 : 1)>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            else if (VMAX >= 3 && vrows == 3) serve_search<kF32, EPL, (VMAX >= 3 ? 3 : 1)>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            else if (VMAX >= 4) serve_search<kF32, EPL, (VMAX >= 4 ? 4 : 1)>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
         } else if (D.precision == kBF16) {
-            if (vrows <= 1) search_one_inter<kBF16, EPL, 1, false>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-            else if (VMAX >= 3) search_one_inter<kBF16, EPL, (VMAX >= 3 ? 2 : 1), false>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            if (vrows <= 1) serve_search<kBF16, EPL, 1>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            else if (VMAX >= 3) serve_search<kBF16, EPL, (VMAX >= 3 ? 2 : 1)>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
         } else {
-            search_one_inter<kFP8, EPL, 1, false>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+            serve_search<kFP8, EPL, 1>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
         }
         if (rerank) {
             __syncwarp();
