@@ -38,9 +38,12 @@ HNSW_M = 32
 # (ef, mc, mg, cand_queue_size, bloom_bits): the configuration's ef values with
 # the reference's 32-entry candidate queue and 2^16-bit Bloom filter, then
 # larger ef, queues and filters (a query here visits 10^4-10^5 nodes, which
-# saturates a 2^16-bit filter)
+# saturates a 2^16-bit filter; 2^19 bits keep the per-warp filters of a full
+# GPU near the L2 size at a false-positive rate that still reaches the recall
+# target)
 SWEEP = ([(ef, mc, mg, 32, 16) for ef in (64, 128, 256) for mc in (1, 2, 4) for mg in (1, 4)] +
-         [(ef, mc, 1, cq, 20) for ef in (256, 512, 1024) for cq in (64, 256) for mc in (1, 2)])
+         [(ef, mc, 1, cq, 20) for ef in (256, 512, 1024) for cq in (64, 256) for mc in (1, 2)] +
+         [(ef, 1, 1, cq, 19) for ef in (768, 896, 1024) for cq in (128, 256)])
 
 
 def log(*a):
@@ -297,7 +300,7 @@ def run_ours(args):
     from falcon_b200 import FalconIndex
     from falcon_b200.groundtruth import recall_at_k
     x, q, g, gt, upper = make_workload(rank, dev, upper_layers=True)
-    ix = FalconIndex(g, storage=("f32", "bf16"), device=local)
+    ix = FalconIndex(g, storage=("f32", "bf16", "fp8"), device=local)
     ix.set_upper_layers(upper)   # every search descends the upper layers, then searches the base layer
     if args.fixed:
         ef_, mc_, mg_, cq_, bits_ = [int(v) for v in args.fixed.split(",")]
@@ -324,8 +327,12 @@ def run_ours(args):
         torch.cuda.synchronize()
     if args.profile_region:
         torch.cuda.profiler.stop()
+        hops_p, vis_p = r.hops.cpu().numpy(), r.visited.cpu().numpy()
         print(json.dumps({"profiled_steps": args.steps, "ef": ef, "mc": mc, "mg": mg, "cq": cq,
-                          "ms_per_step": ev0.elapsed_time(ev1) / args.steps}))
+                          "ms_per_step": ev0.elapsed_time(ev1) / args.steps, "n_base": N_BASE,
+                          "queries_per_step": N_QUERIES, "hops_mean": float(hops_p.mean()),
+                          "visited_mean": float(vis_p.mean()),
+                          "bytes_per_query": algorithmic_bytes(hops_p, vis_p, ef) / N_QUERIES}))
         ix.close()
         return 0
     ms = ev0.elapsed_time(ev1)
@@ -397,6 +404,16 @@ def run_ours(args):
     torch.cuda.synchronize()
     bf_ms = a.elapsed_time(b) / 3
     bf_recall = recall_at_k(rb.ids.cpu().numpy(), gt, K)
+    # FP8 E4M3 (+ per-vector scale) traversal + exact FP32 rerank at the same point
+    rf = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, precision="fp8", rerank=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(3):
+        rf = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, precision="fp8", rerank=True)
+    b.record()
+    torch.cuda.synchronize()
+    f8_ms = a.elapsed_time(b) / 3
+    f8_recall = recall_at_k(rf.ids.cpu().numpy(), gt, K)
     served = None if args.no_serve else serve_measurements(ix, q, gt, ef, mc, mg, cq, bits,
                                                            N_QUERIES / (bf_ms / 1e3))
 
@@ -406,12 +423,16 @@ def run_ours(args):
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": None, "peak_kind": peak_kind,
             "bytes_per_query": alg / N_QUERIES, "kernel": "inter_kernel<f32>"}
+    # DRAM traffic per launch: the ratio of measured to algorithmic bytes from an
+    # ncu capture of a smaller case of the same operating point (profiles/),
+    # applied to this launch's algorithmic bytes
     tp = os.path.join(REPO, "profiles", "traffic.json")
     if os.path.exists(tp):
         tr = json.load(open(tp))
-        key = "ef%d_mc%d_mg%d" % (ef, mc, mg)
+        key = "ef%d_mc%d_mg%d_cq%d_bits%d" % (ef, mc, mg, cq, bits)
         if key in tr:
-            roof["traffic"] = tr[key]["bytes_per_query"] * N_QUERIES
+            roof["traffic"] = tr[key]["ratio"] * alg
+            roof["traffic_note"] = tr[key]["note"]
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(x, q, g, gt, ef, os.cpu_count() or 1)
@@ -431,6 +452,7 @@ def run_ours(args):
         "e2e": {"value": e2e_qps, "unit": "queries/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(q.nbytes), "d2h_bytes_per_step": int(N_QUERIES * K * 8 + N_QUERIES * 8)},
         "bf16_rerank": {"value": N_QUERIES / (bf_ms / 1e3), "unit": "queries/s", "recall@10": bf_recall},
+        "fp8_rerank": {"value": N_QUERIES / (f8_ms / 1e3), "unit": "queries/s", "recall@10": f8_recall},
         "served": served,
         "gpu_launches": 2 * args.steps,   # per step: the upper-layer descent and the base-layer search
         "clocks": clk.summary(),

@@ -8,7 +8,10 @@ measures on the device, for an index and a query sample with ground truth:
   * Bloom size: the smallest filter whose false-rejection rate at the measured
     visited count stays under `fp_target` (a query that visits V nodes sets
     ~3V bits of 2^b; a new node is wrongly rejected with probability
-    (1 - exp(-3V/2^b))^3);
+    (1 - exp(-3V/2^b))^3), and the next smaller one: filters above 2^18 bits
+    live in global memory, one per resident warp, and halving them can matter
+    more for speed (L2 footprint) than the few extra false rejections cost in
+    recall, so both are measured;
   * candidate-queue capacity and mc/mg: a grid, keeping the fastest point whose
     recall@k meets the target;
   * threads per query: inter-query (one warp) for throughput; for batch-1
@@ -80,12 +83,12 @@ def tune(index, queries, gt, dim, degree, ef_list=(64, 128, 256, 512, 1024), k=1
         # pilot at a large filter: visited count -> Bloom size
         _, r = _time_batch(index, dq, reps=1, k=k, ef=ef, cand_queue_size=min(256, max(32, ef // 4)), bloom_bits=22)
         vis = float(np.percentile(r.visited.cpu().numpy(), 90))
-        bits = bloom_bits_for(vis, fp_target)
+        bits_fp = bloom_bits_for(vis, fp_target)
         rows = []
         for cq in cq_grid:
             if cq > max(32, ef):
                 continue
-            for mc, mg in mcmg_grid:
+            for (mc, mg), bits in [(m, b) for m in mcmg_grid for b in sorted({bits_fp, max(16, bits_fp - 1)})]:
                 p = dict(k=k, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
                 ms, r = _time_batch(index, dq, **p)
                 rec = recall_at_k(r.ids.cpu().numpy(), gt, k)
