@@ -77,12 +77,6 @@ __device__ __forceinline__ int ld_nc_s32(const int32_t *p)
     return r;
 }
 
-__device__ __forceinline__ float fp8_to_f32(uint32_t byte)
-{
-    __half_raw hr = __nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)byte, __NV_E4M3);
-    return __half2float(__half(hr));
-}
-
 template <int ELEM>
 __device__ __forceinline__ void decode_seg(const uint4 raw, float scale, float (&x)[ET<ELEM>::EPS])
 {
@@ -99,11 +93,18 @@ __device__ __forceinline__ void decode_seg(const uint4 raw, float scale, float (
             x[2 * i + 1] = __uint_as_float(w[i] & 0xffff0000u);
         }
     } else {
+        // two codes per conversion (E4M3 -> f16 -> f32 is exact), then the scale
         const uint32_t w[4] = {raw.x, raw.y, raw.z, raw.w};
 #pragma unroll
         for (int i = 0; i < 4; i++) {
 #pragma unroll
-            for (int b = 0; b < 4; b++) x[4 * i + b] = __fmul_rn(fp8_to_f32((w[i] >> (8 * b)) & 0xffu), scale);
+            for (int h = 0; h < 2; h++) {
+                const __half2_raw hr =
+                    __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)((w[i] >> (16 * h)) & 0xffffu), __NV_E4M3);
+                const float2 f = __half22float2(__half2(hr));
+                x[4 * i + 2 * h] = __fmul_rn(f.x, scale);
+                x[4 * i + 2 * h + 1] = __fmul_rn(f.y, scale);
+            }
         }
     }
 }
