@@ -580,8 +580,11 @@ struct QueryIO {
     int32_t *status;
 };
 
+// Whole-row Bloom path for vectors of one register row (FP32 dim <= 128, BF16
+// <= 256, FP8 <= 512); wider vectors keep the per-32-id path, whose register
+// footprint leaves room for their extra gather rows.
 template <int ELEM, int VROWS>
-constexpr bool kRowBloom = (VROWS == 1 && ELEM != kFP8);
+constexpr bool kRowBloom = (VROWS == 1);
 
 // Traversal trace of one query (the reference's trace kernel,
 // FPGA_multi_DDR/eval_trace_FPGA_inter_query_v1.3/src/DRAM_utils.hpp:389-474,
