@@ -136,6 +136,19 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def distance_error_f64(x, q, ids, dists):
+    """Relative error of returned distances against FP64 recomputation (same
+    ids): max and mean over all valid results."""
+    ids = np.asarray(ids)
+    d = np.asarray(dists, dtype=np.float64)
+    m = ids >= 0
+    qq = np.repeat(np.arange(ids.shape[0]), ids.shape[1]).reshape(ids.shape)[m]
+    diff = x[ids[m]].astype(np.float64) - q[qq].astype(np.float64)
+    ref = (diff * diff).sum(1)
+    rel = np.abs(d[m] - ref) / np.maximum(ref, 1e-30)
+    return {"max_rel": float(rel.max()), "mean_rel": float(rel.mean())}
+
+
 def algorithmic_bytes(hops, visited, ef, elem_bytes=4, rerank=False):
     """Bytes a query must move: gathered vectors, adjacency rows (count word +
     max_degree ids per hop), the query and the k results."""
@@ -414,6 +427,14 @@ def run_ours(args):
     torch.cuda.synchronize()
     f8_ms = a.elapsed_time(b) / 3
     f8_recall = recall_at_k(rf.ids.cpu().numpy(), gt, K)
+    # distance error against FP64: after the exact FP32 rerank, and of the
+    # reduced-precision traversal distances themselves (no rerank)
+    derr = {"f32": distance_error_f64(x, q, r.ids.cpu().numpy(), r.dists.cpu().numpy())}
+    for prec, res in (("bf16", rb), ("fp8", rf)):
+        raw = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, precision=prec)
+        derr[prec + "_rerank"] = distance_error_f64(x, q, res.ids.cpu().numpy(), res.dists.cpu().numpy())
+        derr[prec + "_traversal"] = distance_error_f64(x, q, raw.ids.cpu().numpy(), raw.dists.cpu().numpy())
+        derr[prec + "_traversal"]["recall@10"] = recall_at_k(raw.ids.cpu().numpy(), gt, K)
     served = None if args.no_serve else serve_measurements(ix, q, gt, ef, mc, mg, cq, bits,
                                                            N_QUERIES / (bf_ms / 1e3))
 
@@ -453,6 +474,7 @@ def run_ours(args):
                 "h2d_bytes_per_step": int(q.nbytes), "d2h_bytes_per_step": int(N_QUERIES * K * 8 + N_QUERIES * 8)},
         "bf16_rerank": {"value": N_QUERIES / (bf_ms / 1e3), "unit": "queries/s", "recall@10": bf_recall},
         "fp8_rerank": {"value": N_QUERIES / (f8_ms / 1e3), "unit": "queries/s", "recall@10": f8_recall},
+        "distance_error_vs_f64": derr,
         "served": served,
         "gpu_launches": 2 * args.steps,   # per step: the upper-layer descent and the base-layer search
         "clocks": clk.summary(),
