@@ -254,6 +254,28 @@ def cpu_baseline(x, q, g, gt, ef, threads, budget_s=15.0):
             "recall@10": rec}
 
 
+def cpu_port(q, g, gt, ef, mc, mg, cq, bits, threads, budget_s=10.0):
+    """The C restatement of the FPGA semantics (the parity oracle: literal
+    systolic queues, Bloom filter, adder tree) timed on the host cores, on a
+    bounded sample of the same queries and parameters."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    from falcon_b200.groundtruth import recall_at_k
+    og = oracle.OracleGraph(g.vectors, g.links, g.max_degree, g.ids_offset)
+    p = oracle.make_params(k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
+    n = min(len(q), 2 * threads)
+    t = time.time()
+    oracle.search(og, q[:n], g.entry_point, p, threads=threads)
+    per_q = (time.time() - t) / n
+    n = int(min(len(q), max(n, budget_s / max(per_q, 1e-6))))
+    t = time.time()
+    ids, _, _, _, _ = oracle.search(og, q[:n], g.entry_point, p, threads=threads)
+    dt = time.time() - t
+    return {"value": n / dt, "unit": "queries/s", "cores": threads, "kind": "port",
+            "sample": "%d queries, oracle (C restatement of the FPGA traversal) at the GPU's parameters" % n,
+            "recall@10": recall_at_k(ids, gt[:n], K)}
+
+
 def run_reference(args):
     ws, rank, local = dist_env()
     if rank != 0:
@@ -454,9 +476,10 @@ def run_ours(args):
         if key in tr:
             roof["traffic"] = tr[key]["ratio"] * alg
             roof["traffic_note"] = tr[key]["note"]
-    cpu = None
+    cpu = cpu_fpga_port = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(x, q, g, gt, ef, os.cpu_count() or 1)
+        cpu_fpga_port = cpu_port(q, g, gt, ef, mc, mg, cq, bits, os.cpu_count() or 1)
     out = {
         "metric": "QPS at recall@10>=0.95 (batched search)", "value": qps, "unit": "queries/s",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
@@ -480,6 +503,7 @@ def run_ours(args):
         "clocks": clk.summary(),
         "roofline": roof,
         "cpu_baseline": cpu,
+        "cpu_fpga_semantics_port": cpu_fpga_port,
     }
     if rank == 0:
         print(json.dumps(out))
