@@ -254,6 +254,27 @@ def cpu_baseline(x, q, g, gt, ef, threads, budget_s=15.0):
             "recall@10": rec}
 
 
+def mixed_params(ix, q, steps=3):
+    """One persistent launch over queries of uneven cost: per query ef from
+    {32, 64, 128, 256}, k from {1, 10, 100} (ef raised to k), mc from {1, 2, 4},
+    the reference's 32-entry candidate queue and 2^16-bit filter; host query
+    and result buffers (copies inside the timed calls)."""
+    from falcon_b200 import make_params
+    rng = np.random.default_rng(7)
+    n = len(q)
+    efs, ks, mcs = rng.choice([32, 64, 128, 256], n), rng.choice([1, 10, 100], n), rng.choice([1, 2, 4], n)
+    per = [make_params(k=int(k), ef=int(max(e, k)), mc=int(m), mg=1, cand_queue_size=32, bloom_bits=16)
+           for e, k, m in zip(efs, ks, mcs)]
+    ix.search(q, per_query=per)
+    t = time.perf_counter()
+    for _ in range(steps):
+        r = ix.search(q, per_query=per)
+    dt = (time.perf_counter() - t) / steps
+    return {"value": n / dt, "unit": "queries/s", "queries_per_step": n, "ms_per_step": dt * 1e3,
+            "params": "ef in {32,64,128,256}, k in {1,10,100}, mc in {1,2,4} per query (seeded), cq 32, 2^16 bits",
+            "hops_mean": float(r.hops.mean()), "visited_mean": float(r.visited.mean())}
+
+
 def cpu_port(q, g, gt, ef, mc, mg, cq, bits, threads, budget_s=10.0):
     """The C restatement of the FPGA semantics (the parity oracle: literal
     systolic queues, Bloom filter, adder tree) timed on the host cores, on a
@@ -457,6 +478,7 @@ def run_ours(args):
         derr[prec + "_rerank"] = distance_error_f64(x, q, res.ids.cpu().numpy(), res.dists.cpu().numpy())
         derr[prec + "_traversal"] = distance_error_f64(x, q, raw.ids.cpu().numpy(), raw.dists.cpu().numpy())
         derr[prec + "_traversal"]["recall@10"] = recall_at_k(raw.ids.cpu().numpy(), gt, K)
+    mixed = mixed_params(ix, q)
     served = None if args.no_serve else serve_measurements(ix, q, gt, ef, mc, mg, cq, bits,
                                                            N_QUERIES / (bf_ms / 1e3))
 
@@ -498,6 +520,7 @@ def run_ours(args):
         "bf16_rerank": {"value": N_QUERIES / (bf_ms / 1e3), "unit": "queries/s", "recall@10": bf_recall},
         "fp8_rerank": {"value": N_QUERIES / (f8_ms / 1e3), "unit": "queries/s", "recall@10": f8_recall},
         "distance_error_vs_f64": derr,
+        "mixed_per_query_params": mixed,
         "served": served,
         "gpu_launches": 2 * args.steps,   # per step: the upper-layer descent and the base-layer search
         "clocks": clk.summary(),
