@@ -373,22 +373,33 @@ def run_ours(args):
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    extra = {}
+    if args.profile_region and args.profile_search == "intra":
+        extra = dict(mode="intra", channels=4)
+    elif args.profile_region and args.profile_search == "bf16_rerank":
+        extra = dict(precision="bf16", rerank=True)
+    if extra:
+        ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, **extra)
+        torch.cuda.synchronize()
     if args.profile_region:
         torch.cuda.profiler.start()
     with ClockSampler(local) as clk:
         ev0.record()
         for _ in range(args.steps):
-            r = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
+            r = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, **extra)
         ev1.record()
         torch.cuda.synchronize()
     if args.profile_region:
         torch.cuda.profiler.stop()
         hops_p, vis_p = r.hops.cpu().numpy(), r.visited.cpu().numpy()
-        print(json.dumps({"profiled_steps": args.steps, "ef": ef, "mc": mc, "mg": mg, "cq": cq,
+        print(json.dumps({"profiled_steps": args.steps, "search": args.profile_search, "ef": ef, "mc": mc, "mg": mg,
+                          "cq": cq,
                           "ms_per_step": ev0.elapsed_time(ev1) / args.steps, "n_base": N_BASE,
                           "queries_per_step": N_QUERIES, "hops_mean": float(hops_p.mean()),
                           "visited_mean": float(vis_p.mean()),
-                          "bytes_per_query": algorithmic_bytes(hops_p, vis_p, ef) / N_QUERIES}))
+                          "bytes_per_query": algorithmic_bytes(hops_p, vis_p, ef,
+                                                               elem_bytes=2 if "precision" in extra else 4,
+                                                               rerank="precision" in extra) / N_QUERIES}))
         ix.close()
         return 0
     ms = ev0.elapsed_time(ev1)
@@ -549,6 +560,9 @@ def main():
     ap.add_argument("--fixed", default=None, help="ef,mc,mg,cq,bloom_bits: skip the sweep")
     ap.add_argument("--profile-region", action="store_true",
                     help="bracket only the timed steps with cudaProfilerStart/Stop and exit after them")
+    ap.add_argument("--profile-search", default="inter", choices=["inter", "intra", "bf16_rerank"],
+                    help="with --profile-region: the search the timed steps run (inter-query FP32, intra-query "
+                         "4 channels FP32, or BF16 traversal + FP32 rerank)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
