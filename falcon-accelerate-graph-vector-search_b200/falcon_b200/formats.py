@@ -309,3 +309,76 @@ def read_fpga_upper(index_dir):
         rows[:data.shape[0], 0] = data[:, 0]
         rows[:data.shape[0], 1:] = data[:, 16:16 + max_m]
     return UpperLayers(max_level, max_m, entry, levels, row_start, rows)
+
+
+# ---------------------------------------------------------------------------
+# NSG graph files and dataset vector files read by the reference's scripts
+# ---------------------------------------------------------------------------
+
+def read_nsg_index(path, vectors):
+    """An NSG save file (the format nsg_to_FPGA.py:31-47 reads: width u32,
+    entry point u32, then per node a count u32 and that many ids u32) over
+    `vectors` as a Graph; max degree = the file's width (or the longest row)."""
+    raw = np.fromfile(path, dtype="<u4")
+    width, ep = int(raw[0]), int(raw[1])
+    n = vectors.shape[0]
+    rows, pos = [], 2
+    while pos < raw.size:
+        k = int(raw[pos])
+        rows.append(raw[pos + 1:pos + 1 + k].astype(np.int64))
+        pos += 1 + k
+    if len(rows) != n:
+        raise ValueError("%s holds %d rows for %d vectors" % (path, len(rows), n))
+    md = max(width, max((len(r) for r in rows), default=0))
+    adj = np.full((n, md), -1, dtype=np.int32)
+    for i, r in enumerate(rows):
+        adj[i, :len(r)] = r
+    return Graph.from_adjacency(vectors, adj, ep)
+
+
+def write_nsg_index(path, graph):
+    """Write `graph` as an NSG save file (width = max degree)."""
+    adj = graph.adjacency()
+    out = [np.array([graph.max_degree, graph.entry_point], dtype="<u4")]
+    for row in adj:
+        r = row[row >= 0]
+        out.append(np.array([len(r)], dtype="<u4"))
+        out.append(r.astype("<u4"))
+    np.concatenate(out).tofile(path)
+
+
+def read_fvecs(path):
+    """TEXMEX .fvecs: per row an int32 dimension, then that many float32."""
+    a = np.fromfile(path, dtype="<i4")
+    d = int(a[0])
+    return a.reshape(-1, d + 1)[:, 1:].view("<f4").copy()
+
+
+def read_ivecs(path):
+    """TEXMEX .ivecs (ground-truth ids): per row an int32 count, then int32 ids."""
+    a = np.fromfile(path, dtype="<i4")
+    d = int(a[0])
+    return a.reshape(-1, d + 1)[:, 1:].copy()
+
+
+def read_bvecs(path):
+    """TEXMEX .bvecs (SIFT1B): per row an int32 dimension, then uint8 values; as float32."""
+    a = np.fromfile(path, dtype=np.uint8)
+    d = int(a[:4].view("<i4")[0])
+    return a.reshape(-1, d + 4)[:, 4:].astype(np.float32)
+
+
+def read_bin(path, dtype="<f4"):
+    """big-ann-benchmarks .fbin / .ibin / .u8bin: n u32, dim u32, then n x dim values."""
+    n, d = (int(v) for v in np.fromfile(path, dtype="<u4", count=2))
+    return np.fromfile(path, dtype=dtype, offset=8).reshape(n, d)
+
+
+def write_vecs(path, array):
+    """Write a TEXMEX .fvecs (float32), .ivecs (int32) or .bvecs (uint8) file by the array's dtype."""
+    a = np.ascontiguousarray(array)
+    n, d = a.shape
+    with open(path, "wb") as f:
+        for row in a:
+            f.write(np.int32(d).tobytes())
+            f.write(row.tobytes())
