@@ -444,20 +444,27 @@ def run_ours(args):
         lat.append(a.elapsed_time(b))
     lat = np.array(lat[10:])
     # the same batch-1 latency in intra-query mode (one block of channel warps per query)
+    # In intra-query mode each channel's filter sees 1/channels of the ids, so
+    # bits - log2(channels) + 1 per channel keeps the false-rejection rate of the
+    # whole-query filter; up to 2^18 bits it lives in shared memory.
+    from falcon_b200.autotune import channel_bloom_bits
     lat_intra = {}
     for ch in (4, 8):
+        cbits = channel_bloom_bits(bits, ch)
+        pi = dict(k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=cbits, mode="intra", channels=ch)
+        ri = ix.search(dq, **pi)
         li = []
         for i in range(min(300, N_QUERIES)):
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record()
-            ix.search(dq[i:i + 1], k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, mode="intra",
-                      channels=ch)
+            ix.search(dq[i:i + 1], **pi)
             b.record()
             b.synchronize()
             li.append(a.elapsed_time(b))
         li = np.array(li[10:])
-        lat_intra[ch] = (float(np.percentile(li, 50)), float(np.percentile(li, 99)))
+        lat_intra[ch] = (float(np.percentile(li, 50)), float(np.percentile(li, 99)), cbits,
+                         recall_at_k(ri.ids.cpu().numpy(), gt, K))
 
     # BF16 + exact FP32 rerank at the same point
     rb = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, precision="bf16", rerank=True)
@@ -525,7 +532,8 @@ def run_ours(args):
                    "sweep": [{k2: (round(v, 4) if isinstance(v, float) else v) for k2, v in s.items()} for s in table]},
         "latency_ms": {"batch": 1, "p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "samples": int(len(lat)), "timer": "CUDA events around one search call", "mode": "inter",
-                       "intra": {("channels_%d" % c): {"p50": v[0], "p99": v[1]} for c, v in lat_intra.items()}},
+                       "intra": {("channels_%d" % c): {"p50": v[0], "p99": v[1], "bloom_bits_per_channel": v[2],
+                                                       "recall@10": v[3]} for c, v in lat_intra.items()}},
         "e2e": {"value": e2e_qps, "unit": "queries/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(q.nbytes), "d2h_bytes_per_step": int(N_QUERIES * K * 8 + N_QUERIES * 8)},
         "bf16_rerank": {"value": N_QUERIES / (bf_ms / 1e3), "unit": "queries/s", "recall@10": bf_recall},

@@ -15,7 +15,8 @@ measures on the device, for an index and a query sample with ground truth:
   * candidate-queue capacity and mc/mg: a grid, keeping the fastest point whose
     recall@k meets the target;
   * threads per query: inter-query (one warp) for throughput; for batch-1
-    latency, intra-query blocks of 4 or 8 channel warps are timed as well.
+    latency, intra-query blocks of 4 or 8 channel warps are timed as well, each
+    channel with a filter sized for the ids it sees (channel_bloom_bits).
 
 Profiles are JSON files keyed "D{dim}_R{degree}_ef{ef}".
 """
@@ -33,6 +34,14 @@ def bloom_bits_for(visited, fp_target=0.01, lo=16, hi=24):
         if (1.0 - math.exp(-3.0 * v / (1 << b))) ** 3 <= fp_target:
             return b
     return hi
+
+
+def channel_bloom_bits(bits, channels, smem_max=18):
+    """Per-channel filter size in intra-query mode: each channel's filter sees
+    1/channels of the ids, so bits - log2(channels) + 1 keeps (with a bit to
+    spare) the false-rejection rate of a `bits` whole-query filter; capped at
+    the largest shared-memory filter, 2^18 bits."""
+    return max(10, min(smem_max, bits - int(round(math.log2(channels))) + 1))
 
 
 def _time_batch(ix, dq, reps=2, **p):
@@ -101,13 +110,16 @@ def tune(index, queries, gt, dim, degree, ef_list=(64, 128, 256, 512, 1024), k=1
         params = {kk: best[kk] for kk in ("k", "ef", "mc", "mg", "cand_queue_size", "bloom_bits")}
         lat = {"inter": _time_single(index, dq, **params)}
         for ch in latency_channels:
-            lat["intra_%d" % ch] = _time_single(index, dq, mode="intra", channels=ch, **params)
+            pc = dict(params, bloom_bits=channel_bloom_bits(params["bloom_bits"], ch))
+            lat["intra_%d" % ch] = _time_single(index, dq, mode="intra", channels=ch, **pc)
         fastest = min(lat, key=lat.get)
         prof[profile_key(dim, degree, ef)] = {
             "throughput": {"params": dict(params, mode="inter"), "qps": best["qps"], "recall": best["recall"]},
             "latency": {"threads_per_query": 32 if fastest == "inter" else 32 * int(fastest.split("_")[1]),
                         "mode": "inter" if fastest == "inter" else "intra",
                         "channels": None if fastest == "inter" else int(fastest.split("_")[1]),
+                        "bloom_bits": params["bloom_bits"] if fastest == "inter" else
+                        channel_bloom_bits(params["bloom_bits"], int(fastest.split("_")[1])),
                         "median_ms": lat},
             "visited_p90": vis, "recall_target_met": bool(ok), "grid": rows,
         }
@@ -151,4 +163,6 @@ def pick(profile, dim, degree, ef, objective="throughput"):
     p["mode"] = lat["mode"]
     if lat["channels"]:
         p["channels"] = lat["channels"]
+    if lat.get("bloom_bits"):
+        p["bloom_bits"] = lat["bloom_bits"]
     return p

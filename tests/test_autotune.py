@@ -60,3 +60,21 @@ def test_tune_small_index():
             assert t["recall"] >= 0.9
         assert e["latency"]["mode"] in ("inter", "intra")
     assert prof["D96_R64_ef128"]["throughput"]["recall"] >= prof["D96_R64_ef32"]["throughput"]["recall"]
+
+
+def test_channel_bloom_bits():
+    """Each intra-query channel sees 1/channels of the ids: a filter of
+    bits - log2(channels) + 1 has at most the whole-query false-rejection rate;
+    shared-memory filters stop at 2^18 bits."""
+    import math
+    from falcon_b200.autotune import channel_bloom_bits
+    assert channel_bloom_bits(19, 4) == 18 and channel_bloom_bits(19, 8) == 17 and channel_bloom_bits(22, 2) == 18
+    assert channel_bloom_bits(16, 1) == 17 - 0 - 0 and channel_bloom_bits(10, 8) == 10
+    for bits in range(14, 21):
+        for ch in (2, 4, 8):
+            v = 0.3 * (1 << bits) / 3        # visited ids filling ~26 % of the whole-query filter
+            whole = (1 - math.exp(-3 * v / (1 << bits))) ** 3
+            b = channel_bloom_bits(bits, ch)
+            if b < 18:
+                per = (1 - math.exp(-3 * (v / ch) / (1 << b))) ** 3
+                assert per <= whole
