@@ -371,21 +371,18 @@ int falcon_server_submit(falcon_server *sv, int32_t n, const int32_t *index_ids,
     return rc != FALCON_OK ? rc : admitted;
 }
 
-int falcon_server_poll(falcon_server *sv, int64_t request_id, int32_t *out_ids, float *out_dists, int32_t *hops,
-                       int32_t *visited)
+}  // extern "C"
+
+namespace {
+// Collect one request if its done word is set (the lock is held): 1 done,
+// 0 pending, < 0 error.  No CUDA call.
+int collect_locked(falcon_server *sv, unsigned long long seq, int32_t *out_ids, float *out_dists, int32_t *hops,
+                   int32_t *visited)
 {
-    if (!sv || request_id < 0) return set_error_code(FALCON_ERR_ARG, "falcon_server_poll: bad argument");
-    const unsigned long long seq = (unsigned long long)request_id;
     const int e = (int)(seq % (unsigned long long)sv->cap);
-    std::lock_guard<std::mutex> lock(sv->mu);
     if (sv->entry_seq[e] != seq) return set_error_code(FALCON_ERR_ARG, "unknown or already collected request");
     const unsigned long long d = *reinterpret_cast<volatile unsigned long long *>(sv->h_done + e);
-    if (d != seq + 1) {
-        // the kernel may have left on idleness just before this request was published
-        cudaSetDevice(sv->device);
-        const int rc = ensure_running(sv);
-        return rc != FALCON_OK ? rc : 0;
-    }
+    if (d != seq + 1) return 0;
     std::atomic_thread_fence(std::memory_order_acquire);
     const int k = sv->entry_k[e];
     if (out_ids) memcpy(out_ids, sv->h_out_ids + (size_t)e * sv->cfg.max_k, sizeof(int32_t) * k);
@@ -395,6 +392,24 @@ int falcon_server_poll(falcon_server *sv, int64_t request_id, int32_t *out_ids, 
     sv->entry_seq[e] = ~0ull;
     sv->in_flight--;
     return 1;
+}
+}  // namespace
+
+extern "C" {
+
+int falcon_server_poll(falcon_server *sv, int64_t request_id, int32_t *out_ids, float *out_dists, int32_t *hops,
+                       int32_t *visited)
+{
+    if (!sv || request_id < 0) return set_error_code(FALCON_ERR_ARG, "falcon_server_poll: bad argument");
+    std::lock_guard<std::mutex> lock(sv->mu);
+    const int rc = collect_locked(sv, (unsigned long long)request_id, out_ids, out_dists, hops, visited);
+    if (rc == 0) {
+        // the kernel may have left on idleness just before this request was published
+        cudaSetDevice(sv->device);
+        const int lr = ensure_running(sv);
+        return lr != FALCON_OK ? lr : 0;
+    }
+    return rc;
 }
 
 int falcon_server_wait(falcon_server *sv, int64_t request_id, int64_t timeout_us, int32_t *out_ids,
@@ -441,22 +456,32 @@ int falcon_server_replay(falcon_server *sv, int32_t n, const int32_t *index_ids,
             for (int i = 0; i < rc; i++) pending.push_back(next + i);
             next += rc;
         }
-        // collect completions
-        for (size_t j = 0; j < pending.size();) {
-            const int i = pending[j];
-            int32_t h = 0, v = 0;
-            const int rc = falcon_server_poll(sv, rid[i], out_ids ? out_ids + (size_t)i * out_stride : tmp_ids.data(),
+        // collect completions: one lock and no CUDA call per pass; the kernel is
+        // relaunched (if it left on idleness) at most once per pass
+        {
+            std::lock_guard<std::mutex> lock(sv->mu);
+            for (size_t j = 0; j < pending.size();) {
+                const int i = pending[j];
+                int32_t h = 0, v = 0;
+                const int rc = collect_locked(sv, (unsigned long long)rid[i],
+                                              out_ids ? out_ids + (size_t)i * out_stride : tmp_ids.data(),
                                               out_dists ? out_dists + (size_t)i * out_stride : tmp_d.data(), &h, &v);
-            if (rc < 0) return rc;
-            if (rc == 1) {
-                latency_us[i] = now_us() - arrival_us[i];
-                if (hops) hops[i] = h;
-                if (visited) visited[i] = v;
-                pending[j] = pending.back();
-                pending.pop_back();
-                done++;
-            } else {
-                j++;
+                if (rc < 0) return rc;
+                if (rc == 1) {
+                    latency_us[i] = now_us() - arrival_us[i];
+                    if (hops) hops[i] = h;
+                    if (visited) visited[i] = v;
+                    pending[j] = pending.back();
+                    pending.pop_back();
+                    done++;
+                } else {
+                    j++;
+                }
+            }
+            if (!pending.empty()) {
+                cudaSetDevice(sv->device);
+                const int lr = ensure_running(sv);
+                if (lr != FALCON_OK) return lr;
             }
         }
         if (pending.empty() && next < n) {   // idle until the next arrival
