@@ -131,12 +131,31 @@ struct ServeDesc {
     QParams p;
 };
 
+// Serving kernels are specialised per request class, the traversal precision
+// and the 16-byte register rows per lane its vectors take: FP32 1..4, BF16
+// 1..2, FP8 1.  One kernel holding several traversal variants (called or
+// inlined) spills inside the hop loop, so each class has its own kernel and
+// its own claim queue, and the host runs one class kernel at a time.
+constexpr int kServeClasses = 7;
+
+__host__ __device__ constexpr int serve_class(int precision, int vrows)
+{
+    return precision == kF32 ? vrows - 1 : (precision == kBF16 ? 3 + vrows : 6);
+}
+
+// 16-byte register rows per lane of a padded dimension at a precision.
+__host__ __device__ constexpr int serve_vrows(int dpad, int precision)
+{
+    return (dpad * (precision == kF32 ? 4 : (precision == kBF16 ? 2 : 1)) / 16 + 31) / 32;
+}
+
 struct ServeCtl {
-    unsigned long long head;        // requests claimed by warps
-    unsigned long long tail;        // requests published by the host
+    unsigned long long head[kServeClasses];   // per class queue: requests claimed by warps
+    unsigned long long tail[kServeClasses];   // per class queue: requests published by the host
     long long last_active_ns;       // last claim or completion (globaltimer)
     int32_t stop;                   // host: leave when idle
     int32_t error;
+    uint32_t yield_epoch;           // host: the launch with this epoch leaves between requests
 };
 
 struct ServeLaunch {
@@ -144,6 +163,8 @@ struct ServeLaunch {
     int32_t nviews;
     const ServeDesc *ring;
     int32_t ring_cap;
+    const int32_t *class_slots;     // kServeClasses x ring_cap: ring entries in each class's claim order
+    const uint32_t *run_epoch;      // host-mapped: epoch of the current launch, read once at start
     const float *qpool;             // ring_cap x qstride (device)
     int32_t qstride;
     int32_t *out_ids;               // ring_cap x out_stride (host-mapped)
@@ -171,9 +192,9 @@ __host__ __device__ inline size_t serve_warp_smem_bytes(int bloom_bits_max, int 
     return (b + 15) & ~(size_t)15;
 }
 
-// Serving kernel launch configuration for entries-per-lane `epl` (8 or 32).
-cudaError_t serve_config(const ServeLaunch &s, int epl, int vmax, int num_sms, int *grid, size_t *smem);
-cudaError_t launch_serve(const ServeLaunch &s, int epl, int vmax, int grid, size_t smem, cudaStream_t st);
+// Serving kernel of request class `cls` for entries-per-lane `epl` (8 or 32).
+cudaError_t serve_config(const ServeLaunch &s, int epl, int cls, int num_sms, int *grid, size_t *smem);
+cudaError_t launch_serve(const ServeLaunch &s, int epl, int cls, int grid, size_t smem, cudaStream_t st);
 
 // A validated search request (host side), used by falcon_search_noalloc.
 struct SearchPlan {

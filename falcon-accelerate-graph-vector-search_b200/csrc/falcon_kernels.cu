@@ -1414,15 +1414,18 @@ __global__ void __launch_bounds__(128) rerank_kernel(const RerankLaunch A)
 
 // ---------------------------------------------------------------------------
 // Serving kernel: a persistent grid whose warps pull requests one at a time
-// from a device ring that the host keeps appending to while the kernel runs
-// (continuous batching: a request admitted while others are in flight starts
-// as soon as a warp is free).  A request names a resident index, its
-// precision and its own k/ef/mc/mg; results, hops and visited go to
-// host-mapped memory, then a per-entry done word (seq + 1) is released to the
-// host.  Claiming uses compare-and-swap so no request is ever claimed before
-// it is published.  Every wait is bounded: a warp that finds no work sleeps
-// and leaves after `idle_ns` of idleness (or at once when `stop` is set); the
-// host relaunches the kernel when new work arrives.
+// from the claim queue of one request class (precision x register rows),
+// which the host keeps appending to while the kernel runs (continuous
+// batching: a request admitted while others are in flight starts as soon as
+// a warp is free).  A request names a resident index, its precision and its
+// own k/ef/mc/mg; results, hops and visited go to host-mapped memory, then a
+// per-entry done word (seq + 1) is released to the host.  Claiming uses
+// compare-and-swap so no request is ever claimed before it is published.
+// Every wait is bounded: a warp that finds no work sleeps and leaves after
+// `idle_ns` of idleness (or at once when `stop` is set), and every warp
+// leaves between requests once the host sets yield_epoch to this launch's
+// epoch (another class is waiting); the host relaunches a class kernel when
+// work is waiting.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ unsigned long long load_acquire_u64(const unsigned long long *p)
 {
@@ -1438,23 +1441,43 @@ __device__ __forceinline__ long long global_ns()
     return t;
 }
 
-// VMAX: FP32 16-byte rows per lane the server's largest dimension needs
-// (ceil(dpad/128)); only the traversal variants up to it are compiled in.
-// One request's traversal in the serving kernel.  Kept out of line so that
-// each (precision, row count) instance gets its own register allocation: the
-// serving kernel holds all of them, and inlined together they would leave no
-// room for the whole-row Bloom path.
-template <int ELEM, int EPL, int VROWS>
-__device__ __noinline__ void serve_search(const GraphView &g, const QParams &P, const QueryIO &io, uint32_t *bloom,
-                                          int *fifo, int *fifo_len, int *sids, uint64_t *hkey, int *hid, int lane)
+// Exact FP32 rerank of a served request's ef candidates (the warp's scratch
+// row).  Everything it needs is reloaded from the ring entry, so nothing of
+// the request stays live in registers through the traversal.  FP32 rows:
+// BF16 one row -> 1..2, BF16 two rows -> 3..4, FP8 -> 1..4.
+template <int ELEM, int VROWS>
+__device__ __forceinline__ void serve_rerank(const ServeLaunch &S, int e, float *rsd, int *rsi, int lane)
 {
-    search_one_inter<ELEM, EPL, VROWS, kRowBloom<ELEM, VROWS>>(g, P, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
+    ServeDesc D;
+    {
+        const int *src = reinterpret_cast<const int *>(S.ring + e);
+        int *dst = reinterpret_cast<int *>(&D);
+#pragma unroll
+        for (int w = 0; w < (int)(sizeof(ServeDesc) / sizeof(int)); w++) dst[w] = __ldcg(src + w);
+    }
+    const GraphView &v = S.views[D.index];
+    const int32_t *cand_ids = S.cand_ids + ((size_t)blockIdx.x * 4 + (threadIdx.x >> 5)) * S.ef_max;
+    const float *query = S.qpool + (int64_t)e * S.qstride;
+    int32_t *orow = S.out_ids + (int64_t)e * S.out_stride;
+    float *drow = S.out_d + (int64_t)e * S.out_stride;
+    const int vr32 = serve_vrows(v.dpad, kF32);
+    if ((ELEM == kFP8 || VROWS == 1) && vr32 <= 1)
+        rerank_one<1>(v, D.p, query, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
+    else if ((ELEM == kFP8 || VROWS == 1) && vr32 == 2)
+        rerank_one<2>(v, D.p, query, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
+    else if ((ELEM == kFP8 || VROWS == 2) && vr32 == 3)
+        rerank_one<3>(v, D.p, query, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
+    else if (ELEM == kFP8 || VROWS == 2)
+        rerank_one<4>(v, D.p, query, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
 }
 
-template <int EPL, int VMAX>
+// One serving kernel per request class (precision ELEM, VROWS register rows):
+// a single traversal variant per kernel keeps the hop loop free of spills.
+template <int ELEM, int EPL, int VROWS>
 __global__ void __launch_bounds__(128, 3) serve_kernel(const ServeLaunch S)
 {
     extern __shared__ uint4 smem_u4[];
+    constexpr int CLS = serve_class(ELEM, VROWS);
     constexpr int HEAP_CAP = (EPL > 8) ? 32 * EPL : 0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const size_t wbytes = serve_warp_smem_bytes(S.bloom_bits_max, S.mc_max, S.mg_max, HEAP_CAP, S.ef_max);
@@ -1478,18 +1501,25 @@ __global__ void __launch_bounds__(128, 3) serve_kernel(const ServeLaunch S)
     const size_t gw = (size_t)blockIdx.x * 4 + warp;
     int32_t *cand_ids = S.cand_ids + gw * S.ef_max;
     float *cand_d = S.cand_d + gw * S.ef_max;
+    const int32_t *slots = S.class_slots + (size_t)CLS * S.ring_cap;
+    uint32_t epoch = 0;
+    if (lane == 0) epoch = *reinterpret_cast<const volatile uint32_t *>(S.run_epoch);
 
     for (;;) {
         unsigned long long h = ~0ull;
+        int yielded = 0;
         if (lane == 0) {
-            for (int tries = 0; tries < 256; tries++) {
-                const unsigned long long hd = atomicAdd(&S.ctl->head, 0ull);
-                const unsigned long long tl = load_acquire_u64(&S.ctl->tail);
+            // the host hands the GPU to another class: leave between requests
+            yielded = *reinterpret_cast<volatile uint32_t *>(&S.ctl->yield_epoch) == epoch;
+            for (int tries = 0; !yielded && tries < 256; tries++) {
+                const unsigned long long hd = atomicAdd(&S.ctl->head[CLS], 0ull);
+                const unsigned long long tl = load_acquire_u64(&S.ctl->tail[CLS]);
                 if (hd >= tl) break;
-                if (atomicCAS(&S.ctl->head, hd, hd + 1) == hd) { h = hd; break; }
+                if (atomicCAS(&S.ctl->head[CLS], hd, hd + 1) == hd) { h = hd; break; }
             }
             if (h != ~0ull) atomicMax(&S.ctl->last_active_ns, global_ns());
         }
+        if (__shfl_sync(kFull, yielded, 0)) break;
         h = __shfl_sync(kFull, h, 0);
         if (h == ~0ull) {
             // leave only when the whole server has been idle for idle_ns
@@ -1503,7 +1533,7 @@ __global__ void __launch_bounds__(128, 3) serve_kernel(const ServeLaunch S)
             __nanosleep(1000);
             continue;
         }
-        const int e = (int)(h % (unsigned long long)S.ring_cap);
+        const int e = __ldcg(slots + (int)(h % (unsigned long long)S.ring_cap));
         ServeDesc D;
         {
             const int *src = reinterpret_cast<const int *>(S.ring + e);
@@ -1512,7 +1542,7 @@ __global__ void __launch_bounds__(128, 3) serve_kernel(const ServeLaunch S)
             for (int w = 0; w < (int)(sizeof(ServeDesc) / sizeof(int)); w++) dst[w] = __ldcg(src + w);
         }
         const GraphView &v = S.views[D.index];
-        const bool rerank = D.p.rerank != 0 && D.precision != kF32;
+        const bool rerank = ELEM != kF32 && D.p.rerank != 0;
         QueryIO io;
         io.query = S.qpool + (int64_t)e * S.qstride;
         io.entry = D.entry;
@@ -1523,28 +1553,13 @@ __global__ void __launch_bounds__(128, 3) serve_kernel(const ServeLaunch S)
         io.hops = S.out_hops + e;
         io.visited = S.out_visited + e;
         io.status = S.status;
-        const int seg_bytes = (D.precision == kF32) ? 4 : (D.precision == kBF16 ? 2 : 1);
-        const int vrows = (v.dpad * seg_bytes / 16 + 31) / 32;
-        if (D.precision == kF32) {
-            if (vrows <= 1) serve_search<kF32, EPL, 1>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-            else if (VMAX >= 2 && vrows == 2) serve_search<kF32, EPL, (VMAX >= 2 ? 2 : 1)>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-            else if (VMAX >= 3 && vrows == 3) serve_search<kF32, EPL, (VMAX >= 3 ? 3 : 1)>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-            else if (VMAX >= 4) serve_search<kF32, EPL, (VMAX >= 4 ? 4 : 1)>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-        } else if (D.precision == kBF16) {
-            if (vrows <= 1) serve_search<kBF16, EPL, 1>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-            else if (VMAX >= 3) serve_search<kBF16, EPL, (VMAX >= 3 ? 2 : 1)>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-        } else {
-            serve_search<kFP8, EPL, 1>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid, lane);
-        }
-        if (rerank) {
-            __syncwarp();
-            const int vr32 = (v.dpad * 4 / 16 + 31) / 32;
-            int32_t *orow = S.out_ids + (int64_t)e * S.out_stride;
-            float *drow = S.out_d + (int64_t)e * S.out_stride;
-            if (vr32 <= 1) rerank_one<1>(v, D.p, io.query, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
-            else if (VMAX >= 2 && vr32 == 2) rerank_one<(VMAX >= 2 ? 2 : 1)>(v, D.p, io.query, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
-            else if (VMAX >= 3 && vr32 == 3) rerank_one<(VMAX >= 3 ? 3 : 1)>(v, D.p, io.query, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
-            else if (VMAX >= 4) rerank_one<(VMAX >= 4 ? 4 : 1)>(v, D.p, io.query, cand_ids, orow, drow, S.out_stride, rsd, rsi, lane);
+        search_one_inter<ELEM, EPL, VROWS, kRowBloom<ELEM, VROWS>>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid,
+                                                                   lane);
+        if constexpr (ELEM != kF32) {
+            if (rerank) {
+                __syncwarp();
+                serve_rerank<ELEM, VROWS>(S, e, rsd, rsi, lane);
+            }
         }
         __syncwarp();
         if (lane == 0) {
@@ -1731,15 +1746,16 @@ cudaError_t search_bloom_slots(const SearchLaunch &a, int elem, int num_sms, int
     return search_dispatch(a, elem, num_sms, nullptr, slots);
 }
 
-template <int EPL, int VMAX>
+template <int ELEM, int EPL, int VROWS>
 static cudaError_t serve_config_t(const ServeLaunch &sv, int num_sms, int *grid, size_t *smem)
 {
     const int heap_cap = (EPL > 8) ? 32 * EPL : 0;
     *smem = serve_warp_smem_bytes(sv.bloom_bits_max, sv.mc_max, sv.mg_max, heap_cap, sv.ef_max) * 4;
-    cudaError_t e = cudaFuncSetAttribute(serve_kernel<EPL, VMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(serve_kernel<ELEM, EPL, VROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)*smem);
     int per_sm = 0;
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel<EPL, VMAX>, 128, *smem);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel<ELEM, EPL, VROWS>, 128, *smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     *grid = per_sm * num_sms;
@@ -1747,41 +1763,47 @@ static cudaError_t serve_config_t(const ServeLaunch &sv, int num_sms, int *grid,
 }
 
 template <int EPL>
-static cudaError_t serve_config_v(const ServeLaunch &sv, int vmax, int num_sms, int *grid, size_t *smem)
+static cudaError_t serve_config_c(const ServeLaunch &sv, int cls, int num_sms, int *grid, size_t *smem)
 {
-    switch (vmax) {
-        case 1: return serve_config_t<EPL, 1>(sv, num_sms, grid, smem);
-        case 2: return serve_config_t<EPL, 2>(sv, num_sms, grid, smem);
-        case 3: return serve_config_t<EPL, 3>(sv, num_sms, grid, smem);
-        case 4: return serve_config_t<EPL, 4>(sv, num_sms, grid, smem);
+    switch (cls) {
+        case serve_class(kF32, 1): return serve_config_t<kF32, EPL, 1>(sv, num_sms, grid, smem);
+        case serve_class(kF32, 2): return serve_config_t<kF32, EPL, 2>(sv, num_sms, grid, smem);
+        case serve_class(kF32, 3): return serve_config_t<kF32, EPL, 3>(sv, num_sms, grid, smem);
+        case serve_class(kF32, 4): return serve_config_t<kF32, EPL, 4>(sv, num_sms, grid, smem);
+        case serve_class(kBF16, 1): return serve_config_t<kBF16, EPL, 1>(sv, num_sms, grid, smem);
+        case serve_class(kBF16, 2): return serve_config_t<kBF16, EPL, 2>(sv, num_sms, grid, smem);
+        case serve_class(kFP8, 1): return serve_config_t<kFP8, EPL, 1>(sv, num_sms, grid, smem);
     }
     return cudaErrorInvalidValue;
 }
 
-cudaError_t serve_config(const ServeLaunch &sv, int epl, int vmax, int num_sms, int *grid, size_t *smem)
+cudaError_t serve_config(const ServeLaunch &sv, int epl, int cls, int num_sms, int *grid, size_t *smem)
 {
-    if (epl == 8) return serve_config_v<8>(sv, vmax, num_sms, grid, smem);
-    if (epl == 32) return serve_config_v<32>(sv, vmax, num_sms, grid, smem);
+    if (epl == 8) return serve_config_c<8>(sv, cls, num_sms, grid, smem);
+    if (epl == 32) return serve_config_c<32>(sv, cls, num_sms, grid, smem);
     return cudaErrorInvalidValue;
 }
 
 template <int EPL>
-static cudaError_t launch_serve_v(const ServeLaunch &sv, int vmax, int grid, size_t smem, cudaStream_t st)
+static cudaError_t launch_serve_c(const ServeLaunch &sv, int cls, int grid, size_t smem, cudaStream_t st)
 {
-    switch (vmax) {
-        case 1: serve_kernel<EPL, 1><<<grid, 128, smem, st>>>(sv); break;
-        case 2: serve_kernel<EPL, 2><<<grid, 128, smem, st>>>(sv); break;
-        case 3: serve_kernel<EPL, 3><<<grid, 128, smem, st>>>(sv); break;
-        case 4: serve_kernel<EPL, 4><<<grid, 128, smem, st>>>(sv); break;
+    switch (cls) {
+        case serve_class(kF32, 1): serve_kernel<kF32, EPL, 1><<<grid, 128, smem, st>>>(sv); break;
+        case serve_class(kF32, 2): serve_kernel<kF32, EPL, 2><<<grid, 128, smem, st>>>(sv); break;
+        case serve_class(kF32, 3): serve_kernel<kF32, EPL, 3><<<grid, 128, smem, st>>>(sv); break;
+        case serve_class(kF32, 4): serve_kernel<kF32, EPL, 4><<<grid, 128, smem, st>>>(sv); break;
+        case serve_class(kBF16, 1): serve_kernel<kBF16, EPL, 1><<<grid, 128, smem, st>>>(sv); break;
+        case serve_class(kBF16, 2): serve_kernel<kBF16, EPL, 2><<<grid, 128, smem, st>>>(sv); break;
+        case serve_class(kFP8, 1): serve_kernel<kFP8, EPL, 1><<<grid, 128, smem, st>>>(sv); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
 
-cudaError_t launch_serve(const ServeLaunch &sv, int epl, int vmax, int grid, size_t smem, cudaStream_t st)
+cudaError_t launch_serve(const ServeLaunch &sv, int epl, int cls, int grid, size_t smem, cudaStream_t st)
 {
-    if (epl == 8) return launch_serve_v<8>(sv, vmax, grid, smem, st);
-    if (epl == 32) return launch_serve_v<32>(sv, vmax, grid, smem, st);
+    if (epl == 8) return launch_serve_c<8>(sv, cls, grid, smem, st);
+    if (epl == 32) return launch_serve_c<32>(sv, cls, grid, smem, st);
     return cudaErrorInvalidValue;
 }
 

@@ -2,11 +2,18 @@
 // device-resident indexes.
 //
 // The host appends requests to a device ring (descriptor + query vector,
-// copied on a copy stream, then the ring's tail counter); a persistent
-// serve_kernel (falcon_kernels.cu) whose launch is captured once in a CUDA
-// graph pulls them one at a time, so a request admitted while others are on
-// the GPU starts as soon as a warp frees up and its work overlaps theirs.
-// Each request carries its own index, precision, k, ef, mc, mg (mixed freely).
+// copied on a copy stream) and each ring entry to the claim queue of its
+// class (traversal precision x register rows, falcon_internal.h), then
+// publishes the queues' tail counters.  A persistent serve_kernel
+// (falcon_kernels.cu) specialised for one class, its launch captured once in
+// a CUDA graph, pulls that class's requests one at a time, so a request
+// admitted while others are on the GPU starts as soon as a warp frees up and
+// its work overlaps theirs.  Each request carries its own index, precision,
+// k, ef, mc, mg (mixed freely).  One class kernel runs at a time; while
+// another class has requests waiting, the running kernel is asked to yield
+// (its warps leave between requests) once its class has nothing uncollected
+// or it has run for kClassSliceUs, and the next class with work (round
+// robin) is launched.
 // Results go to host-mapped memory and complete with a per-entry done word,
 // so the host collects them without any CUDA call.  The ring's size is
 // chosen from the free device memory at creation (admission by memory): a
@@ -37,19 +44,26 @@ int check_search_params(const falcon_search_params &p, const falcon_index *ix, i
 
 struct falcon_server {
     falcon_server_config cfg;
-    int device = 0, num_sms = 0, epl = 8, vmax = 1, grid = 0;
-    size_t smem = 0;
+    int device = 0, num_sms = 0, epl = 8, vmax = 1, max_grid = 0;
+    int grid[kServeClasses] = {};
+    size_t smem[kServeClasses] = {};
+    bool class_ok[kServeClasses] = {};   // compiled for this server's dim_max
     int cap = 0;                          // ring entries
     int qstride = 0;                      // floats per query slot
     std::mutex mu;
     cudaStream_t kstream = nullptr, cstream = nullptr;
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph[kServeClasses] = {};
     cudaEvent_t kernel_done = nullptr;
     bool launched = false;
     int64_t launches = 0;
+    int run_cls = kServeClasses - 1;      // class of the current (or last) launch
+    uint32_t epoch = 0;                   // launches so far; the current launch's epoch
+    bool yield_sent = false;
+    std::chrono::steady_clock::time_point run_t0;
     // device
     GraphView *d_views = nullptr;
     ServeDesc *d_ring = nullptr;
+    int32_t *d_class_slots = nullptr;     // kServeClasses x cap
     float *d_qpool = nullptr;
     ServeCtl *d_ctl = nullptr;
     int32_t *d_status = nullptr;
@@ -59,7 +73,10 @@ struct falcon_server {
     // host pinned (staging) and host-mapped (results)
     ServeDesc *h_desc = nullptr;
     float *h_qstage = nullptr;
-    unsigned long long *h_tail = nullptr;       // one pinned value per ring entry (async copy source)
+    int32_t *h_class_slots = nullptr;
+    unsigned long long *h_tail = nullptr;       // kServeClasses pinned values per ring entry (async copy source)
+    uint32_t *h_run_epoch = nullptr;            // host-mapped: read by each launch at start
+    uint32_t *h_yield = nullptr;                // pinned sources of yield copies, one per launch mod 16
     int32_t *h_out_ids = nullptr;
     float *h_out_d = nullptr;
     int32_t *h_hops = nullptr, *h_vis = nullptr;
@@ -67,6 +84,10 @@ struct falcon_server {
     // bookkeeping
     std::vector<const falcon_index *> indexes;
     std::vector<int> index_dim, index_entry;
+    std::vector<int> index_vrows;               // per index and precision
+    unsigned long long ctail[kServeClasses] = {};   // published per class queue
+    int64_t unfinished[kServeClasses] = {};     // submitted, not collected
+    std::vector<int> entry_cls;
     std::vector<unsigned long long> entry_seq;  // seq occupying each entry, or ~0 when free
     std::vector<int> entry_k;
     unsigned long long next_seq = 0;
@@ -86,12 +107,14 @@ int cuda_fail(cudaError_t e, const char *what)
 
 void free_server(falcon_server *sv)
 {
-    if (sv->graph) cudaGraphExecDestroy(sv->graph);
+    for (int c = 0; c < kServeClasses; c++)
+        if (sv->graph[c]) cudaGraphExecDestroy(sv->graph[c]);
     if (sv->kernel_done) cudaEventDestroy(sv->kernel_done);
     if (sv->kstream) cudaStreamDestroy(sv->kstream);
     if (sv->cstream) cudaStreamDestroy(sv->cstream);
     cudaFree(sv->d_views);
     cudaFree(sv->d_ring);
+    cudaFree(sv->d_class_slots);
     cudaFree(sv->d_qpool);
     cudaFree(sv->d_ctl);
     cudaFree(sv->d_status);
@@ -101,6 +124,9 @@ void free_server(falcon_server *sv)
     cudaFreeHost(sv->h_desc);
     cudaFreeHost(sv->h_qstage);
     cudaFreeHost(sv->h_tail);
+    cudaFreeHost(sv->h_class_slots);
+    cudaFreeHost(sv->h_run_epoch);
+    cudaFreeHost(sv->h_yield);
     cudaFreeHost(sv->h_out_ids);
     cudaFreeHost(sv->h_out_d);
     cudaFreeHost(sv->h_hops);
@@ -109,19 +135,71 @@ void free_server(falcon_server *sv)
     delete sv;
 }
 
-// Launch the serving kernel (graph) unless it is still running.  Caller holds mu.
+// A class kernel that has run this long yields to another class with
+// requests waiting.
+constexpr double kClassSliceUs = 20000.0;
+
+// Whether class c has a request that is neither collected nor done: with no
+// kernel running, exactly the requests still to be claimed.  Walks the
+// class queue back from its tail until all of the class's uncollected
+// entries have been seen (the newest are the likeliest to be pending).
+bool class_pending(const falcon_server *sv, int c)
+{
+    int64_t seen = 0;
+    const unsigned long long t = sv->ctail[c];
+    for (unsigned long long k = 0; k < t && k < (unsigned long long)sv->cap && seen < sv->unfinished[c]; k++) {
+        const int e = sv->h_class_slots[(size_t)c * sv->cap + (t - 1 - k) % (unsigned long long)sv->cap];
+        const unsigned long long seq = sv->entry_seq[e];
+        if (seq == ~0ull || sv->entry_cls[e] != c) continue;
+        seen++;
+        if (*reinterpret_cast<volatile unsigned long long *>(sv->h_done + e) != seq + 1) return true;
+    }
+    return false;
+}
+
+// Keep a class kernel running while any class has requests to claim:
+// relaunch after an idle exit, switch classes round robin, and ask the
+// running kernel to yield when another class waits (see the file comment).
+// Caller holds mu.
 int ensure_running(falcon_server *sv)
 {
     if (sv->launched) {
         const cudaError_t q = cudaEventQuery(sv->kernel_done);
-        if (q == cudaErrorNotReady) return FALCON_OK;
+        if (q == cudaErrorNotReady) {
+            if (!sv->yield_sent) {
+                bool other = false;
+                for (int c = 0; c < kServeClasses; c++) other |= (c != sv->run_cls && sv->unfinished[c] > 0);
+                const double ran = std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() -
+                                                                             sv->run_t0).count();
+                if (other && (sv->unfinished[sv->run_cls] == 0 || ran >= kClassSliceUs)) {
+                    uint32_t *src = sv->h_yield + (sv->epoch % 16);
+                    *src = sv->epoch;
+                    const cudaError_t e = cudaMemcpyAsync(&sv->d_ctl->yield_epoch, src, sizeof(uint32_t),
+                                                          cudaMemcpyHostToDevice, sv->cstream);
+                    if (e != cudaSuccess) return cuda_fail(e, "serve yield");
+                    sv->yield_sent = true;
+                }
+            }
+            return FALCON_OK;
+        }
         if (q != cudaSuccess) return cuda_fail(q, "serve kernel");
+        sv->launched = false;
     }
-    cudaError_t e = cudaGraphLaunch(sv->graph, sv->kstream);
+    int cls = -1;
+    for (int i = 1; i <= kServeClasses && cls < 0; i++) {
+        const int c = (sv->run_cls + i) % kServeClasses;
+        if (sv->unfinished[c] > 0 && class_pending(sv, c)) cls = c;
+    }
+    if (cls < 0) return FALCON_OK;
+    *sv->h_run_epoch = ++sv->epoch;
+    cudaError_t e = cudaGraphLaunch(sv->graph[cls], sv->kstream);
     if (e == cudaSuccess) e = cudaEventRecord(sv->kernel_done, sv->kstream);
     if (e != cudaSuccess) return cuda_fail(e, "serve kernel launch");
     sv->launched = true;
     sv->launches++;
+    sv->run_cls = cls;
+    sv->yield_sent = false;
+    sv->run_t0 = std::chrono::steady_clock::now();
     return FALCON_OK;
 }
 
@@ -190,11 +268,20 @@ int falcon_server_create(const falcon_server_config *c, falcon_server **out)
     L.ef_max = c->ef_max;
     L.cq_max = c->cand_queue_max;
     L.idle_ns = (long long)c->idle_exit_us * 1000;
-    if ((e = serve_config(L, sv->epl, sv->vmax, sv->num_sms, &sv->grid, &sv->smem)) != cudaSuccess) {
-        free_server(sv);
-        return cuda_fail(e, "serve kernel configuration");
+    // the classes a registered index can need: FP32 rows up to vmax, BF16 up
+    // to ceil(vmax / 2), FP8 one row (dimensions <= 512)
+    for (int r = 1; r <= 4; r++) sv->class_ok[serve_class(kF32, r)] = r <= sv->vmax;
+    for (int r = 1; r <= 2; r++) sv->class_ok[serve_class(kBF16, r)] = r <= (sv->vmax + 1) / 2;
+    sv->class_ok[serve_class(kFP8, 1)] = true;
+    for (int c = 0; c < kServeClasses; c++) {
+        if (!sv->class_ok[c]) continue;
+        if ((e = serve_config(L, sv->epl, c, sv->num_sms, &sv->grid[c], &sv->smem[c])) != cudaSuccess) {
+            free_server(sv);
+            return cuda_fail(e, "serve kernel configuration");
+        }
+        if (sv->grid[c] > sv->max_grid) sv->max_grid = sv->grid[c];
     }
-    const size_t warps = (size_t)sv->grid * 4;
+    const size_t warps = (size_t)sv->max_grid * 4;
 #define SV_ALLOC(call, what)                      \
     if ((e = (call)) != cudaSuccess) {            \
         free_server(sv);                          \
@@ -205,6 +292,7 @@ int falcon_server_create(const falcon_server_config *c, falcon_server **out)
     SV_ALLOC(cudaEventCreateWithFlags(&sv->kernel_done, cudaEventDisableTiming), "event");
     SV_ALLOC(cudaMalloc(&sv->d_views, sizeof(GraphView) * 48), "views");
     SV_ALLOC(cudaMalloc(&sv->d_ring, sizeof(ServeDesc) * sv->cap), "ring");
+    SV_ALLOC(cudaMalloc(&sv->d_class_slots, sizeof(int32_t) * kServeClasses * (size_t)sv->cap), "class queues");
     SV_ALLOC(cudaMalloc(&sv->d_qpool, sizeof(float) * (size_t)sv->qstride * sv->cap), "query pool");
     SV_ALLOC(cudaMalloc(&sv->d_ctl, sizeof(ServeCtl)), "control");
     SV_ALLOC(cudaMemset(sv->d_ctl, 0, sizeof(ServeCtl)), "control");
@@ -216,7 +304,13 @@ int falcon_server_create(const falcon_server_config *c, falcon_server **out)
         SV_ALLOC(cudaMalloc(&sv->d_bloom, warps << (c->bloom_bits_max - 3)), "Bloom filters");
     SV_ALLOC(cudaHostAlloc(&sv->h_desc, sizeof(ServeDesc) * sv->cap, cudaHostAllocDefault), "pinned");
     SV_ALLOC(cudaHostAlloc(&sv->h_qstage, sizeof(float) * (size_t)sv->qstride * sv->cap, cudaHostAllocDefault), "pinned");
-    SV_ALLOC(cudaHostAlloc(&sv->h_tail, sizeof(unsigned long long) * sv->cap, cudaHostAllocDefault), "pinned");
+    SV_ALLOC(cudaHostAlloc(&sv->h_tail, sizeof(unsigned long long) * kServeClasses * sv->cap, cudaHostAllocDefault),
+             "pinned");
+    SV_ALLOC(cudaHostAlloc(&sv->h_class_slots, sizeof(int32_t) * kServeClasses * (size_t)sv->cap, cudaHostAllocDefault),
+             "pinned");
+    SV_ALLOC(cudaHostAlloc(&sv->h_run_epoch, sizeof(uint32_t), cudaHostAllocMapped), "mapped");
+    SV_ALLOC(cudaHostAlloc(&sv->h_yield, sizeof(uint32_t) * 16, cudaHostAllocDefault), "pinned");
+    *sv->h_run_epoch = 0;
     SV_ALLOC(cudaHostAlloc(&sv->h_out_ids, sizeof(int32_t) * (size_t)c->max_k * sv->cap, cudaHostAllocMapped), "mapped");
     SV_ALLOC(cudaHostAlloc(&sv->h_out_d, sizeof(float) * (size_t)c->max_k * sv->cap, cudaHostAllocMapped), "mapped");
     SV_ALLOC(cudaHostAlloc(&sv->h_hops, sizeof(int32_t) * sv->cap, cudaHostAllocMapped), "mapped");
@@ -224,12 +318,15 @@ int falcon_server_create(const falcon_server_config *c, falcon_server **out)
     SV_ALLOC(cudaHostAlloc(&sv->h_done, sizeof(unsigned long long) * sv->cap, cudaHostAllocMapped), "mapped");
     memset(sv->h_done, 0, sizeof(unsigned long long) * sv->cap);
     memset(sv->h_qstage, 0, sizeof(float) * (size_t)sv->qstride * sv->cap);
-    sv->device_bytes = (int64_t)(sizeof(ServeDesc) + sizeof(float) * sv->qstride) * sv->cap +
+    sv->device_bytes = (int64_t)(sizeof(ServeDesc) + sizeof(float) * sv->qstride + 4 * kServeClasses) * sv->cap +
                        (int64_t)warps * c->ef_max * 8 +
                        (c->bloom_bits_max > kMaxSmemBloomBits ? (int64_t)(warps << (c->bloom_bits_max - 3)) : 0);
     void *dp;
     L.views = sv->d_views;
     L.ring = sv->d_ring;
+    L.class_slots = sv->d_class_slots;
+    SV_ALLOC(cudaHostGetDevicePointer(&dp, sv->h_run_epoch, 0), "mapped pointer");
+    L.run_epoch = (const uint32_t *)dp;
     L.qpool = sv->d_qpool;
     SV_ALLOC(cudaHostGetDevicePointer(&dp, sv->h_out_ids, 0), "mapped pointer");
     L.out_ids = (int32_t *)dp;
@@ -246,20 +343,22 @@ int falcon_server_create(const falcon_server_config *c, falcon_server **out)
     L.bloom_global = sv->d_bloom;
     L.cand_ids = sv->d_cand_ids;
     L.cand_d = sv->d_cand_d;
-    // capture the persistent launch once; every (re)start replays the graph
-    {
+    // capture each class's persistent launch once; every (re)start replays its graph
+    for (int c = 0; c < kServeClasses; c++) {
+        if (!sv->class_ok[c]) continue;
         cudaGraph_t g = nullptr;
         SV_ALLOC(cudaStreamBeginCapture(sv->kstream, cudaStreamCaptureModeThreadLocal), "capture");
-        e = launch_serve(L, sv->epl, sv->vmax, sv->grid, sv->smem, sv->kstream);
+        e = launch_serve(L, sv->epl, c, sv->grid[c], sv->smem[c], sv->kstream);
         cudaError_t e2 = cudaStreamEndCapture(sv->kstream, &g);
         if (e == cudaSuccess) e = e2;
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&sv->graph, g, 0);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&sv->graph[c], g, 0);
         if (g) cudaGraphDestroy(g);
         if (e != cudaSuccess) { free_server(sv); return cuda_fail(e, "serve graph"); }
     }
 #undef SV_ALLOC
     sv->entry_seq.assign(sv->cap, ~0ull);
     sv->entry_k.assign(sv->cap, 0);
+    sv->entry_cls.assign(sv->cap, 0);
     *out = sv;
     return FALCON_OK;
 }
@@ -287,6 +386,7 @@ int falcon_server_add_index(falcon_server *sv, falcon_index *ix, int32_t *index_
     sv->indexes.push_back(ix);
     sv->index_dim.push_back(dim);
     sv->index_entry.push_back(entry);
+    for (int pr = 0; pr < 3; pr++) sv->index_vrows.push_back(serve_vrows(views[pr].dpad, pr));
     *index_id = id;
     return FALCON_OK;
 }
@@ -299,9 +399,7 @@ int falcon_server_submit(falcon_server *sv, int32_t n, const int32_t *index_ids,
         return set_error_code(FALCON_ERR_ARG, "falcon_server_submit: null argument");
     std::lock_guard<std::mutex> lock(sv->mu);
     if (cudaSetDevice(sv->device) != cudaSuccess) return set_error_code(FALCON_ERR_CUDA, "select device");
-    // validate, then admit while ring entries are free
-    int admitted = 0;
-    const unsigned long long first = sv->next_seq;
+    // validate every request first, so a refused call stages nothing
     for (int i = 0; i < n; i++) {
         const int idx = index_ids[i];
         if (idx < 0 || idx >= (int)sv->indexes.size()) return set_error_code(FALCON_ERR_ARG, "unknown index id");
@@ -314,6 +412,20 @@ int falcon_server_submit(falcon_server *sv, int32_t n, const int32_t *index_ids,
             p.mode != FALCON_MODE_INTER)
             return set_error_code(FALCON_ERR_ARG, "request parameters exceed the server's configuration");
         if (query_stride < sv->index_dim[idx]) return set_error_code(FALCON_ERR_ARG, "query_stride < dim");
+        const int cls = serve_class(p.precision, sv->index_vrows[3 * idx + p.precision]);
+        if (cls < 0 || cls >= kServeClasses || !sv->class_ok[cls])
+            return set_error_code(FALCON_ERR_ARG, "request class not built for this server's dim_max");
+    }
+    // then admit in order while ring entries are free
+    int admitted = 0;
+    const unsigned long long first = sv->next_seq;
+    unsigned long long ctail0[kServeClasses];
+    memcpy(ctail0, sv->ctail, sizeof(ctail0));
+    for (int i = 0; i < n; i++) {
+        const int idx = index_ids[i];
+        const falcon_search_params &p = params[per_request_params ? i : 0];
+        const int ef = p.ef < p.k ? p.k : p.ef;
+        const int cls = serve_class(p.precision, sv->index_vrows[3 * idx + p.precision]);
         const unsigned long long seq = first + (unsigned long long)i;
         const int e = (int)(seq % (unsigned long long)sv->cap);
         if (sv->entry_seq[e] != ~0ull) break;   // entry still in use: stop admitting
@@ -340,6 +452,10 @@ int falcon_server_submit(falcon_server *sv, int32_t n, const int32_t *index_ids,
         for (int j = sv->index_dim[idx]; j < sv->qstride; j++) qs[j] = 0.0f;
         sv->entry_seq[e] = seq;
         sv->entry_k[e] = p.k;
+        sv->entry_cls[e] = cls;
+        sv->h_class_slots[(size_t)cls * sv->cap + sv->ctail[cls] % (unsigned long long)sv->cap] = e;
+        sv->ctail[cls]++;
+        sv->unfinished[cls]++;
         request_ids[i] = (int64_t)seq;
         admitted++;
     }
@@ -358,12 +474,25 @@ int falcon_server_submit(falcon_server *sv, int32_t n, const int32_t *index_ids,
             err = cudaMemcpyAsync(sv->d_ring + s0, sv->h_desc + s0, sizeof(ServeDesc) * cnt, cudaMemcpyHostToDevice,
                                   sv->cstream);
     }
+    // each class queue's new slots (at most two contiguous ranges), then all tails in one copy
+    for (int c = 0; c < kServeClasses && err == cudaSuccess; c++) {
+        const unsigned long long n_new = sv->ctail[c] - ctail0[c];
+        if (n_new == 0) continue;
+        const int q0 = (int)(ctail0[c] % (unsigned long long)sv->cap);
+        const int r1 = (int)(n_new < (unsigned long long)(sv->cap - q0) ? n_new : (unsigned long long)(sv->cap - q0));
+        int32_t *dq = sv->d_class_slots + (size_t)c * sv->cap;
+        const int32_t *hq = sv->h_class_slots + (size_t)c * sv->cap;
+        err = cudaMemcpyAsync(dq + q0, hq + q0, sizeof(int32_t) * r1, cudaMemcpyHostToDevice, sv->cstream);
+        if (err == cudaSuccess && (int)n_new > r1)
+            err = cudaMemcpyAsync(dq, hq, sizeof(int32_t) * ((int)n_new - r1), cudaMemcpyHostToDevice, sv->cstream);
+    }
     const unsigned long long tail = first + admitted;
     const int te = (int)((tail - 1) % (unsigned long long)sv->cap);
-    sv->h_tail[te] = tail;
+    unsigned long long *tails = sv->h_tail + (size_t)te * kServeClasses;
+    memcpy(tails, sv->ctail, sizeof(unsigned long long) * kServeClasses);
     if (err == cudaSuccess)
-        err = cudaMemcpyAsync(&sv->d_ctl->tail, &sv->h_tail[te], sizeof(unsigned long long), cudaMemcpyHostToDevice,
-                              sv->cstream);
+        err = cudaMemcpyAsync(sv->d_ctl->tail, tails, sizeof(unsigned long long) * kServeClasses,
+                              cudaMemcpyHostToDevice, sv->cstream);
     if (err != cudaSuccess) return cuda_fail(err, "publish requests");
     sv->next_seq = tail;
     sv->in_flight += admitted;
@@ -391,6 +520,7 @@ int collect_locked(falcon_server *sv, unsigned long long seq, int32_t *out_ids, 
     if (visited) *visited = sv->h_vis[e];
     sv->entry_seq[e] = ~0ull;
     sv->in_flight--;
+    sv->unfinished[sv->entry_cls[e]]--;
     return 1;
 }
 }  // namespace
@@ -500,7 +630,7 @@ int falcon_server_info_get(falcon_server *sv, falcon_server_info *info)
     info->in_flight = sv->in_flight;
     info->submitted = (int64_t)sv->next_seq;
     info->kernel_launches = sv->launches;
-    info->warps = sv->grid * 4;
+    info->warps = sv->max_grid * 4;
     info->device_bytes = sv->device_bytes;
     return FALCON_OK;
 }
