@@ -344,6 +344,50 @@ def run_reference(args):
     return 0
 
 
+def profile_serve(args, ix, q, dq, ef, mc, mg, cq, bits):
+    """--profile-region --profile-search serve: each profiled step is one
+    batched FP32 search of the query set, then the same queries as single
+    requests through the serving kernel (all submitted at once, each waited
+    for), so one capture holds inter_kernel and serve_kernel on the same work."""
+    import torch
+    from falcon_b200 import make_params
+    from falcon_b200.serving import FalconServer
+    sv = FalconServer(ring_capacity=max(2 * len(q), 1024), max_k=K, ef_max=ef, cand_queue_max=cq,
+                      bloom_bits_max=bits, mc_max=max(mc, 1), mg_max=max(mg, 1), dim_max=DIM, idle_exit_us=500)
+    iid = sv.add_index(ix)
+    p = make_params(k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
+    index_ids = np.full(len(q), iid, dtype=np.int32)
+
+    def served():
+        rids = sv.submit(index_ids, q, p)
+        for r in rids:
+            sv.wait(int(r), K, timeout_us=120_000_000)
+        return len(rids)
+
+    served()                                  # first launch outside the region
+    torch.cuda.synchronize()
+    l0 = sv.info().kernel_launches
+    tb = ts = 0.0
+    torch.cuda.profiler.start()
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
+        torch.cuda.synchronize()
+        tb += time.perf_counter() - t
+        t = time.perf_counter()
+        n = served()
+        ts += time.perf_counter() - t
+    torch.cuda.profiler.stop()
+    print(json.dumps({"profiled_steps": args.steps, "search": "serve", "ef": ef, "mc": mc, "mg": mg, "cq": cq,
+                      "bloom_bits": bits, "n_base": N_BASE, "requests_per_step": n,
+                      "batched_ms_per_step": tb * 1e3 / args.steps, "served_ms_per_step": ts * 1e3 / args.steps,
+                      "serve_warps": int(sv.info().warps),
+                      "serve_launches_per_step": (sv.info().kernel_launches - l0) / args.steps}))
+    sv.close()
+    ix.close()
+    return 0
+
+
 def run_ours(args):
     import torch
     ws, rank, local = dist_env()
@@ -374,6 +418,8 @@ def run_ours(args):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     extra = {}
+    if args.profile_region and args.profile_search == "serve":
+        return profile_serve(args, ix, q, dq, ef, mc, mg, cq, bits)
     if args.profile_region and args.profile_search == "intra":
         extra = dict(mode="intra", channels=4)
     elif args.profile_region and args.profile_search == "bf16_rerank":
@@ -568,9 +614,10 @@ def main():
     ap.add_argument("--fixed", default=None, help="ef,mc,mg,cq,bloom_bits: skip the sweep")
     ap.add_argument("--profile-region", action="store_true",
                     help="bracket only the timed steps with cudaProfilerStart/Stop and exit after them")
-    ap.add_argument("--profile-search", default="inter", choices=["inter", "intra", "bf16_rerank"],
+    ap.add_argument("--profile-search", default="inter", choices=["inter", "intra", "bf16_rerank", "serve"],
                     help="with --profile-region: the search the timed steps run (inter-query FP32, intra-query "
-                         "4 channels FP32, or BF16 traversal + FP32 rerank)")
+                         "4 channels FP32, BF16 traversal + FP32 rerank, or FP32 batched then the same queries "
+                         "through the serving kernel)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

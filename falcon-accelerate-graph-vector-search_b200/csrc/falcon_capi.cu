@@ -873,6 +873,17 @@ int index_graph_view(const falcon_index *ix, int precision, GraphView *v, int *d
 int index_device(const falcon_index *ix) { return ix->device; }
 bool index_has_upper(const falcon_index *ix) { return ix->upper_max_level > 0; }
 
+// The descent launch of an index (upper layers and FP32 vectors; queries and
+// outputs left for the caller): false when the index has no upper layers.
+// *has_f32 tells whether the FP32 vectors the descent reads are resident.
+bool index_descend_launch(const falcon_index *ix, DescendLaunch *a, bool *has_f32)
+{
+    *has_f32 = ix->d_f32 != nullptr;
+    if (ix->upper_max_level < 1) return false;
+    *a = descend_launch(ix);
+    return true;
+}
+
 // Validates a no-allocation request; needs ef >= k in every struct so the
 // caller's structs can be copied to the device unchanged (the kernels'
 // QParams has the same layout, checked below).

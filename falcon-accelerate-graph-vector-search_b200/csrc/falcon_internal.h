@@ -62,6 +62,7 @@ struct DescendLaunch {
     int64_t qstride;
     int64_t nq;
     int32_t *out_entry;
+    int64_t out_entry_stride;       // int32 units between queries' entries (0: contiguous)
     int32_t *out_hops;              // may be null
 };
 

@@ -1324,7 +1324,7 @@ __global__ void __launch_bounds__(128) descend_kernel(const DescendLaunch A)
             }
         }
         if (lane == 0) {
-            A.out_entry[qi] = cur;
+            A.out_entry[qi * (A.out_entry_stride > 0 ? A.out_entry_stride : 1)] = cur;
             if (A.out_hops) A.out_hops[qi] = hops;
         }
     }

@@ -13,7 +13,10 @@
 // another class has requests waiting, the running kernel is asked to yield
 // (its warps leave between requests) once its class has nothing uncollected
 // or it has run for kClassSliceUs, and the next class with work (round
-// robin) is launched.
+// robin) is launched.  Requests to an index with HNSW upper layers get their
+// entry from the descent kernel, launched at submit on the copy stream over
+// the new queries and writing into the ring descriptors before the tails
+// are published; the class kernels leave block slots free for it.
 // Results go to host-mapped memory and complete with a per-entry done word,
 // so the host collects them without any CUDA call.  The ring's size is
 // chosen from the free device memory at creation (admission by memory): a
@@ -39,6 +42,7 @@ namespace falcon {
 int set_error_code(int code, const char *msg);
 int index_device(const falcon_index *ix);
 int index_graph_view(const falcon_index *ix, int precision, GraphView *v, int *dim, int *entry);
+bool index_descend_launch(const falcon_index *ix, DescendLaunch *a, bool *has_f32);
 int check_search_params(const falcon_search_params &p, const falcon_index *ix, int64_t qi);
 }  // namespace falcon
 
@@ -85,6 +89,8 @@ struct falcon_server {
     std::vector<const falcon_index *> indexes;
     std::vector<int> index_dim, index_entry;
     std::vector<int> index_vrows;               // per index and precision
+    std::vector<char> index_upper;              // requests start from the upper-layer descent
+    std::vector<DescendLaunch> index_dl;
     unsigned long long ctail[kServeClasses] = {};   // published per class queue
     int64_t unfinished[kServeClasses] = {};     // submitted, not collected
     std::vector<int> entry_cls;
@@ -138,6 +144,9 @@ void free_server(falcon_server *sv)
 // A class kernel that has run this long yields to another class with
 // requests waiting.
 constexpr double kClassSliceUs = 20000.0;
+
+// Block slots the serve kernels leave free for the submit-time descent.
+constexpr int kDescendSlots = 2;
 
 // Whether class c has a request that is neither collected nor done: with no
 // kernel running, exactly the requests still to be claimed.  Walks the
@@ -279,6 +288,10 @@ int falcon_server_create(const falcon_server_config *c, falcon_server **out)
             free_server(sv);
             return cuda_fail(e, "serve kernel configuration");
         }
+        // leave kDescendSlots block slots free, so that the descent of newly
+        // submitted requests (an ordinary kernel on the copy stream) finds room
+        // while a persistent class kernel holds the GPU
+        if (sv->grid[c] > kDescendSlots) sv->grid[c] -= kDescendSlots;
         if (sv->grid[c] > sv->max_grid) sv->max_grid = sv->grid[c];
     }
     const size_t warps = (size_t)sv->max_grid * 4;
@@ -385,7 +398,13 @@ int falcon_server_add_index(falcon_server *sv, falcon_index *ix, int32_t *index_
     if (e != cudaSuccess) return cuda_fail(e, "register index");
     sv->indexes.push_back(ix);
     sv->index_dim.push_back(dim);
-    sv->index_entry.push_back(entry);
+    DescendLaunch dl;
+    bool has_f32 = false;
+    const bool upper = index_descend_launch(ix, &dl, &has_f32);
+    if (upper && !has_f32) return set_error_code(FALCON_ERR_UNSUPPORTED, "the upper-layer descent needs FP32 storage");
+    sv->index_entry.push_back(upper ? -1 : entry);
+    sv->index_upper.push_back(upper ? 1 : 0);
+    sv->index_dl.push_back(dl);
     for (int pr = 0; pr < 3; pr++) sv->index_vrows.push_back(serve_vrows(views[pr].dpad, pr));
     *index_id = id;
     return FALCON_OK;
@@ -473,6 +492,27 @@ int falcon_server_submit(falcon_server *sv, int32_t n, const int32_t *index_ids,
         if (err == cudaSuccess)
             err = cudaMemcpyAsync(sv->d_ring + s0, sv->h_desc + s0, sizeof(ServeDesc) * cnt, cudaMemcpyHostToDevice,
                                   sv->cstream);
+    }
+    // entries of requests to indexes with upper layers: the greedy descent of
+    // their queries, written into the ring descriptors before the tails are
+    // published (same stream), one launch per run of consecutive entries of one
+    // index (a run ends at the ring's wrap)
+    for (int i = 0; i < admitted && err == cudaSuccess;) {
+        const int idx = index_ids[i];
+        const int es = (int)((first + (unsigned long long)i) % (unsigned long long)sv->cap);
+        int j = i + 1;
+        while (j < admitted && index_ids[j] == idx && es + (j - i) < sv->cap) j++;
+        if (sv->index_upper[idx]) {
+            DescendLaunch dl = sv->index_dl[idx];
+            dl.queries = sv->d_qpool + (size_t)es * sv->qstride;
+            dl.qstride = sv->qstride;
+            dl.nq = j - i;
+            dl.out_entry = &sv->d_ring[es].entry;
+            dl.out_entry_stride = (int64_t)(sizeof(ServeDesc) / sizeof(int32_t));
+            dl.out_hops = nullptr;
+            err = launch_descend(dl, sv->num_sms, sv->cstream);
+        }
+        i = j;
     }
     // each class queue's new slots (at most two contiguous ranges), then all tails in one copy
     for (int c = 0; c < kServeClasses && err == cudaSuccess; c++) {

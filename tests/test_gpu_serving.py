@@ -127,3 +127,39 @@ def test_server_replay_poisson(two_indexes):
         got = (out_ids[i, :p["k"]], out_d[i, :p["k"]], int(hops[i]), int(vis[i]))
         assert _same(got, _alone(ix1 if w == 0 else ix2, q, p))
     sv.close()
+
+
+def test_server_descends_upper_layers():
+    """Requests to an index with HNSW upper layers start from the greedy
+    descent of their own query (run on the copy stream at submit), like
+    falcon_search without entry points: every served result equals the same
+    request searched alone, FP32 and BF16 + rerank, in bursts and by replay."""
+    from falcon_b200 import FalconIndex, make_params
+    from falcon_b200.graph import build_graph, build_upper_layers
+    from falcon_b200.serving import FalconServer, poisson_arrivals
+    from falcon_b200.synthetic import unit_normal
+    x = unit_normal(6000, 96, 41)
+    q = unit_normal(96, 96, 42)
+    g = build_graph(x, 64, device="cuda")
+    upper = build_upper_layers(x, 32, seed=5, device="cuda")
+    g.entry_point = upper.entry
+    ix = FalconIndex(g, storage=("f32", "bf16"))
+    ix.set_upper_layers(upper)
+    sv = FalconServer(ring_capacity=512, max_k=10, ef_max=128, cand_queue_max=64, bloom_bits_max=17, dim_max=96,
+                      idle_exit_us=3000)
+    iid = sv.add_index(ix)
+    params = [dict(k=10, ef=128, mc=2, mg=2, cand_queue_size=64, bloom_bits=17),
+              dict(k=10, ef=96, cand_queue_size=32, bloom_bits=16, precision="bf16", rerank=True)]
+    reqs = [(q[i], params[i % 2]) for i in range(len(q))]
+    rids = []
+    for s in range(0, len(reqs), 8):
+        for qq, p in reqs[s:s + 8]:
+            rids.append(sv.submit([iid], qq[None, :], p)[0])
+    for (qq, p), rid in zip(reqs, rids):
+        assert _same(sv.wait(rid, p["k"]), _alone(ix, qq, p)), p
+    lat, ids, d, hops, vis, el = sv.replay(np.full(len(q), iid), q, [make_params(**p) for _, p in reqs],
+                                           poisson_arrivals(len(q), 50000.0, seed=7), 10)
+    for i, (qq, p) in enumerate(reqs):
+        assert _same((ids[i], d[i], int(hops[i]), int(vis[i])), _alone(ix, qq, p)), (i, p)
+    sv.close()
+    ix.close()
