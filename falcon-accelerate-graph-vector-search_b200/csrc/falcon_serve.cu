@@ -91,6 +91,7 @@ struct falcon_server {
     std::vector<int> index_vrows;               // per index and precision
     std::vector<char> index_upper;              // requests start from the upper-layer descent
     std::vector<DescendLaunch> index_dl;
+    bool any_upper = false;                     // some index descends: submits launch a descent
     unsigned long long ctail[kServeClasses] = {};   // published per class queue
     int64_t unfinished[kServeClasses] = {};     // submitted, not collected
     std::vector<int> entry_cls;
@@ -405,6 +406,7 @@ int falcon_server_add_index(falcon_server *sv, falcon_index *ix, int32_t *index_
     sv->index_entry.push_back(upper ? -1 : entry);
     sv->index_upper.push_back(upper ? 1 : 0);
     sv->index_dl.push_back(dl);
+    if (upper) sv->any_upper = true;
     for (int pr = 0; pr < 3; pr++) sv->index_vrows.push_back(serve_vrows(views[pr].dpad, pr));
     *index_id = id;
     return FALCON_OK;
@@ -612,12 +614,25 @@ int falcon_server_replay(falcon_server *sv, int32_t n, const int32_t *index_ids,
     std::vector<int32_t> tmp_ids(sv->cfg.max_k);
     std::vector<float> tmp_d(sv->cfg.max_k);
     const int kBatch = 512;
+    // Every submit to an index with upper layers launches one descent, a chain
+    // of dependent row reads of about 50 us that holds the copy stream; a
+    // submit per few arrivals would queue them faster than the stream drains.
+    // With such an index, arrivals are gathered into micro-batches instead.
+    bool any_upper;
+    {
+        std::lock_guard<std::mutex> lock(sv->mu);
+        any_upper = sv->any_upper;
+    }
+    const double kSubmitWindowUs = 200.0;
+    double last_submit = -1e30;
     while (done < n) {
         const double t = now_us();
         // submit everything that has arrived (in order), as ring entries allow
         int end = next;
         while (end < n && arrival_us[end] <= t && end - next < kBatch) end++;
-        if (end > next) {
+        const bool wait_window = any_upper && end - next < kBatch && t - last_submit < kSubmitWindowUs;
+        if (end > next && !wait_window) {
+            last_submit = t;
             const int cnt = end - next;
             const int rc = falcon_server_submit(sv, cnt, index_ids + next, queries + (size_t)next * query_stride,
                                                 query_stride, params + (per_request_params ? next : 0),

@@ -322,8 +322,10 @@ int falcon_server_wait(falcon_server *sv, int64_t request_id, int64_t timeout_us
                        float *out_dists, int32_t *hops, int32_t *visited);
 /* Load driver: replay an arrival schedule (microsecond offsets from the call,
    ascending) from the calling thread.  Each request is submitted when it has
-   arrived and a ring entry is free, completions are detected by polling, and
-   latency_us[i] = completion - arrival (queueing included).  Results go to
+   arrived and a ring entry is free (with an index that has upper layers in
+   the server, arrivals are gathered for up to 200 us or 512 requests per
+   submit, since each submit launches one descent), completions are detected
+   by polling, and latency_us[i] = completion - arrival (queueing included).  Results go to
    out_ids / out_dists (n x out_stride, may be NULL), hops, visited. */
 int falcon_server_replay(falcon_server *sv, int32_t n, const int32_t *index_ids, const float *queries,
                          int64_t query_stride, const falcon_search_params *params, int32_t per_request_params,
