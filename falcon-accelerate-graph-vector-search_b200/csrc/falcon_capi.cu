@@ -3,6 +3,7 @@
 // issued on the caller's stream.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdarg>
 #include <cstddef>
 #include <cstdio>
@@ -16,6 +17,7 @@
 using namespace falcon;
 
 struct falcon_index {
+    std::atomic<int> server_refs{0};   // servers holding device pointers into this index
     int device = 0;
     int num_sms = 0;
     int64_t n = 0;
@@ -291,6 +293,8 @@ done:
 int falcon_index_free(falcon_index *ix)
 {
     if (!ix) return FALCON_OK;
+    if (ix->server_refs.load() > 0)
+        return set_error(FALCON_ERR_ARG, "the index is registered with a server: free the server first");
     DeviceGuard guard(ix->device);
     free_index_buffers(ix);
     delete ix;
@@ -396,6 +400,9 @@ int falcon_index_set_upper_layers(falcon_index *ix, const falcon_upper_layers_de
 {
     if (!ix || !d || !d->levels || !d->row_start || (d->num_rows > 0 && !d->rows))
         return set_error(FALCON_ERR_ARG, "null argument");
+    if (ix->server_refs.load() > 0)
+        return set_error(FALCON_ERR_ARG, "the index is registered with a server: set its upper layers before "
+                                         "falcon_server_add_index");
     if (d->max_level < 1 || d->max_degree < 1 || d->max_degree > kMaxDegree || d->ids_offset < 1 ||
         d->row_stride < d->ids_offset + d->max_degree || d->num_rows < 0)
         return set_error(FALCON_ERR_ARG, "bad upper-layer shape (max_level=%d, max_degree=%d, ids_offset=%d, "
@@ -872,6 +879,11 @@ int index_graph_view(const falcon_index *ix, int precision, GraphView *v, int *d
 
 int index_device(const falcon_index *ix) { return ix->device; }
 bool index_has_upper(const falcon_index *ix) { return ix->upper_max_level > 0; }
+
+// A server registers (+1) and releases (-1) the indexes whose device
+// pointers it holds; freeing the index or replacing its upper layers is
+// refused meanwhile.
+void index_server_ref(falcon_index *ix, int delta) { ix->server_refs += delta; }
 
 // The descent launch of an index (upper layers and FP32 vectors; queries and
 // outputs left for the caller): false when the index has no upper layers.

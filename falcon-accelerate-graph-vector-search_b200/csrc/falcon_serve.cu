@@ -43,6 +43,7 @@ int set_error_code(int code, const char *msg);
 int index_device(const falcon_index *ix);
 int index_graph_view(const falcon_index *ix, int precision, GraphView *v, int *dim, int *entry);
 bool index_descend_launch(const falcon_index *ix, DescendLaunch *a, bool *has_f32);
+void index_server_ref(falcon_index *ix, int delta);
 int check_search_params(const falcon_search_params &p, const falcon_index *ix, int64_t qi);
 }  // namespace falcon
 
@@ -398,6 +399,7 @@ int falcon_server_add_index(falcon_server *sv, falcon_index *ix, int32_t *index_
     cudaError_t e = cudaMemcpy(sv->d_views + 3 * id, views, sizeof(views), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(e, "register index");
     sv->indexes.push_back(ix);
+    index_server_ref(ix, +1);
     sv->index_dim.push_back(dim);
     DescendLaunch dl;
     bool has_f32 = false;
@@ -701,6 +703,7 @@ int falcon_server_free(falcon_server *sv)
     }
     cudaStreamSynchronize(sv->cstream);
     cudaStreamSynchronize(sv->kstream);
+    for (const falcon_index *ix : sv->indexes) index_server_ref(const_cast<falcon_index *>(ix), -1);
     free_server(sv);
     return FALCON_OK;
 }

@@ -178,7 +178,8 @@ class FalconIndex:
 
     def close(self):
         if getattr(self, "_h", None):
-            _lib.load().falcon_index_free(self._h)
+            # refused while a server holds the index: keep the handle
+            _lib.check(_lib.load().falcon_index_free(self._h))
             self._h = None
 
     def __del__(self):

@@ -135,6 +135,7 @@ int falcon_index_info_get(const falcon_index *ix, falcon_index_info *info);
    reference keeps its index only in host files (hnsw.py:264-377); this has no
    kernel-side counterpart there. */
 int falcon_index_copy_storage(const falcon_index *ix, int32_t which, void *dst, int64_t bytes);
+/* Fails (FALCON_ERR_ARG) while a server holds the index: free the server first. */
 int falcon_index_free(falcon_index *ix);
 
 /*
@@ -165,6 +166,7 @@ typedef struct falcon_upper_layers_desc {
     const int32_t *rows;            /* num_rows x row_stride */
 } falcon_upper_layers_desc;
 
+/* Fails (FALCON_ERR_ARG) once the index is registered with a server. */
 int falcon_index_set_upper_layers(falcon_index *ix, const falcon_upper_layers_desc *desc);
 
 /*

@@ -163,3 +163,24 @@ def test_server_descends_upper_layers():
         assert _same((ids[i], d[i], int(hops[i]), int(vis[i])), _alone(ix, qq, p)), (i, p)
     sv.close()
     ix.close()
+
+
+def test_registered_index_cannot_be_freed_or_changed():
+    """A server holds device pointers into its indexes: freeing a registered
+    index or replacing its upper layers is refused until the server is freed."""
+    from falcon_b200 import FalconIndex, _lib
+    from falcon_b200.graph import build_upper_layers
+    from falcon_b200.serving import FalconServer
+    from falcon_b200.synthetic import unit_normal
+    g, q = small_graph("unit", 2000, 64, 32, 8, seed=51)
+    ix = FalconIndex(g, storage=("f32",))
+    sv = FalconServer(ring_capacity=64, max_k=10, ef_max=64, dim_max=64, idle_exit_us=2000)
+    iid = sv.add_index(ix)
+    with pytest.raises(_lib.FalconError):
+        ix.close()
+    with pytest.raises(_lib.FalconError):
+        ix.set_upper_layers(build_upper_layers(unit_normal(2000, 64, 51), 16, seed=1, device="cuda"))
+    r = sv.submit([iid], q[:1], dict(k=10, ef=64))[0]
+    assert _same(sv.wait(r, 10), _alone(ix, q[0], dict(k=10, ef=64)))
+    sv.close()
+    ix.close()
