@@ -207,7 +207,8 @@ def serve_measurements(ix, q, gt, ef, mc, mg, cq, bits, batched_bf16_qps):
     p = make_params(k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, precision="bf16", rerank=True)
     n = 2 * N_QUERIES
     qq = np.concatenate([q, q])
-    out = {"precision": "bf16+fp32 rerank", "requests_per_point": n, "points": []}
+    out = {"precision": "bf16+fp32 rerank", "requests_per_point": n, "points": [],
+           "entry": "each request descends the HNSW upper layers (replay submits micro-batches of up to 200 us)"}
     sv.replay(np.full(1000, iid), qq[:1000], p, poisson_arrivals(1000, batched_bf16_qps, 9), K)   # warm-up
     for frac in (0.5, 0.8, 10.0):
         rate = batched_bf16_qps * frac
