@@ -899,8 +899,8 @@ bool index_descend_launch(const falcon_index *ix, DescendLaunch *a, bool *has_f3
 // Validates a no-allocation request; needs ef >= k in every struct so the
 // caller's structs can be copied to the device unchanged (the kernels'
 // QParams has the same layout, checked below).
-int prepare_search(const falcon_index *ix, int64_t nq, const falcon_search_params *params, int32_t per_query_params,
-                   int32_t out_stride, SearchPlan *plan)
+int prepare_search(const falcon_index *ix, int64_t nq, int64_t query_stride, const falcon_search_params *params,
+                   int32_t per_query_params, int32_t out_stride, SearchPlan *plan)
 {
     static_assert(sizeof(QParams) == sizeof(falcon_search_params), "QParams layout");
     static_assert(offsetof(QParams, k) == offsetof(falcon_search_params, k) &&
@@ -916,6 +916,10 @@ int prepare_search(const falcon_index *ix, int64_t nq, const falcon_search_param
                       offsetof(QParams, rerank) == offsetof(falcon_search_params, rerank) &&
                       offsetof(QParams, max_hops) == offsetof(falcon_search_params, max_hops),
                   "QParams layout");
+    // every argument check comes before the caller queues any device work
+    if (nq < 0) return set_error(FALCON_ERR_ARG, "nq %lld < 0", (long long)nq);
+    if (query_stride < ix->dim)
+        return set_error(FALCON_ERR_ARG, "query_stride %lld < dim %d", (long long)query_stride, ix->dim);
     plan->per_query = per_query_params != 0;
     plan->np = plan->per_query ? nq : 1;
     int prec = -1, mode = -1, channels = -1;

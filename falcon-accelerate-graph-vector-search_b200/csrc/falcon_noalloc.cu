@@ -82,8 +82,8 @@ void *scratch_address(int device, cudaError_t *err)
 
 // Defined in falcon_capi.cu: validation and the launch shared with falcon_search.
 namespace falcon {
-int prepare_search(const falcon_index *ix, int64_t nq, const falcon_search_params *params, int32_t per_query_params,
-                   int32_t out_stride, SearchPlan *plan);
+int prepare_search(const falcon_index *ix, int64_t nq, int64_t query_stride, const falcon_search_params *params,
+                   int32_t per_query_params, int32_t out_stride, SearchPlan *plan);
 int run_search_plan(const falcon_index *ix, const SearchPlan &plan, int64_t nq, const float *queries,
                     int64_t query_stride, const int32_t *entry_points, QParams *d_params, int32_t *d_scratch,
                     int32_t *d_cand_ids, float *d_cand_d, int32_t *out_ids, float *out_dists, int32_t out_stride,
@@ -100,9 +100,10 @@ extern "C" int falcon_search_noalloc(falcon_index *ix, const float *queries, int
 {
     if (!ix || !params || !out_ids || !out_dists || (nq > 0 && !queries))
         return set_error_code(FALCON_ERR_ARG, "falcon_search_noalloc: null argument");
+    if (nq < 0) return set_error_code(FALCON_ERR_ARG, "falcon_search_noalloc: nq < 0");
     if (nq == 0) return FALCON_OK;
     SearchPlan plan;
-    int rc = prepare_search(ix, nq, params, per_query_params, out_stride, &plan);
+    int rc = prepare_search(ix, nq, query_stride, params, per_query_params, out_stride, &plan);
     if (rc != FALCON_OK) return rc;
     const size_t param_bytes = sizeof(QParams) * (size_t)plan.np;
     const size_t param_off = kHeaderBytes;

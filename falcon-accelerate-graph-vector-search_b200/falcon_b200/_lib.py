@@ -133,6 +133,8 @@ SIGNATURES = {
                                      _VP, _VP, _I32, _VP, _VP, _VP]),
     "falcon_vadd": (_I32, [_I32, _I32, _I32, _I32, _I32, _I32, _I32, ctypes.c_uint32, _I32, _I32, _I32, _I64,
                            _VP, _VP, _VP, _VP, _VP, _VP, _VP, _I32]),
+    "falcon_graph_prune": (_I32, [_VP, _I64, _I32, _I64, _VP, _I64, _I32, _VP, _I64, ctypes.c_float, _I32, _VP,
+                                  _I64, _VP, _I32, _VP]),
     "falcon_server_default_config": (None, [ctypes.POINTER(ServerConfig)]),
     "falcon_server_create": (_I32, [ctypes.POINTER(ServerConfig), ctypes.POINTER(_VP)]),
     "falcon_server_add_index": (_I32, [_VP, _VP, ctypes.POINTER(ctypes.c_int32)]),

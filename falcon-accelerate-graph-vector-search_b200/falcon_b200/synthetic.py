@@ -40,6 +40,43 @@ def unit_normal(n, dim, seed=0, chunk=1 << 20):
     return out
 
 
+def _blocks(n, dim, seed, fill, threads=None, block=1 << 20):
+    """Rows [b*block, (b+1)*block) come from their own generator seeded by
+    (seed, b), so the result does not depend on how many threads fill it."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+    out = np.empty((n, dim), dtype=np.float32)
+    nb = (n + block - 1) // block
+
+    def run(b):
+        s, e = b * block, min(n, (b + 1) * block)
+        fill(np.random.default_rng([seed, b]), out[s:e])
+
+    with ThreadPoolExecutor(max_workers=threads or min(32, os.cpu_count() or 1)) as ex:
+        list(ex.map(run, range(nb)))
+    return out
+
+
+def sift_like_blocks(n, dim=128, seed=0, threads=None):
+    """sift_like's distribution from block-seeded generators filled in
+    parallel (for bases of 10^7 rows); a different stream than sift_like."""
+    def fill(rng, dst):
+        v = np.rint(np.abs(rng.normal(0.0, 40.0, size=dst.shape)))
+        np.clip(v, 0, 255, out=v)
+        dst[...] = v
+    return _blocks(n, dim, seed, fill, threads)
+
+
+def unit_normal_blocks(n, dim, seed=0, threads=None):
+    """unit_normal's distribution from block-seeded generators filled in
+    parallel; a different stream than unit_normal."""
+    def fill(rng, dst):
+        v = rng.standard_normal(size=dst.shape)
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+        dst[...] = v
+    return _blocks(n, dim, seed, fill, threads)
+
+
 def make(distribution, n, dim, seed):
     if distribution == "sift":
         return sift_like(n, dim, seed)

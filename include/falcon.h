@@ -273,6 +273,33 @@ int falcon_vadd(int32_t query_num, int32_t query_batch_size, int32_t ef, int32_t
                 int32_t *mem_debug, int32_t device);
 
 /*
+ * Graph construction: neighbour selection for one set of nodes, the step the
+ * reference's offline builders run per node -- hnswlib's
+ * getNeighborsByHeuristic2 (networked_FPGA/CPU_programs_oldest/hnswlib/
+ * hnswalg.h:328-369) and NSG's occlusion prune behind
+ * vector_search_baselines/scripts_nsg (the NSG tool itself is not vendored).
+ * For every node in `nodes` (or 0..num_nodes-1 when NULL), in that order:
+ * its num_candidates ids at candidates[node * cand_stride ..] (any order;
+ * -1, out-of-range ids, the node itself and repeats are skipped) are sorted by
+ * (FP32 squared distance to the node, id), then scanned nearest first; a
+ * candidate c is kept unless an already kept neighbour i has
+ * alpha * d(i, c) < d(c, node) (alpha = 1 is hnswlib's and NSG's rule),
+ * until max_degree are kept.  out_neighbors[node * out_stride ..] receives
+ * the kept ids nearest first, then -1; out_counts[node] (may be NULL) their
+ * number.  Distances sum the dimensions in ascending order with every product
+ * and sum rounded separately.  All pointers are device pointers on `device`;
+ * vectors are FP32 rows of vector_stride floats.  Limits: num_candidates
+ * <= 256, max_degree <= 128, alpha in [1, 4], and num_candidates x
+ * (round4(dim) + 4) x 4 bytes within shared memory (227 KB).  Enqueued on
+ * `stream` (cudaStream_t); returns after the launch.
+ */
+int falcon_graph_prune(const float *vectors, int64_t num_vectors, int32_t dim, int64_t vector_stride,
+                       const int32_t *candidates, int64_t cand_stride, int32_t num_candidates,
+                       const int32_t *nodes, int64_t num_nodes, float alpha, int32_t max_degree,
+                       int32_t *out_neighbors, int64_t out_stride, int32_t *out_counts, int32_t device,
+                       void *stream);
+
+/*
  * Serving: continuous batching of single-query requests against several
  * device-resident indexes.  Extends the reference's networked serving path
  * (networked_FPGA/CPU_programs/README.md:50-72, CPU_client.cpp:455-612: a

@@ -1,0 +1,102 @@
+"""GPU graph builder: the neighbour-selection kernel (falcon_graph_prune)
+against a sequential FP32 restatement of hnswlib's heuristic
+(hnswalg.h:328-369, getNeighborsByHeuristic2), and the builder's host-side
+steps (reverse lists, reachability, attaching unreached nodes) on CPU."""
+import numpy as np
+import pytest
+import torch
+
+
+def _d32(a, b):
+    """Squared L2 in FP32, dimensions in ascending order, each product and sum
+    rounded on its own (the kernel's order)."""
+    s = np.float32(0.0)
+    for j in range(a.shape[0]):
+        t = np.float32(a[j] - b[j])
+        s = np.float32(s + np.float32(t * t))
+    return s
+
+
+def prune_model(x, node, cand, R, alpha=1.0):
+    ids = sorted({int(c) for c in cand if 0 <= c < len(x) and c != node})
+    keyed = sorted((_d32(x[c], x[node]).view(np.uint32).item(), c) for c in ids)
+    kept = []
+    for dbits, c in keyed:
+        if len(kept) >= R:
+            break
+        dc = np.uint32(dbits).view(np.float32)
+        if all(not (np.float32(np.float32(alpha) * _d32(x[i], x[c])) < dc) for i in kept):
+            kept.append(c)
+    return kept
+
+
+def test_reverse_lists_and_reachability_cpu():
+    from falcon_b200.nsg import attach_unreached, reachable, reverse_lists
+    adj = torch.tensor([[1, 2, -1], [2, -1, -1], [0, -1, -1], [0, 1, -1], [-1, -1, -1]], dtype=torch.int32)
+    rev = reverse_lists(adj, 2)
+    assert rev.tolist() == [[2, 3], [0, 3], [0, 1], [-1, -1], [-1, -1]]
+    seen = reachable(adj, 0)
+    assert seen.tolist() == [True, True, True, False, False]
+    cnt = (adj >= 0).sum(1).to(torch.int32)
+    cand = torch.tensor([[1], [0], [1], [2], [3]], dtype=torch.int32)
+    added, seen = attach_unreached(adj, cnt, seen, cand, 0)
+    assert added >= 2 and bool(seen.all())
+    # node 3's first reached candidate is 2: the edge goes into 2's free slot
+    assert 3 in adj[2].tolist()
+
+
+def test_ivf_knn_cpu_small():
+    from falcon_b200.nsg import ivf_knn
+    from falcon_b200.synthetic import sift_like
+    x = torch.from_numpy(sift_like(3000, 16, 5))
+    ids, order = ivf_knn(x, 8, n_clusters=6, n_probe=6, seed=1)
+    # every cluster is probed: the lists are the exact 8 nearest (up to ties)
+    d = ((x[:, None, :] - x[None, :, :]) ** 2).sum(-1)
+    d.fill_diagonal_(float("inf"))
+    exact = torch.topk(d, 8, dim=1, largest=False).values
+    got = torch.gather(d, 1, ids.to(torch.int64)).sort(1).values
+    assert torch.equal(got, exact)
+    assert sorted(order.tolist()) == list(range(3000))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,K,R,alpha", [(128, 96, 32, 1.0), (37, 40, 16, 1.0), (96, 160, 64, 1.2),
+                                           (384, 64, 32, 1.0)])
+def test_prune_kernel_matches_sequential_model(dim, K, R, alpha):
+    from falcon_b200.nsg import prune
+    from falcon_b200.synthetic import sift_like, unit_normal
+    rng = np.random.default_rng(dim + K)
+    n = 3000
+    x = sift_like(n, dim, seed=dim) if dim % 2 == 0 else unit_normal(n, dim, seed=dim)
+    cand = rng.integers(-1, n, size=(n, K)).astype(np.int32)
+    cand[:, 5] = np.arange(n)               # the node itself is skipped
+    cand[:, 7] = cand[:, 3]                 # repeats count once
+    xd = torch.from_numpy(x).cuda()
+    order = torch.from_numpy(rng.permutation(n)).cuda()
+    out, cnt = prune(xd, torch.from_numpy(cand).cuda(), R, alpha, order)
+    out, cnt = out.cpu().numpy(), cnt.cpu().numpy()
+    for v in rng.choice(n, 60, replace=False):
+        kept = prune_model(x, int(v), cand[v], R, alpha)
+        assert cnt[v] == len(kept)
+        assert out[v, :len(kept)].tolist() == kept
+        assert (out[v, len(kept):] == -1).all()
+
+
+@pytest.mark.gpu
+def test_build_nsg_small_graph_searchable():
+    from falcon_b200 import FalconIndex
+    from falcon_b200.groundtruth import brute_force_f64, recall_at_k
+    from falcon_b200.nsg import build_nsg
+    from falcon_b200.synthetic import sift_like
+    x = sift_like(20000, 32, seed=3)
+    q = sift_like(200, 32, seed=4)
+    st = {}
+    g = build_nsg(x, max_degree=32, seed=1, knn_k=48, n_clusters=40, n_probe=8, stats=st)
+    assert st["unreached_after"] == 0
+    adj = g.adjacency()
+    assert adj.shape == (20000, 32) and adj.max() < 20000
+    ix = FalconIndex(g)
+    r = ix.search(q, k=10, ef=128, cand_queue_size=64, bloom_bits=16)
+    gt, _ = brute_force_f64(x, q, 10)
+    assert recall_at_k(r.ids, gt, 10) > 0.9
+    ix.close()

@@ -101,4 +101,15 @@ def test_noalloc_rejects_oversized_and_ef_below_k():
     assert "4 MiB" in _lib.last_error()
     rc = _run(lib, "falcon_search_noalloc", ix, torch.from_numpy(q).cuda(), make_params(k=20, ef=10), False, 20)[0]
     assert rc == _lib.FALCON_ERR_ARG
+    # a negative query count and a query stride below the dimension are refused
+    # before anything is queued on the stream
+    dq = torch.from_numpy(q).cuda()
+    out_i = torch.zeros((len(q), 10), dtype=torch.int32, device="cuda")
+    out_d = torch.zeros((len(q), 10), dtype=torch.float32, device="cuda")
+    p = make_params(k=10, ef=64)
+    for nq, stride in ((-1, 96), (len(q), 95)):
+        rc = lib.falcon_search_noalloc(ix._h, dq.data_ptr(), nq, stride, None, ctypes.byref(p), 0, out_i.data_ptr(),
+                                       out_d.data_ptr(), 10, None, None, None)
+        assert rc == _lib.FALCON_ERR_ARG, (nq, stride)
+    torch.cuda.synchronize()
     ix.close()
