@@ -1,15 +1,29 @@
 """Benchmark: QPS at recall@10 >= 0.95 (plus p50/p99 latency) of the graph
-traversal path on B200, against the reference's CPU search on the host cores.
+traversal path on B200, plain vs batched/served, against the reference's CPU
+search on the host cores.
 
-Workload (one GPU): 1M base vectors, D=96, i.i.d. N(0,1) rows normalised to
-unit norm (seeded stand-in for Deep1M), 10k queries of the same distribution,
-single-layer graph of max degree 64 (HNSW M=32 base layer), k=10, ef in
-{64,128,256}, mc in {1,2,4}.  A step is one batched search of the 10k queries.
-The operating point is the fastest (ef, mc, mg) of a short sweep whose
-recall@10 (against FP64 ground truth) is >= 0.95; if none reaches it, the
-highest-recall point is used and the JSON says so.
+Headline (one GPU): the batched persistent kernel on a flat graph --
+10M base vectors, D=128, integers round(|N(0,40)|) clipped to [0,255]
+(seeded stand-in for SIFT10M), NSG-style single-layer graph of max degree 64
+from the medoid built on the GPU (seed 1), 100k queries in ONE launch with ef
+drawn from {32,64,128,256}, k from {1,10,100} and mc from {1,2,4} per query
+(seeded).  A step is that launch with the queries resident in HBM; `e2e`
+repeats it through the public API from pinned host buffers.  Recall is scored
+against FP64 ground truth on the first 10k queries.  Beside it, the same
+graph and queries at uniform k=10 and growing ef, to show where recall@10
+reaches 0.95.
 
-usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Extra keys (the other workloads, same run):
+  cfg0: 100k x 128 sift-like, HNSW-style M=16 graph, 1000 queries, k=10, ef=64, mc=1
+  cfg1: 1M x 96 unit-normal, HNSW-style M=32, 10k queries: throughput sweep to
+        recall >= 0.95, batch-1 latency grid ef {64,128,256} x mc {1,2,4}
+        (inter and intra), BF16/FP8 traversal + FP32 rerank, served
+  cfg3: 1M x 384 unit-normal, HNSW-style M=32, BF16 and FP8-E4M3 traversal
+        with FP32 rerank, ef {64,128}, mc=2, distance error vs FP64
+  cfg4: cfg2 and cfg3 resident together, Poisson arrivals 10k-500k QPS,
+        each request a random index, k, ef and mc; p50/p99 and sustained QPS
+
+usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--configs 2,0,1,3,4]
        multi-GPU: python -m torch.distributed.run --nproc-per-node N bench.py --gpus N
 """
 import argparse
@@ -26,24 +40,16 @@ import numpy as np
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(REPO, "falcon-accelerate-graph-vector-search_b200"))
 
-N_BASE = 1_000_000
-DIM = 96
-N_QUERIES = 10_000
-MAX_DEGREE = 64
-K = 10
 RECALL_TARGET = 0.95
-WORKLOAD = ("deep1m_hnsw_m32: 1M x 96 unit-normal base, 10k queries, HNSW M=32 (degree-64 base layer + upper "
-            "layers), k=10")
-HNSW_M = 32
-# (ef, mc, mg, cand_queue_size, bloom_bits): the configuration's ef values with
-# the reference's 32-entry candidate queue and 2^16-bit Bloom filter, then
-# larger ef, queues and filters (a query here visits 10^4-10^5 nodes, which
-# saturates a 2^16-bit filter; 2^19 bits keep the per-warp filters of a full
-# GPU near the L2 size at a false-positive rate that still reaches the recall
-# target)
-SWEEP = ([(ef, mc, mg, 32, 16) for ef in (64, 128, 256) for mc in (1, 2, 4) for mg in (1, 4)] +
-         [(ef, mc, 1, cq, 20) for ef in (256, 512, 1024) for cq in (64, 256) for mc in (1, 2)] +
-         [(ef, 1, 1, cq, 19) for ef in (768, 896, 1024) for cq in (128, 256)])
+METRIC = "QPS at recall@10>=0.95 (batched search; plain vs batched/served)"
+
+# the headline workload
+CFG2 = dict(n=10_000_000, dim=128, nq=100_000, degree=64, seed_data=0, seed_query=1, seed_graph=1, ngt=10_000,
+            efs=(32, 64, 128, 256), ks=(1, 10, 100), mcs=(1, 2, 4), cq=32, bits=16, param_seed=7,
+            search_passes=((128, 1.0),))
+WORKLOAD2 = ("sift10m_nsg_r64: 10M x 128 clipped-integer base (seeded SIFT10M stand-in), NSG-style graph max degree 64 "
+             "from the medoid (GPU-built, seed 1), 100k queries in one launch, per-query ef in {32,64,128,256}, "
+             "k in {1,10,100}, mc in {1,2,4}")
 
 
 def log(*a):
@@ -55,31 +61,6 @@ def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return ws, rank, local
-
-
-def make_workload(rank, device, upper_layers=False):
-    from falcon_b200.graph import build_graph, build_upper_layers
-    from falcon_b200.groundtruth import shortlist_f64
-    from falcon_b200.synthetic import unit_normal
-    t = time.time()
-    x = unit_normal(N_BASE, DIM, seed=0)
-    q = unit_normal(N_QUERIES, DIM, seed=1 + 1000 * rank)
-    log("data %.1fs" % (time.time() - t))
-    t = time.time()
-    g = build_graph(x, MAX_DEGREE, device=device)
-    log("graph %.1fs (mean degree %.1f)" % (time.time() - t, g.counts().mean()))
-    upper = None
-    if upper_layers:
-        t = time.time()
-        upper = build_upper_layers(x, HNSW_M, seed=0, device=device)
-        log("upper layers %.1fs (levels %d, %d nodes above the base)" % (time.time() - t, upper.max_level,
-                                                                          int((upper.levels > 0).sum())))
-    t = time.time()
-    gt, _ = shortlist_f64(x, q, K, device=device)
-    log("ground truth %.1fs" % (time.time() - t))
-    if upper_layers:
-        return x, q, g, gt, upper
-    return x, q, g, gt
 
 
 class ClockSampler:
@@ -136,6 +117,26 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def measured_peak():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(hops, visited, dim, degree, ks, efs=None, elem_bytes=4, scale_bytes=0, rerank=False):
+    """Bytes each query must move, summed: its gathered vectors, its expanded
+    adjacency rows (count word + max_degree ids), the query and its k results
+    (id + distance); with a rerank the FP32 vectors of its ef candidates."""
+    dpad = (dim + 15) // 16 * 16
+    b = visited.astype(np.float64) * (dpad * elem_bytes + scale_bytes) + hops.astype(np.float64) * (4 + 4 * degree)
+    b += dim * 4 + np.asarray(ks, dtype=np.float64) * 8
+    if rerank:
+        b += np.asarray(efs, dtype=np.float64) * dpad * 4
+    return float(b.sum())
+
+
 def distance_error_f64(x, q, ids, dists):
     """Relative error of returned distances against FP64 recomputation (same
     ids): max and mean over all valid results."""
@@ -149,244 +150,560 @@ def distance_error_f64(x, q, ids, dists):
     return {"max_rel": float(rel.max()), "mean_rel": float(rel.mean())}
 
 
-def algorithmic_bytes(hops, visited, ef, elem_bytes=4, rerank=False):
-    """Bytes a query must move: gathered vectors, adjacency rows (count word +
-    max_degree ids per hop), the query and the k results."""
-    b = visited.astype(np.float64) * DIM * elem_bytes + hops.astype(np.float64) * (4 + 4 * MAX_DEGREE)
-    if rerank:
-        b += ef * DIM * 4
-    return float((b + DIM * 4 + K * 8).sum())
-
-
-def measured_peak():
-    p = os.path.join(REPO, "MEASURED_PEAKS.json")
-    if os.path.exists(p):
-        d = json.load(open(p))
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
-
-
-def sweep(ix, q, gt):
-    from falcon_b200.groundtruth import recall_at_k
+def timed(fn, reps=3):
+    """Best CUDA-event time (ms) of fn() over reps, after one warm call; returns (ms, last result)."""
     import torch
-    res = []
-    dq = torch.from_numpy(q).cuda()
-    for ef, mc, mg, cq, bits in SWEEP:
-        r = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
+    r = fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = float("inf")
+    for _ in range(reps):
+        a.record()
+        r = fn()
+        b.record()
         torch.cuda.synchronize()
-        t0 = torch.cuda.Event(enable_timing=True)
-        t1 = torch.cuda.Event(enable_timing=True)
-        ms = 1e30
-        for _ in range(2):
-            t0.record()
-            r = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
-            t1.record()
-            torch.cuda.synchronize()
-            ms = min(ms, t0.elapsed_time(t1))
-        rec = recall_at_k(r.ids.cpu().numpy(), gt, K)
-        res.append(dict(ef=ef, mc=mc, mg=mg, cq=cq, bits=bits, recall=rec, ms=ms, qps=len(q) / ms * 1e3))
-        log("sweep ef=%d mc=%d mg=%d cq=%d bits=%d recall=%.4f %.2f ms %.0f QPS" % (
-            ef, mc, mg, cq, bits, rec, ms, len(q) / ms * 1e3))
-    ok = [r for r in res if r["recall"] >= RECALL_TARGET]
-    best = max(ok, key=lambda r: r["qps"]) if ok else max(res, key=lambda r: (r["recall"], r["qps"]))
-    return best, bool(ok), res
+        best = min(best, a.elapsed_time(b))
+    return best, r
 
 
-def serve_measurements(ix, q, gt, ef, mc, mg, cq, bits, batched_bf16_qps):
-    """Continuous batching: single-query requests with Poisson arrivals through
-    the serving kernel (BF16 traversal + exact FP32 rerank), at fractions of the
-    batched BF16 throughput and at saturation.  Reports sustained QPS (completed
-    requests / wall time), p50/p99 latency (arrival to completion, queueing
-    included) and recall@10 of the served results."""
+def batch1_latency(ix, dq, n, **p):
+    """p50/p99 (ms) of one-query search calls, CUDA events around each call."""
+    import torch
+    lat = []
+    for i in range(n):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        ix.search(dq[i:i + 1], **p)
+        b.record()
+        b.synchronize()
+        lat.append(a.elapsed_time(b))
+    lat = np.array(lat[min(10, n // 4):])
+    return float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
+
+
+def rounded(d):
+    return {k: (round(v, 5) if isinstance(v, float) else v) for k, v in d.items()}
+
+
+# ---------------------------------------------------------------------------
+# configs[2]: data, graph, ground truth, mixed per-query parameters
+# ---------------------------------------------------------------------------
+def cfg2_params(nq):
+    """Per-query (ef, k, mc) drawn by a seeded generator; ef is raised to k."""
+    rng = np.random.default_rng(CFG2["param_seed"])
+    efs = rng.choice(CFG2["efs"], nq)
+    ks = rng.choice(CFG2["ks"], nq)
+    mcs = rng.choice(CFG2["mcs"], nq)
+    return np.maximum(efs, ks), ks, mcs
+
+
+def cfg2_workload(dev, rank=0, timings=None):
+    """Base, queries (seeded by rank for replicas), graph (host formats.Graph),
+    FP64 ground truth (top 100) of the first ngt queries."""
+    import torch
+    from falcon_b200.groundtruth import shortlist_f64_tiled
+    from falcon_b200.nsg import build_nsg
+    from falcon_b200.synthetic import sift_like_blocks
+    tm = timings if timings is not None else {}
+    t = time.time()
+    x = sift_like_blocks(CFG2["n"], CFG2["dim"], seed=CFG2["seed_data"])
+    q = sift_like_blocks(CFG2["nq"], CFG2["dim"], seed=CFG2["seed_query"] + 1000 * rank)
+    tm["data_s"] = time.time() - t
+    xd = torch.from_numpy(x).to(dev)
+    st = {}
+    t = time.time()
+    g = build_nsg(x, CFG2["degree"], seed=CFG2["seed_graph"], search_passes=CFG2["search_passes"], device=dev,
+                  vectors_device=xd, stats=st, verbose=True)
+    tm["graph_s"] = time.time() - t
+    t = time.time()
+    gt, _ = shortlist_f64_tiled(x, q[:CFG2["ngt"]], 100, shortlist=128, base_device=xd, device=dev)
+    tm["ground_truth_s"] = time.time() - t
+    del xd
+    torch.cuda.empty_cache()
+    log("cfg2 workload: %s" % rounded(tm))
+    return x, q, g, gt, st
+
+
+def mixed_recall(ids, gt, ks):
+    """recall@10 over the queries with k >= 10 (first 10 results against the
+    10 true nearest), recall@1 over k = 1, recall@100 over k = 100."""
+    from falcon_b200.groundtruth import recall_at_k
+    n = len(gt)
+    ids, ks = np.asarray(ids)[:n], np.asarray(ks)[:n]
+    out = {}
+    m10 = ks >= 10
+    if m10.any():
+        out["recall@10_k>=10"] = recall_at_k(ids[m10], gt[m10], 10)
+    m1 = ks == 1
+    if m1.any():
+        out["recall@1_k=1"] = recall_at_k(ids[m1], gt[m1], 1)
+    m100 = ks == 100
+    if m100.any():
+        out["recall@100_k=100"] = recall_at_k(ids[m100], gt[m100], 100)
+    out["queries_scored"] = int(n)
+    return out
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def headline_cfg2(args, dev, local, rank, ws, out):
+    import torch
+    from falcon_b200 import FalconIndex, make_params
+    from falcon_b200.index import params_array
+    tm = {}
+    x, q, g, gt, gstats = cfg2_workload(dev, rank, tm)
+    t = time.time()
+    ix = FalconIndex(g, device=local)
+    tm["index_s"] = time.time() - t
+    nq = len(q)
+    efs, ks, mcs = cfg2_params(nq)
+    parr = params_array([make_params(k=int(k), ef=int(e), mc=int(m), mg=1, cand_queue_size=CFG2["cq"],
+                                     bloom_bits=CFG2["bits"]) for e, k, m in zip(efs, ks, mcs)])
+    dq = torch.from_numpy(q).to(dev)
+    for _ in range(args.warmup):
+        r = ix.search(dq, per_query=parr)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if args.profile_region:
+        torch.cuda.profiler.start()
+    with ClockSampler(local) as clk:
+        ev0.record()
+        for _ in range(args.steps):
+            r = ix.search(dq, per_query=parr)
+        ev1.record()
+        torch.cuda.synchronize()
+    if args.profile_region:
+        torch.cuda.profiler.stop()
+    ms = ev0.elapsed_time(ev1)
+    if ws > 1:
+        tt = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        ms = float(tt.item())
+        torch.distributed.barrier()
+    ms_step = ms / args.steps
+    ids = r.ids.cpu().numpy()
+    hops, vis = r.hops.cpu().numpy(), r.visited.cpu().numpy()
+    rec = mixed_recall(ids, gt, ks)
+    log("cfg2 headline: %.2f ms/step, %.0f QPS, %s, hops %.1f visited %.1f" % (
+        ms_step, nq / ms_step * 1e3, rounded(rec), hops.mean(), vis.mean()))
+    if args.profile_region:
+        print(json.dumps({"profiled_steps": args.steps, "search": "cfg2 mixed", "ms_per_step": ms_step,
+                          "n_base": CFG2["n"], "queries_per_step": nq, "hops_mean": float(hops.mean()),
+                          "visited_mean": float(vis.mean()),
+                          "bytes_per_query": algorithmic_bytes(hops, vis, CFG2["dim"], CFG2["degree"], ks) / nq}))
+        ix.close()
+        return None
+
+    # end to end through the public API: pinned host queries, host results
+    qh = torch.from_numpy(q).pin_memory().numpy()
+    e2e = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        rh = ix.search(qh, per_query=parr)
+        if i >= args.warmup:
+            e2e.append(time.perf_counter() - t)
+    e2e_ms = sum(e2e) / len(e2e) * 1e3
+    if ws > 1:
+        tt = torch.tensor([e2e_ms], device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    same = bool(np.array_equal(rh.ids, ids) and np.array_equal(rh.hops, hops))
+
+    peak, peak_kind = measured_peak()
+    alg = algorithmic_bytes(hops, vis, CFG2["dim"], CFG2["degree"], ks)
+    achieved = alg / (ms_step / 1e3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "peak_kind": peak_kind, "bytes_per_query": alg / nq,
+            "kernel": "inter_kernel<f32, EPL=8, VROWS=1>",
+            "achieved_from": "algorithmic bytes of the step / CUDA-event step time (the search kernel is the "
+                             "step's only kernel)"}
+    traffic_from_profile(roof, "cfg2_mixed", alg)
+    out.update({
+        "metric": METRIC, "value": ws * nq / (ms_step / 1e3), "unit": "queries/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded clipped-integer stand-in for SIFT10M; the reference's datasets are not available)",
+        "config": {"workload": WORKLOAD2, "queries_per_step": nq, "per_query": "ef/k/mc drawn per query (seed 7), "
+                   "ef raised to k, cand_queue_size 32, bloom_bits 16, mg 1 (the reference defaults)",
+                   "mode": "inter", "recall": rec, "recall_target_reached": bool(rec.get("recall@10_k>=10", 0) >=
+                                                                             RECALL_TARGET),
+                   "hops_mean": float(hops.mean()), "visited_mean": float(vis.mean()),
+                   "graph": {k: v for k, v in gstats.items() if not k.endswith("_s")},
+                   "graph_build_s": round(gstats.get("build_s", 0.0), 1), "timings_s": rounded(tm),
+                   "parallelism": "replicas" if ws > 1 else "single",
+                   "l2": "inputs larger than L2 (5.1 GB vectors + 3.2 GB links vs 126 MB L2)"},
+        "e2e": {"value": ws * nq / (e2e_ms / 1e3), "unit": "queries/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(q.nbytes + nq * 48),
+                "d2h_bytes_per_step": int(nq * int(ks.max()) * 8 + nq * 8),
+                "results_equal_device_run": same},
+        "gpu_launches": args.steps,   # one search kernel per step (no upper layers on this graph)
+        "clocks": clk.summary(),
+        "roofline": roof,
+    })
+    return dict(ix=ix, x=x, q=q, g=g, gt=gt, dq=dq, parr=parr, efs=efs, ks=ks, mcs=mcs, ids=ids,
+                dists=r.dists.cpu().numpy(), hops=hops, vis=vis)
+
+
+def traffic_from_profile(roof, key, alg_bytes):
+    """DRAM traffic per launch from the ncu capture recorded in
+    profiles/traffic.json, used only while it was taken on the current kernel
+    source (the file records the source's hash)."""
+    import hashlib
+    tp = os.path.join(REPO, "profiles", "traffic.json")
+    if not os.path.exists(tp):
+        return
+    tr = json.load(open(tp))
+    e = tr.get(key)
+    src = os.path.join(REPO, "falcon-accelerate-graph-vector-search_b200", "csrc", "falcon_kernels.cu")
+    h = hashlib.sha256(open(src, "rb").read()).hexdigest()[:16]
+    if not e or e.get("kernel_source_sha16") != h:
+        roof["traffic_note"] = "no ncu capture of the current kernel source for this workload"
+        return
+    roof["traffic"] = e["ratio"] * alg_bytes
+    roof["traffic_ratio"] = e["ratio"]
+    roof["traffic_note"] = e["note"]
+
+
+def recall_curve_cfg2(H, out):
+    """Same graph and the ground-truth queries at uniform k=10 and growing ef:
+    the smallest ef whose recall@10 reaches the target, or the best reached."""
+    import torch
+    from falcon_b200.groundtruth import recall_at_k
+    ix, dq, gt = H["ix"], H["dq"], H["gt"]
+    n = len(gt)
+    pts = []
+    for ef, cq, bits, mc, mg in ((64, 32, 16, 1, 1), (256, 32, 16, 1, 1), (256, 64, 18, 2, 4), (512, 128, 18, 1, 1),
+                                 (1024, 256, 20, 1, 1), (1024, 256, 20, 2, 4)):
+        ms, r = timed(lambda: ix.search(dq[:n], k=10, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits), 2)
+        rec = recall_at_k(r.ids.cpu().numpy(), gt, 10)
+        pts.append(dict(ef=ef, cq=cq, bits=bits, mc=mc, mg=mg, recall=rec, qps=n / ms * 1e3,
+                        visited=float(r.visited.float().mean()), hops=float(r.hops.float().mean())))
+        log("cfg2 uniform k=10: %s" % rounded(pts[-1]))
+    ok = [p for p in pts if p["recall"] >= RECALL_TARGET]
+    best = min(ok, key=lambda p: (p["ef"], -p["qps"])) if ok else max(pts, key=lambda p: p["recall"])
+    out["cfg2_uniform_k10"] = {"queries": n, "points": [rounded(p) for p in pts], "selected": rounded(best),
+                               "recall_target_reached": bool(ok),
+                               "note": "i.i.d. coordinates give full intrinsic dimension (128): graph search needs "
+                                       "a large ef on this stand-in; the kernel's ef limit is 1024"}
+
+
+def cpu_baselines_cfg2(H, out, threads, budget_s=15.0):
+    """Reference CPU search (the reference's vendored hnswlib, built from its
+    headers) on the same graph from the same medoid with the same per-query ef
+    and k, all host threads, bounded sample; then the oracle (the C
+    restatement of the FPGA traversal) on a smaller sample, whose results are
+    also compared bit for bit with the GPU's rows for the same queries."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    g, q, gt = H["g"], H["q"], H["gt"]
+    efs, ks, mcs = H["efs"], H["ks"], H["mcs"]
+    res = {}
+    if oracle.Hnsw.available():
+        t = time.time()
+        h = oracle.Hnsw.from_graph(g.vectors, g.adjacency(), g.entry_point)
+        load_s = time.time() - t
+        n = min(len(gt), 2000)
+        t = time.time()
+        h.search_mixed(q[:n], ks[:n], efs[:n], threads)
+        dt = time.time() - t
+        reps = int(max(1, min(10, budget_s / max(dt, 1e-3))))
+        n = int(min(len(gt), max(n, n * reps)))
+        t = time.time()
+        lab, _ = h.search_mixed(q[:n], ks[:n], efs[:n], threads)
+        dt = time.time() - t
+        h.free()
+        res["cpu_baseline"] = {"value": n / dt, "unit": "queries/s", "cores": threads, "kind": "reference",
+                               "isa": oracle.Hnsw.isa(), "cpu": oracle.Hnsw.cpu_model(),
+                               "sample": "first %d of the 100k queries, hnswlib searchKnn with each query's ef and k "
+                                         "(setEf per (ef, k) group), base layer from the same medoid; mc has no "
+                                         "hnswlib counterpart" % n,
+                               "recall": mixed_recall(lab, gt[:n], ks[:n]), "graph_load_s": load_s}
+        log("cfg2 cpu baseline: %s" % rounded({k: v for k, v in res["cpu_baseline"].items() if k != "recall"}))
+    # oracle port + parity sample
+    og = oracle.OracleGraph(g.vectors, g.links, g.max_degree, g.ids_offset)
+    m = min(len(q), 4 * threads)
+    plist = [oracle.make_params(k=int(k), ef=int(e), mc=int(c), mg=1, cand_queue_size=CFG2["cq"],
+                                bloom_bits=CFG2["bits"]) for e, k, c in zip(efs[:m], ks[:m], mcs[:m])]
+    t = time.time()
+    ids, d, hops, vis, _ = oracle.search(og, q[:m], g.entry_point, plist, out_stride=H["ids"].shape[1],
+                                         threads=threads)
+    dt = time.time() - t
+    exact = [bool(np.array_equal(ids[i], H["ids"][i]) and np.array_equal(d[i].view(np.uint32),
+                                                                         H["dists"][i].view(np.uint32))
+                  and hops[i] == H["hops"][i] and vis[i] == H["vis"][i]) for i in range(m)]
+    res["cpu_fpga_semantics_port"] = {"value": m / dt, "unit": "queries/s", "cores": threads, "kind": "port",
+                                      "sample": "first %d queries, oracle (C restatement of the FPGA traversal) with "
+                                                "the GPU's per-query parameters" % m}
+    res["parity_sample"] = {"queries": m, "bit_exact": int(sum(exact)),
+                            "compared": "ids, distance bits, hops, visited of the GPU headline rows against the "
+                                        "oracle on the same 10M graph"}
+    log("cfg2 parity sample: %d/%d bit-exact; oracle %.1f QPS" % (sum(exact), m, m / dt))
+    del og
+    return res
+
+
+def run_cfg1(args, dev, local, out):
+    """1M x 96 unit-normal, HNSW-style M=32; throughput at the
+    recall target, batch-1 latency grid, reduced precision + rerank, served."""
+    import torch
+    from falcon_b200 import FalconIndex
+    from falcon_b200.autotune import channel_bloom_bits
+    from falcon_b200.graph import build_graph, build_upper_layers
+    from falcon_b200.groundtruth import recall_at_k, shortlist_f64
+    from falcon_b200.synthetic import unit_normal
+    n, dim, nq, k = args.cfg1_n, 96, 10_000, 10
+    t0 = time.time()
+    x = unit_normal(n, dim, seed=0)
+    q = unit_normal(nq, dim, seed=1)
+    g = build_graph(x, 64, device=dev)
+    upper = build_upper_layers(x, 32, seed=0, device=dev)
+    gt, _ = shortlist_f64(x, q, k, device=dev)
+    ix = FalconIndex(g, storage=("f32", "bf16", "fp8"), device=local)
+    ix.set_upper_layers(upper)
+    dq = torch.from_numpy(q).to(dev)
+    build_s = time.time() - t0
+    sweep = [(64, 1, 1, 32, 16), (128, 1, 1, 32, 16), (256, 1, 1, 32, 16), (256, 2, 4, 32, 16),
+             (512, 1, 1, 64, 20), (1024, 1, 1, 256, 19), (1024, 2, 4, 256, 19), (1024, 1, 4, 256, 19)]
+    pts = []
+    for ef, mc, mg, cq, bits in sweep:
+        ms, r = timed(lambda: ix.search(dq, k=k, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits), 2)
+        rec = recall_at_k(r.ids.cpu().numpy(), gt, k)
+        pts.append(dict(ef=ef, mc=mc, mg=mg, cq=cq, bits=bits, recall=rec, qps=nq / ms * 1e3, ms=ms,
+                        hops=float(r.hops.float().mean()), visited=float(r.visited.float().mean())))
+        log("cfg1 sweep %s" % rounded(pts[-1]))
+    ok = [p for p in pts if p["recall"] >= RECALL_TARGET]
+    sel = max(ok, key=lambda p: p["qps"]) if ok else max(pts, key=lambda p: p["recall"])
+    ef, mc, mg, cq, bits = sel["ef"], sel["mc"], sel["mg"], sel["cq"], sel["bits"]
+    P = dict(k=k, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
+    ms_b, rb = timed(lambda: ix.search(dq, precision="bf16", rerank=True, **P))
+    ms_f, rf = timed(lambda: ix.search(dq, precision="fp8", rerank=True, **P))
+    r = ix.search(dq, **P)
+    derr = {"f32": distance_error_f64(x, q, r.ids.cpu().numpy(), r.dists.cpu().numpy())}
+    for prec, res in (("bf16", rb), ("fp8", rf)):
+        raw = ix.search(dq, precision=prec, **P)
+        derr[prec + "_rerank"] = distance_error_f64(x, q, res.ids.cpu().numpy(), res.dists.cpu().numpy())
+        derr[prec + "_traversal"] = distance_error_f64(x, q, raw.ids.cpu().numpy(), raw.dists.cpu().numpy())
+        derr[prec + "_traversal"]["recall@10"] = recall_at_k(raw.ids.cpu().numpy(), gt, k)
+    # batch-1 latency grid (configs[1]: ef {64,128,256} x mc {1,2,4}), inter and intra (4 channels)
+    grid = []
+    for ef_l in (64, 128, 256):
+        for mc_l in (1, 2, 4):
+            row = {"ef": ef_l, "mc": mc_l}
+            for mode, extra in (("inter", {}), ("intra4", dict(mode="intra", channels=4))):
+                pl = dict(k=k, ef=ef_l, mc=mc_l, mg=1, cand_queue_size=32, bloom_bits=16, **extra)
+                p50, p99 = batch1_latency(ix, dq, args.latency_samples, **pl)
+                rr = ix.search(dq[:2000], **pl)
+                row[mode] = {"p50_ms": p50, "p99_ms": p99, "recall@10": recall_at_k(rr.ids.cpu().numpy(), gt[:2000], k)}
+            grid.append(row)
+            log("cfg1 batch-1 %s" % row)
+    # batch-1 at the throughput operating point
+    lat_sel = {}
+    for mode, extra in (("inter", {}), ("intra4", dict(mode="intra", channels=4,
+                                                       bloom_bits=channel_bloom_bits(bits, 4)))):
+        pl = dict(P)
+        pl.update(extra)
+        p50, p99 = batch1_latency(ix, dq, args.latency_samples, **pl)
+        lat_sel[mode] = {"p50_ms": p50, "p99_ms": p99}
+    served = None if args.no_serve else serve_cfg1(ix, q, gt, P, nq / (ms_b / 1e3))
+    ix.close()
+    out["cfg1"] = {
+        "workload": "deep1m_hnsw_m32: 1M x 96 unit-normal (seeded Deep1M stand-in), HNSW-style M=32 graph (exact "
+                    "kNN + hnswlib's neighbour heuristic + reverse edges, upper layers with hnswlib's level "
+                    "distribution), 10k queries, k=10; searches descend the upper layers",
+        "n_base": n, "build_s": build_s, "sweep": [rounded(p) for p in pts], "selected": rounded(sel),
+        "recall_target_reached": bool(ok),
+        "bf16_rerank": {"value": nq / (ms_b / 1e3), "unit": "queries/s",
+                        "recall@10": recall_at_k(rb.ids.cpu().numpy(), gt, k)},
+        "fp8_rerank": {"value": nq / (ms_f / 1e3), "unit": "queries/s",
+                       "recall@10": recall_at_k(rf.ids.cpu().numpy(), gt, k)},
+        "distance_error_vs_f64": derr, "latency_batch1_grid": grid, "latency_batch1_selected": lat_sel,
+        "served": served}
+
+
+def serve_cfg1(ix, q, gt, P, batched_bf16_qps):
+    """Continuous batching of single-query requests (BF16 traversal + exact
+    FP32 rerank) with Poisson arrivals at 50 %, 80 % of the batched BF16 rate
+    and at saturation."""
     from falcon_b200 import make_params
     from falcon_b200.groundtruth import recall_at_k
     from falcon_b200.serving import FalconServer, poisson_arrivals
-    sv = FalconServer(ring_capacity=65536, max_k=K, ef_max=ef, cand_queue_max=cq, bloom_bits_max=bits,
-                      mc_max=max(mc, 1), mg_max=max(mg, 1), dim_max=DIM, idle_exit_us=5000)
+    k = P["k"]
+    sv = FalconServer(ring_capacity=65536, max_k=k, ef_max=P["ef"], cand_queue_max=P["cand_queue_size"],
+                      bloom_bits_max=P["bloom_bits"], mc_max=max(P["mc"], 1), mg_max=max(P["mg"], 1), dim_max=96,
+                      idle_exit_us=5000)
     iid = sv.add_index(ix)
-    p = make_params(k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, precision="bf16", rerank=True)
-    n = 2 * N_QUERIES
+    p = make_params(precision="bf16", rerank=True, **P)
+    n = 2 * len(q)
     qq = np.concatenate([q, q])
     out = {"precision": "bf16+fp32 rerank", "requests_per_point": n, "points": [],
-           "entry": "each request descends the HNSW upper layers (replay submits micro-batches of up to 200 us)"}
-    sv.replay(np.full(1000, iid), qq[:1000], p, poisson_arrivals(1000, batched_bf16_qps, 9), K)   # warm-up
+           "entry": "each request descends the HNSW upper layers"}
+    sv.replay(np.full(1000, iid), qq[:1000], p, poisson_arrivals(1000, batched_bf16_qps, 9), k)
     for frac in (0.5, 0.8, 10.0):
         rate = batched_bf16_qps * frac
         arr = poisson_arrivals(n, rate, seed=int(frac * 100))
-        lat, ids, d, hops, vis, el = sv.replay(np.full(n, iid), qq, p, arr, K)
-        rec = recall_at_k(ids[:N_QUERIES], gt, K)
-        pt = {"offered_qps": rate if frac < 10 else None, "offered": "saturation" if frac >= 10 else "%.0f%%" % (frac * 100),
+        lat, ids, d, hops, vis, el = sv.replay(np.full(n, iid), qq, p, arr, k)
+        pt = {"offered_qps": rate if frac < 10 else None,
+              "offered": "saturation" if frac >= 10 else "%.0f%%" % (frac * 100),
               "sustained_qps": n / (el / 1e6), "p50_ms": float(np.percentile(lat, 50)) / 1e3,
-              "p99_ms": float(np.percentile(lat, 99)) / 1e3, "recall@10": rec}
-        log("served %s: %.0f QPS sustained, p50 %.2f ms, p99 %.2f ms, recall %.4f" % (
-            pt["offered"], pt["sustained_qps"], pt["p50_ms"], pt["p99_ms"], rec))
+              "p99_ms": float(np.percentile(lat, 99)) / 1e3, "recall@10": recall_at_k(ids[:len(q)], gt, k)}
+        log("cfg1 served %s" % rounded(pt))
         out["points"].append(pt)
-    inf = sv.info()
-    out["kernel_launches"] = int(inf.kernel_launches)
-    out["ring_entries"] = int(inf.ring_entries)
     sv.close()
     return out
 
 
-def cpu_baseline(x, q, g, gt, ef, threads, budget_s=15.0):
-    """Reference CPU search (vendored hnswlib, built from the reference's
-    headers) on the same graph, all host threads, bounded sample."""
-    sys.path.insert(0, os.path.join(REPO, "oracle"))
-    import oracle
-    from falcon_b200.groundtruth import recall_at_k
-    if not oracle.Hnsw.available():
-        return None
-    h = oracle.Hnsw.from_graph(x, g.adjacency(), g.entry_point)
-    n = min(len(q), 2000)
-    t = time.time()
-    lab, _ = h.search(q[:n], K, ef, threads)
-    dt = time.time() - t
-    # grow the sample to roughly the time budget
-    reps = max(1, int(budget_s / max(dt, 1e-3)) - 1)
-    reps = min(reps, 20)
-    t = time.time()
-    for _ in range(reps):
-        h.search(q[:n], K, ef, threads)
-    dt = (time.time() - t) / reps
-    rec = recall_at_k(lab, gt[:n], K)
-    h.free()
-    return {"value": n / dt, "unit": "queries/s", "cores": threads, "kind": "reference",
-            "sample": "%d queries x %d reps, hnswlib searchKnn setEf(%d) on the same graph" % (n, reps + 1, ef),
-            "recall@10": rec}
-
-
-def mixed_params(ix, q, steps=3):
-    """One persistent launch over queries of uneven cost: per query ef from
-    {32, 64, 128, 256}, k from {1, 10, 100} (ef raised to k), mc from {1, 2, 4},
-    the reference's 32-entry candidate queue and 2^16-bit filter; host query
-    and result buffers (copies inside the timed calls)."""
-    from falcon_b200 import make_params
-    rng = np.random.default_rng(7)
-    n = len(q)
-    efs, ks, mcs = rng.choice([32, 64, 128, 256], n), rng.choice([1, 10, 100], n), rng.choice([1, 2, 4], n)
-    per = [make_params(k=int(k), ef=int(max(e, k)), mc=int(m), mg=1, cand_queue_size=32, bloom_bits=16)
-           for e, k, m in zip(efs, ks, mcs)]
-    ix.search(q, per_query=per)
-    t = time.perf_counter()
-    for _ in range(steps):
-        r = ix.search(q, per_query=per)
-    dt = (time.perf_counter() - t) / steps
-    return {"value": n / dt, "unit": "queries/s", "queries_per_step": n, "ms_per_step": dt * 1e3,
-            "params": "ef in {32,64,128,256}, k in {1,10,100}, mc in {1,2,4} per query (seeded), cq 32, 2^16 bits",
-            "hops_mean": float(r.hops.mean()), "visited_mean": float(r.visited.mean())}
-
-
-def cpu_port(q, g, gt, ef, mc, mg, cq, bits, threads, budget_s=10.0):
-    """The C restatement of the FPGA semantics (the parity oracle: literal
-    systolic queues, Bloom filter, adder tree) timed on the host cores, on a
-    bounded sample of the same queries and parameters."""
-    sys.path.insert(0, os.path.join(REPO, "oracle"))
-    import oracle
-    from falcon_b200.groundtruth import recall_at_k
-    og = oracle.OracleGraph(g.vectors, g.links, g.max_degree, g.ids_offset)
-    p = oracle.make_params(k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
-    n = min(len(q), 2 * threads)
-    t = time.time()
-    oracle.search(og, q[:n], g.entry_point, p, threads=threads)
-    per_q = (time.time() - t) / n
-    n = int(min(len(q), max(n, budget_s / max(per_q, 1e-6))))
-    t = time.time()
-    ids, _, _, _, _ = oracle.search(og, q[:n], g.entry_point, p, threads=threads)
-    dt = time.time() - t
-    return {"value": n / dt, "unit": "queries/s", "cores": threads, "kind": "port",
-            "sample": "%d queries, oracle (C restatement of the FPGA traversal) at the GPU's parameters" % n,
-            "recall@10": recall_at_k(ids, gt[:n], K)}
-
-
-def run_reference(args):
-    ws, rank, local = dist_env()
-    if rank != 0:
-        return 0
+def run_cfg0(args, dev, local, out, threads):
+    """100k x 128 sift-like, HNSW-style M=16 (degree 32), 1000
+    queries, k=10, ef=64, mc=1; hnswlib on the same graph beside it."""
     import torch
-    torch.cuda.set_device(local)
-    threads = os.cpu_count() or 1
-    x, q, g, gt = make_workload(0, "cuda:%d" % local)
-    sys.path.insert(0, os.path.join(REPO, "oracle"))
-    import oracle
-    from falcon_b200.groundtruth import recall_at_k
-    if not oracle.Hnsw.available():
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libhnswlib_ref.so not built"}))
-        return 0
-    h = oracle.Hnsw.from_graph(x, g.adjacency(), g.entry_point)
-    # pick the smallest ef reaching the recall target on a sample
-    n = 2000
-    ef_sel, rec_sel = 256, 0.0
-    for ef in (64, 128, 256, 512, 1024, 2048):
-        lab, _ = h.search(q[:n], K, ef, threads)
-        rec = recall_at_k(lab, gt[:n], K)
-        log("reference ef=%d recall=%.4f" % (ef, rec))
-        ef_sel, rec_sel = ef, rec
-        if rec >= RECALL_TARGET:
-            break
-    times = []
-    for i in range(args.warmup + args.steps):
-        t = time.time()
-        h.search(q[:n], K, ef_sel, threads)
-        if i >= args.warmup:
-            times.append(time.time() - t)
-    dt = sum(times)
-    qps = n * len(times) / dt
-    out = {"metric": "QPS at recall@10>=0.95 (batched search)", "value": qps, "unit": "queries/s",
-           "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / len(times) * 1e3,
-           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-           "data": "synthetic (seeded)", "impl": "reference",
-           "config": {"workload": WORKLOAD, "k": K, "ef": ef_sel, "recall@10": rec_sel,
-                      "step": "%d-query sample of the 10k batch" % n},
-           "cpu_baseline": {"kind": "reference", "cores": threads, "value": qps, "unit": "queries/s",
-                            "sample": "%d queries per step, hnswlib searchKnn (reference's vendored copy)" % n},
-           "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    h.free()
-    print(json.dumps(out))
-    return 0
-
-
-def profile_serve(args, ix, q, dq, ef, mc, mg, cq, bits):
-    """--profile-region --profile-search serve: each profiled step is one
-    batched FP32 search of the query set, then the same queries as single
-    requests through the serving kernel (all submitted at once, each waited
-    for), so one capture holds inter_kernel and serve_kernel on the same work."""
-    import torch
-    from falcon_b200 import make_params
-    from falcon_b200.serving import FalconServer
-    sv = FalconServer(ring_capacity=max(2 * len(q), 1024), max_k=K, ef_max=ef, cand_queue_max=cq,
-                      bloom_bits_max=bits, mc_max=max(mc, 1), mg_max=max(mg, 1), dim_max=DIM, idle_exit_us=500)
-    iid = sv.add_index(ix)
-    p = make_params(k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
-    index_ids = np.full(len(q), iid, dtype=np.int32)
-
-    def served():
-        rids = sv.submit(index_ids, q, p)
-        for r in rids:
-            sv.wait(int(r), K, timeout_us=120_000_000)
-        return len(rids)
-
-    served()                                  # first launch outside the region
-    torch.cuda.synchronize()
-    l0 = sv.info().kernel_launches
-    tb = ts = 0.0
-    torch.cuda.profiler.start()
-    for _ in range(args.steps):
-        t = time.perf_counter()
-        ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
-        torch.cuda.synchronize()
-        tb += time.perf_counter() - t
-        t = time.perf_counter()
-        n = served()
-        ts += time.perf_counter() - t
-    torch.cuda.profiler.stop()
-    print(json.dumps({"profiled_steps": args.steps, "search": "serve", "ef": ef, "mc": mc, "mg": mg, "cq": cq,
-                      "bloom_bits": bits, "n_base": N_BASE, "requests_per_step": n,
-                      "batched_ms_per_step": tb * 1e3 / args.steps, "served_ms_per_step": ts * 1e3 / args.steps,
-                      "serve_warps": int(sv.info().warps),
-                      "serve_launches_per_step": (sv.info().kernel_launches - l0) / args.steps}))
-    sv.close()
+    from falcon_b200 import FalconIndex
+    from falcon_b200.graph import build_graph, build_upper_layers
+    from falcon_b200.groundtruth import brute_force_f64, recall_at_k
+    from falcon_b200.synthetic import sift_like
+    x = sift_like(100_000, 128, seed=0)
+    q = sift_like(1000, 128, seed=1)
+    t = time.time()
+    g = build_graph(x, 32, device=dev)
+    upper = build_upper_layers(x, 16, seed=0, device=dev)
+    build_s = time.time() - t
+    gt, _ = brute_force_f64(x, q, 10)
+    ix = FalconIndex(g, device=local)
+    ix.set_upper_layers(upper)
+    dq = torch.from_numpy(q).to(dev)
+    P = dict(k=10, ef=64, mc=1, mg=1, cand_queue_size=32, bloom_bits=16)
+    ms, r = timed(lambda: ix.search(dq, **P), 5)
+    p50, p99 = batch1_latency(ix, dq, min(args.latency_samples, 1000), **P)
+    res = {"workload": "sift100k_hnsw_m16: 100k x 128 clipped-integer base, HNSW-style M=16 (degree-32 base layer, "
+                       "upper layers), 1000 queries, k=10, ef=64, mc=1, cand queue 32, 2^16-bit filter",
+           "value": len(q) / ms * 1e3, "unit": "queries/s", "recall@10": recall_at_k(r.ids.cpu().numpy(), gt, 10),
+           "hops_mean": float(r.hops.float().mean()), "visited_mean": float(r.visited.float().mean()),
+           "latency_batch1": {"p50_ms": p50, "p99_ms": p99}, "build_s": build_s,
+           "l2": "the 51 MB base fits in L2: no HBM-roofline claim on this workload"}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle
+        if oracle.Hnsw.available():
+            h = oracle.Hnsw.from_graph(x, g.adjacency(), g.entry_point)
+            h.set_upper(upper)
+            h.search(q, 10, 64, threads)
+            t = time.time()
+            lab, _ = h.search(q, 10, 64, threads)
+            dt = time.time() - t
+            res["cpu_baseline"] = {"value": len(q) / dt, "unit": "queries/s", "cores": threads, "kind": "reference",
+                                   "isa": oracle.Hnsw.isa(), "recall@10": recall_at_k(lab, gt, 10),
+                                   "sample": "the 1000 queries, hnswlib searchKnn setEf(64) on the same graph with "
+                                             "the same upper layers"}
+            h.free()
     ix.close()
-    return 0
+    log("cfg0: %s" % rounded({k2: v for k2, v in res.items() if not isinstance(v, dict)}))
+    out["cfg0"] = res
+
+
+def run_cfg3(args, dev, local, out, keep=False):
+    """1M x 384 unit-normal, HNSW-style M=32, BF16 and FP8-E4M3
+    (+ per-vector scale) traversal with FP32 accumulation and an exact FP32
+    rerank of the final ef; ef {64,128}, mc=2, 10k queries."""
+    import torch
+    from falcon_b200 import FalconIndex
+    from falcon_b200.graph import build_graph, build_upper_layers
+    from falcon_b200.groundtruth import recall_at_k, shortlist_f64
+    from falcon_b200.synthetic import unit_normal_blocks
+    n, dim, nq = args.cfg3_n, 384, 10_000
+    t = time.time()
+    x = unit_normal_blocks(n, dim, seed=3)
+    q = unit_normal_blocks(nq, dim, seed=4)
+    g = build_graph(x, 64, device=dev)
+    upper = build_upper_layers(x, 32, seed=0, device=dev)
+    gt, _ = shortlist_f64(x, q, 10, device=dev)
+    ix = FalconIndex(g, storage=("f32", "bf16", "fp8"), device=local)
+    ix.set_upper_layers(upper)
+    build_s = time.time() - t
+    dq = torch.from_numpy(q).to(dev)
+    pts = []
+    for ef in (64, 128):
+        P = dict(k=10, ef=ef, mc=2, mg=1, cand_queue_size=32, bloom_bits=16)
+        ms32, r32 = timed(lambda: ix.search(dq, **P))
+        ids32 = r32.ids.cpu().numpy()
+        row = {"ef": ef, "mc": 2, "f32": {"value": nq / ms32 * 1e3, "recall@10": recall_at_k(ids32, gt, 10),
+                                          "distance_error_vs_f64": distance_error_f64(x, q, ids32, r32.dists.cpu().numpy())}}
+        for prec in ("bf16", "fp8"):
+            ms, rr = timed(lambda: ix.search(dq, precision=prec, rerank=True, **P))
+            raw = ix.search(dq, precision=prec, **P)
+            ids = rr.ids.cpu().numpy()
+            hops, vis = rr.hops.cpu().numpy(), rr.visited.cpu().numpy()
+            alg = algorithmic_bytes(hops, vis, dim, 64, np.full(nq, 10), np.full(nq, ef),
+                                    elem_bytes=2 if prec == "bf16" else 1, scale_bytes=4 if prec == "fp8" else 0,
+                                    rerank=True)
+            row[prec + "_rerank"] = {
+                "value": nq / ms * 1e3, "recall@10": recall_at_k(ids, gt, 10),
+                "recall_vs_f32_path": float(np.mean([len(np.intersect1d(a, b)) / 10.0 for a, b in zip(ids, ids32)])),
+                "distance_error_vs_f64": distance_error_f64(x, q, ids, rr.dists.cpu().numpy()),
+                "traversal_distance_error_vs_f64": distance_error_f64(x, q, raw.ids.cpu().numpy(),
+                                                                      raw.dists.cpu().numpy()),
+                "roofline_achieved_gbs": alg / (ms / 1e3) / 1e9}
+        pts.append(row)
+        log("cfg3 %s" % json.dumps(row)[:600])
+    out["cfg3"] = {"workload": "sbert1m_hnsw_m32: 1M x 384 unit-normal (seeded SBERT1M stand-in), HNSW-style M=32, "
+                               "10k queries, k=10, mc=2, cand queue 32, 2^16-bit filter; BF16 / FP8-E4M3 + per-vector "
+                               "FP32 scale traversal, FP32 accumulation, exact FP32 rerank of the final ef",
+                   "n_base": n, "build_s": build_s, "points": pts}
+    if keep:
+        return dict(ix=ix, q=q, x=x)
+    ix.close()
+    return None
+
+
+def run_cfg4(args, H2, H3, out):
+    """the configs[2] (FP32, D=128, NSG) and configs[3] (BF16 +
+    FP32 rerank, D=384, HNSW) indexes resident together; Poisson arrivals,
+    each request a random index with k from {1,10,100}, ef from {32..256},
+    mc from {1,2,4}."""
+    from falcon_b200 import make_params
+    from falcon_b200.serving import FalconServer, poisson_arrivals
+    sv = FalconServer(ring_capacity=65536, max_k=100, ef_max=256, cand_queue_max=32, bloom_bits_max=16, mc_max=4,
+                      mg_max=1, dim_max=384, idle_exit_us=5000)
+    i2 = sv.add_index(H2["ix"])
+    i3 = sv.add_index(H3["ix"])
+    rng = np.random.default_rng(11)
+    n = 40_000
+    which = rng.integers(0, 2, n)
+    ks = rng.choice([1, 10, 100], n)
+    efs = np.maximum(rng.choice([32, 64, 128, 256], n), ks)
+    mcs = rng.choice([1, 2, 4], n)
+    q2, q3 = H2["q"], H3["q"]
+    qmax = np.zeros((n, 384), dtype=np.float32)
+    idx = rng.integers(0, 10_000, n)
+    params, iids = [], np.where(which == 0, i2, i3).astype(np.int32)
+    for i in range(n):
+        if which[i] == 0:
+            qmax[i, :128] = q2[idx[i]]
+            params.append(make_params(k=int(ks[i]), ef=int(efs[i]), mc=int(mcs[i])))
+        else:
+            qmax[i] = q3[idx[i]]
+            params.append(make_params(k=int(ks[i]), ef=int(efs[i]), mc=int(mcs[i]), precision="bf16", rerank=True))
+    pts = []
+    sv.replay(iids[:2000], qmax[:2000], params[:2000], poisson_arrivals(2000, 20000, 5), 100)
+    for rate in (10_000, 50_000, 100_000, 200_000, 500_000):
+        m = min(n, max(4000, int(rate * 0.25)))
+        arr = poisson_arrivals(m, rate, seed=rate)
+        lat, ids, d, hops, vis, el = sv.replay(iids[:m], qmax[:m], params[:m], arr, 100)
+        pt = {"offered_qps": rate, "requests": m, "sustained_qps": m / (el / 1e6),
+              "p50_ms": float(np.percentile(lat, 50)) / 1e3, "p99_ms": float(np.percentile(lat, 99)) / 1e3,
+              "p50_ms_cfg2": float(np.percentile(lat[which[:m] == 0], 50)) / 1e3,
+              "p50_ms_cfg3": float(np.percentile(lat[which[:m] == 1], 50)) / 1e3}
+        log("cfg4 %s" % rounded(pt))
+        pts.append(pt)
+    inf = sv.info()
+    sv.close()
+    out["cfg4"] = {"workload": "online serving: sift10m_nsg_r64 (FP32) and sbert1m_hnsw_m32 (BF16 + FP32 rerank) "
+                               "resident together, Poisson arrivals, each request a random index, k {1,10,100}, "
+                               "ef {32,64,128,256} (raised to k), mc {1,2,4}",
+                   "points": pts, "kernel_launches": int(inf.kernel_launches)}
 
 
 def run_ours(args):
@@ -397,208 +714,95 @@ def run_ours(args):
     if ws > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    from falcon_b200 import FalconIndex
-    from falcon_b200.groundtruth import recall_at_k
-    x, q, g, gt, upper = make_workload(rank, dev, upper_layers=True)
-    ix = FalconIndex(g, storage=("f32", "bf16", "fp8"), device=local)
-    ix.set_upper_layers(upper)   # every search descends the upper layers, then searches the base layer
-    if args.fixed:
-        ef_, mc_, mg_, cq_, bits_ = [int(v) for v in args.fixed.split(",")]
-        best, reached, table = dict(ef=ef_, mc=mc_, mg=mg_, cq=cq_, bits=bits_), None, []
-    else:
-        best, reached, table = sweep(ix, q, gt)
-    ef, mc, mg, cq, bits = best["ef"], best["mc"], best["mg"], best["cq"], best["bits"]
-    dq = torch.from_numpy(q).to(dev)
-    for _ in range(args.warmup):
-        r = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
-    torch.cuda.synchronize()
-    if ws > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    extra = {}
-    if args.profile_region and args.profile_search == "serve":
-        return profile_serve(args, ix, q, dq, ef, mc, mg, cq, bits)
-    if args.profile_region and args.profile_search == "intra":
-        extra = dict(mode="intra", channels=4)
-    elif args.profile_region and args.profile_search == "bf16_rerank":
-        extra = dict(precision="bf16", rerank=True)
-    if extra:
-        ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, **extra)
-        torch.cuda.synchronize()
-    if args.profile_region:
-        torch.cuda.profiler.start()
-    with ClockSampler(local) as clk:
-        ev0.record()
-        for _ in range(args.steps):
-            r = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, **extra)
-        ev1.record()
-        torch.cuda.synchronize()
-    if args.profile_region:
-        torch.cuda.profiler.stop()
-        hops_p, vis_p = r.hops.cpu().numpy(), r.visited.cpu().numpy()
-        print(json.dumps({"profiled_steps": args.steps, "search": args.profile_search, "ef": ef, "mc": mc, "mg": mg,
-                          "cq": cq,
-                          "ms_per_step": ev0.elapsed_time(ev1) / args.steps, "n_base": N_BASE,
-                          "queries_per_step": N_QUERIES, "hops_mean": float(hops_p.mean()),
-                          "visited_mean": float(vis_p.mean()),
-                          "bytes_per_query": algorithmic_bytes(hops_p, vis_p, ef,
-                                                               elem_bytes=2 if "precision" in extra else 4,
-                                                               rerank="precision" in extra) / N_QUERIES}))
-        ix.close()
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    threads = os.cpu_count() or 1
+    cfgs = [int(c) for c in args.configs.split(",") if c.strip()]
+    out = {}
+    t0 = time.time()
+    H2 = headline_cfg2(args, dev, local, rank, ws, out)
+    if H2 is None:
         return 0
-    ms = ev0.elapsed_time(ev1)
-    if ws > 1:
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-        torch.distributed.barrier()
-    ms_step = ms / args.steps
-    qps = ws * N_QUERIES * args.steps / (ms / 1e3)
-    ids = r.ids.cpu().numpy()
-    hops = r.hops.cpu().numpy()
-    vis = r.visited.cpu().numpy()
-    recall = recall_at_k(ids, gt, K)
-
-    # end to end through the public API with host buffers (pinned), copies inside
-    qh = torch.from_numpy(q).pin_memory()
-    qh_np = qh.numpy()
-    e2e_times = []
-    for i in range(args.warmup + args.steps):
-        torch.cuda.synchronize()
-        t = time.perf_counter()
-        rh = ix.search(qh_np, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
-        if i >= args.warmup:
-            e2e_times.append(time.perf_counter() - t)
-    e2e_ms = sum(e2e_times) / len(e2e_times) * 1e3
-    if ws > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_qps = ws * N_QUERIES / (e2e_ms / 1e3)
-
-    # latency at batch 1 (device-resident query, one search call per query)
-    lat = []
-    for i in range(min(1000, N_QUERIES)):
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record()
-        ix.search(dq[i:i + 1], k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
-        b.record()
-        b.synchronize()
-        lat.append(a.elapsed_time(b))
-    lat = np.array(lat[10:])
-    # the same batch-1 latency in intra-query mode (one block of channel warps per query)
-    # In intra-query mode each channel's filter sees 1/channels of the ids, so
-    # bits - log2(channels) + 1 per channel keeps the false-rejection rate of the
-    # whole-query filter; up to 2^18 bits it lives in shared memory.
-    from falcon_b200.autotune import channel_bloom_bits
-    lat_intra = {}
-    for ch in (4, 8):
-        cbits = channel_bloom_bits(bits, ch)
-        pi = dict(k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=cbits, mode="intra", channels=ch)
-        ri = ix.search(dq, **pi)
-        li = []
-        for i in range(min(300, N_QUERIES)):
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record()
-            ix.search(dq[i:i + 1], **pi)
-            b.record()
-            b.synchronize()
-            li.append(a.elapsed_time(b))
-        li = np.array(li[10:])
-        lat_intra[ch] = (float(np.percentile(li, 50)), float(np.percentile(li, 99)), cbits,
-                         recall_at_k(ri.ids.cpu().numpy(), gt, K))
-
-    # BF16 + exact FP32 rerank at the same point
-    rb = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, precision="bf16", rerank=True)
-    torch.cuda.synchronize()
-    a = torch.cuda.Event(enable_timing=True)
-    b = torch.cuda.Event(enable_timing=True)
-    a.record()
-    for _ in range(3):
-        rb = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, precision="bf16", rerank=True)
-    b.record()
-    torch.cuda.synchronize()
-    bf_ms = a.elapsed_time(b) / 3
-    bf_recall = recall_at_k(rb.ids.cpu().numpy(), gt, K)
-    # FP8 E4M3 (+ per-vector scale) traversal + exact FP32 rerank at the same point
-    rf = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, precision="fp8", rerank=True)
-    torch.cuda.synchronize()
-    a.record()
-    for _ in range(3):
-        rf = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, precision="fp8", rerank=True)
-    b.record()
-    torch.cuda.synchronize()
-    f8_ms = a.elapsed_time(b) / 3
-    f8_recall = recall_at_k(rf.ids.cpu().numpy(), gt, K)
-    # distance error against FP64: after the exact FP32 rerank, and of the
-    # reduced-precision traversal distances themselves (no rerank)
-    derr = {"f32": distance_error_f64(x, q, r.ids.cpu().numpy(), r.dists.cpu().numpy())}
-    for prec, res in (("bf16", rb), ("fp8", rf)):
-        raw = ix.search(dq, k=K, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits, precision=prec)
-        derr[prec + "_rerank"] = distance_error_f64(x, q, res.ids.cpu().numpy(), res.dists.cpu().numpy())
-        derr[prec + "_traversal"] = distance_error_f64(x, q, raw.ids.cpu().numpy(), raw.dists.cpu().numpy())
-        derr[prec + "_traversal"]["recall@10"] = recall_at_k(raw.ids.cpu().numpy(), gt, K)
-    mixed = mixed_params(ix, q)
-    served = None if args.no_serve else serve_measurements(ix, q, gt, ef, mc, mg, cq, bits,
-                                                           N_QUERIES / (bf_ms / 1e3))
-
-    peak, peak_kind = measured_peak()
-    alg = algorithmic_bytes(hops, vis, ef)
-    achieved = alg / (ms_step / 1e3) / 1e9
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None, "peak_kind": peak_kind,
-            "bytes_per_query": alg / N_QUERIES, "kernel": "inter_kernel<f32>"}
-    # DRAM traffic per launch: the ratio of measured to algorithmic bytes from an
-    # ncu capture of a smaller case of the same operating point (profiles/),
-    # applied to this launch's algorithmic bytes
-    tp = os.path.join(REPO, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        tr = json.load(open(tp))
-        key = "ef%d_mc%d_mg%d_cq%d_bits%d" % (ef, mc, mg, cq, bits)
-        if key in tr:
-            roof["traffic"] = tr[key]["ratio"] * alg
-            roof["traffic_note"] = tr[key]["note"]
-    cpu = cpu_fpga_port = None
-    if rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(x, q, g, gt, ef, os.cpu_count() or 1)
-        cpu_fpga_port = cpu_port(q, g, gt, ef, mc, mg, cq, bits, os.cpu_count() or 1)
-    out = {
-        "metric": "QPS at recall@10>=0.95 (batched search)", "value": qps, "unit": "queries/s",
-        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded unit-normal stand-in for Deep1M)",
-        "config": {"workload": WORKLOAD, "k": K, "ef": ef, "mc": mc, "mg": mg, "cand_queue_size": cq, "bloom_bits": bits, "mode": "inter",
-                   "recall@10": recall, "recall_target_reached": reached, "queries_per_step": N_QUERIES,
-                   "parallelism": "replicas" if ws > 1 else "single",
-                   "l2": "inputs larger than L2 (384 MB vectors + 320 MB links vs 126 MB L2)",
-                   "sweep": [{k2: (round(v, 4) if isinstance(v, float) else v) for k2, v in s.items()} for s in table]},
-        "latency_ms": {"batch": 1, "p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                       "samples": int(len(lat)), "timer": "CUDA events around one search call", "mode": "inter",
-                       "intra": {("channels_%d" % c): {"p50": v[0], "p99": v[1], "bloom_bits_per_channel": v[2],
-                                                       "recall@10": v[3]} for c, v in lat_intra.items()}},
-        "e2e": {"value": e2e_qps, "unit": "queries/s", "ms_per_step": e2e_ms,
-                "h2d_bytes_per_step": int(q.nbytes), "d2h_bytes_per_step": int(N_QUERIES * K * 8 + N_QUERIES * 8)},
-        "bf16_rerank": {"value": N_QUERIES / (bf_ms / 1e3), "unit": "queries/s", "recall@10": bf_recall},
-        "fp8_rerank": {"value": N_QUERIES / (f8_ms / 1e3), "unit": "queries/s", "recall@10": f8_recall},
-        "distance_error_vs_f64": derr,
-        "mixed_per_query_params": mixed,
-        "served": served,
-        "gpu_launches": 2 * args.steps,   # per step: the upper-layer descent and the base-layer search
-        "clocks": clk.summary(),
-        "roofline": roof,
-        "cpu_baseline": cpu,
-        "cpu_fpga_semantics_port": cpu_fpga_port,
-    }
+    if ws == 1:
+        recall_curve_cfg2(H2, out)
+        if not args.no_cpu_baseline:
+            res = cpu_baselines_cfg2(H2, out, threads)
+            out["cpu_baseline"] = res.get("cpu_baseline")
+            out["cpu_fpga_semantics_port"] = res.get("cpu_fpga_semantics_port")
+            out["config"]["parity_sample"] = res.get("parity_sample")
+        log("cfg2 done at %.0fs" % (time.time() - t0))
+        H3 = None
+        if 3 in cfgs or 4 in cfgs:
+            H3 = run_cfg3(args, dev, local, out, keep=4 in cfgs)
+            log("cfg3 done at %.0fs" % (time.time() - t0))
+        if 4 in cfgs and H3 is not None and not args.no_serve:
+            run_cfg4(args, H2, H3, out)
+            log("cfg4 done at %.0fs" % (time.time() - t0))
+        if H3 is not None:
+            H3["ix"].close()
+        H2["ix"].close()
+        del H2, H3
+        torch.cuda.empty_cache()
+        if 1 in cfgs:
+            run_cfg1(args, dev, local, out)
+            log("cfg1 done at %.0fs" % (time.time() - t0))
+        if 0 in cfgs:
+            run_cfg0(args, dev, local, out, threads)
+            log("cfg0 done at %.0fs" % (time.time() - t0))
+    else:
+        H2["ix"].close()
     if rank == 0:
         print(json.dumps(out))
-    ix.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# Reference arm: hnswlib (the reference's vendored copy) on the same graph
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    import torch
+    torch.cuda.set_device(local)
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    if not oracle.Hnsw.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libhnswlib_ref.so not built"}))
+        return 0
+    x, q, g, gt, _ = cfg2_workload("cuda:%d" % local)
+    efs, ks, _ = cfg2_params(len(q))
+    h = oracle.Hnsw.from_graph(g.vectors, g.adjacency(), g.entry_point)
+    n = args.ref_queries
+    times = []
+    for i in range(args.warmup + args.steps):
+        s = (i * n) % len(q)
+        t = time.time()
+        lab, _ = h.search_mixed(q[s:s + n], ks[s:s + n], efs[s:s + n], threads)
+        if i >= args.warmup:
+            times.append(time.time() - t)
+    lab, _ = h.search_mixed(q[:min(n, len(gt))], ks[:min(n, len(gt))], efs[:min(n, len(gt))], threads)
+    rec = mixed_recall(lab, gt[:len(lab)], ks[:len(lab)])
+    h.free()
+    dt = sum(times)
+    qps = n * len(times) / dt
+    outj = {"metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt / len(times) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded clipped-integer stand-in for SIFT10M)", "impl": "reference",
+            "config": {"workload": WORKLOAD2, "queries_per_step": n, "recall": rec,
+                       "step": "%d-query slice of the 100k mixed-parameter batch (the slice moves each step); "
+                               "hnswlib searchKnn with each query's ef and k from the same medoid on the same "
+                               "graph; mc has no hnswlib counterpart" % n,
+                       "graph": "built by the same GPU builder as the GPU arm (data preparation, outside the timed "
+                                "region)"},
+            "cpu_baseline": {"kind": "reference", "cores": threads, "value": qps, "unit": "queries/s",
+                             "isa": oracle.Hnsw.isa(), "cpu": oracle.Hnsw.cpu_model(),
+                             "sample": "%d queries per step, hnswlib (the reference's vendored copy)" % n},
+            "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(outj))
     return 0
 
 
@@ -608,25 +812,25 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--configs", default="0,1,3,4", help="extra workloads after the configs[2] headline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the continuous-batching measurements")
-    ap.add_argument("--n-base", type=int, default=None, help="scaled-down runs for quick checks only")
+    ap.add_argument("--n-base", type=int, default=None, help="configs[2] base size (scaled-down runs: checks only)")
     ap.add_argument("--n-queries", type=int, default=None)
-    ap.add_argument("--fixed", default=None, help="ef,mc,mg,cq,bloom_bits: skip the sweep")
+    ap.add_argument("--cfg1-n", type=int, default=1_000_000)
+    ap.add_argument("--cfg3-n", type=int, default=1_000_000)
+    ap.add_argument("--latency-samples", type=int, default=200)
+    ap.add_argument("--ref-queries", type=int, default=4000, help="reference arm: queries per step")
     ap.add_argument("--profile-region", action="store_true",
-                    help="bracket only the timed steps with cudaProfilerStart/Stop and exit after them")
-    ap.add_argument("--profile-search", default="inter", choices=["inter", "intra", "bf16_rerank", "serve"],
-                    help="with --profile-region: the search the timed steps run (inter-query FP32, intra-query "
-                         "4 channels FP32, BF16 traversal + FP32 rerank, or FP32 batched then the same queries "
-                         "through the serving kernel)")
+                    help="bracket only the timed headline steps with cudaProfilerStart/Stop and exit after them")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    global N_BASE, N_QUERIES
     if args.n_base:
-        N_BASE = args.n_base
+        CFG2["n"] = args.n_base
     if args.n_queries:
-        N_QUERIES = args.n_queries
+        CFG2["nq"] = args.n_queries
+        CFG2["ngt"] = min(CFG2["ngt"], args.n_queries)
     from falcon_b200 import build as fb
     fb.build()
     if args.impl == "reference":

@@ -373,11 +373,39 @@ int falcon_index_load_fpga(const char *index_dir, const char *graph_type, int32_
     if (n < 1 || md < 1 || md > kMaxDegree) return set_error(FALCON_ERR_IO, "meta.bin: n=%d max_degree=%d", n, md);
     const int64_t lstride = 16LL * (1 + (md + 15) / 16);
     const int64_t vstride = pad16(dim) + 16;
-    if (!read_file(dir + "/ground_links_1_chan_0.bin", links) || (int64_t)links.size() != (int64_t)n * lstride * 4)
-        return set_error(FALCON_ERR_IO, "ground_links_1_chan_0.bin missing or not %lld bytes", (long long)n * lstride * 4);
-    if (!read_file(dir + "/ground_vectors_1_chan_0.bin", vecs) || (int64_t)vecs.size() != (int64_t)n * vstride * 4)
-        return set_error(FALCON_ERR_IO, "ground_vectors_1_chan_0.bin missing or not %lld bytes for dim %d",
-                         (long long)n * vstride * 4, dim);
+    // The reference writes the rows round robin over nc channel files, node i
+    // as row i / nc of channel i % nc (hnsw.py:324-335, nsg_to_FPGA.py:124-135);
+    // its hosts read the set their kernel was built for (intra v1.5
+    // host.cpp:242-260).  The single-channel set is used when present, else
+    // the first complete set of 2, 4, 8 or 16 channels, de-interleaved.
+    int nc = 0;
+    for (int c : {1, 2, 4, 8, 16}) {
+        FILE *f = fopen((dir + "/ground_links_" + std::to_string(c) + "_chan_0.bin").c_str(), "rb");
+        if (f) {
+            fclose(f);
+            nc = c;
+            break;
+        }
+    }
+    if (nc == 0) return set_error(FALCON_ERR_IO, "no ground_links_{1,2,4,8,16}_chan_0.bin in %s", index_dir);
+    links.resize((size_t)n * lstride * 4);
+    vecs.resize((size_t)n * vstride * 4);
+    for (int c = 0; c < nc; c++) {
+        const int64_t rows = (n - c + nc - 1) / nc;   // nodes c, c + nc, ...
+        const std::string suffix = std::to_string(nc) + "_chan_" + std::to_string(c) + ".bin";
+        std::vector<char> lc, vc;
+        if (!read_file(dir + "/ground_links_" + suffix, lc) || (int64_t)lc.size() != rows * lstride * 4)
+            return set_error(FALCON_ERR_IO, "ground_links_%s missing or not %lld bytes", suffix.c_str(),
+                             (long long)(rows * lstride * 4));
+        if (!read_file(dir + "/ground_vectors_" + suffix, vc) || (int64_t)vc.size() != rows * vstride * 4)
+            return set_error(FALCON_ERR_IO, "ground_vectors_%s missing or not %lld bytes for dim %d", suffix.c_str(),
+                             (long long)(rows * vstride * 4), dim);
+        for (int64_t r = 0; r < rows; r++) {
+            const int64_t node = r * nc + c;
+            memcpy(links.data() + node * lstride * 4, lc.data() + r * lstride * 4, (size_t)lstride * 4);
+            memcpy(vecs.data() + node * vstride * 4, vc.data() + r * vstride * 4, (size_t)vstride * 4);
+        }
+    }
     const bool have_labels = read_file(dir + "/ground_labels.bin", labels) && (int64_t)labels.size() == (int64_t)n * 4;
     falcon_index_desc d;
     memset(&d, 0, sizeof(d));
@@ -569,8 +597,6 @@ static int search_impl(falcon_index *ix, const float *queries, int64_t nq, int64
                          (long long)query_stride, ix->dim);
     if (memory != FALCON_MEM_HOST && memory != FALCON_MEM_DEVICE) return set_error(FALCON_ERR_ARG, "bad memory flag");
     if (nq == 0) return FALCON_OK;
-    if (per_query_params && memory == FALCON_MEM_DEVICE)
-        return set_error(FALCON_ERR_ARG, "per-query params must be host memory");
     const int64_t np = per_query_params ? nq : 1;
     int ef_max = 0, k_max = 0, mc_max = 1, mg_max = 1, bits_max = kMinBloomBits, prec = -1, mode = -1, ch_max = 1;
     int cq_max = 1;

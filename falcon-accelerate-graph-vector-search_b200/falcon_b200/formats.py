@@ -70,10 +70,11 @@ class Graph:
 # Reference FPGA index files (hnsw.py:264-377 / nsg_to_FPGA.py:56-137)
 # ---------------------------------------------------------------------------
 
-def write_fpga_index(out_dir, graph, graph_type="HNSW", max_level=0, max_m=None, upper=None):
-    """Write meta.bin, ground_links_1_chan_0.bin, ground_vectors_1_chan_0.bin
-    and ground_labels.bin in the reference layout (single channel), and with
-    `upper` (HNSW) also upper_links.bin and upper_links_pointers.bin."""
+def write_fpga_index(out_dir, graph, graph_type="HNSW", max_level=0, max_m=None, upper=None, num_channels=(1,)):
+    """Write meta.bin, ground_links_{nc}_chan_{i}.bin, ground_vectors_{nc}_chan_{i}.bin
+    for every nc in num_channels (rows round robin: node j to channel j % nc)
+    and ground_labels.bin in the reference layout, and with `upper` (HNSW)
+    also upper_links.bin and upper_links_pointers.bin."""
     os.makedirs(out_dir, exist_ok=True)
     n, md, dim = graph.n, graph.max_degree, graph.dim
     if upper is not None:
@@ -90,26 +91,48 @@ def write_fpga_index(out_dir, graph, graph_type="HNSW", max_level=0, max_m=None,
     links[:, 0] = graph.links[:, 0]
     links[:, 16:16 + md] = graph.links[:, graph.ids_offset:graph.ids_offset + md]
     links[:, 16:16 + md][np.arange(md)[None, :] >= links[:, :1]] = 0
-    links.tofile(os.path.join(out_dir, "ground_links_1_chan_0.bin"))
+    for nc in num_channels:
+        for c in range(nc):
+            links[c::nc].tofile(os.path.join(out_dir, "ground_links_%d_chan_%d.bin" % (nc, c)))
     vec = np.zeros((n, pad16(dim) + 16), dtype=np.float32)
     vec[:, :dim] = graph.vectors
     vec[:, pad16(dim)] = np.frombuffer(np.int32(-1).tobytes(), dtype=np.float32)[0]   # visited tag -1
-    vec.tofile(os.path.join(out_dir, "ground_vectors_1_chan_0.bin"))
+    for nc in num_channels:
+        for c in range(nc):
+            vec[c::nc].tofile(os.path.join(out_dir, "ground_vectors_%d_chan_%d.bin" % (nc, c)))
     labels = graph.labels if graph.labels is not None else np.arange(n, dtype=np.int32)
     labels.astype(np.int32).tofile(os.path.join(out_dir, "ground_labels.bin"))
     if upper is not None:
         write_fpga_upper(out_dir, upper)
 
 
-def read_fpga_index(index_dir, graph_type, dim):
-    """Read the reference's single-channel FPGA files into a Graph."""
+def fpga_channel_sets(index_dir):
+    """Channel counts nc with a ground_links_{nc}_chan_0.bin in the directory."""
+    return [nc for nc in (1, 2, 4, 8, 16)
+            if os.path.exists(os.path.join(index_dir, "ground_links_%d_chan_0.bin" % nc))]
+
+
+def read_fpga_index(index_dir, graph_type, dim, channels=None):
+    """Read the reference's FPGA files into a Graph.  The writers spread the
+    rows round robin over nc channel files, node i as row i // nc of channel
+    i % nc (hnsw.py:324-335, nsg_to_FPGA.py:124-135); the rows are put back in
+    node order.  channels: the set to read (default: 1 if present, else the
+    smallest available)."""
     meta = np.fromfile(os.path.join(index_dir, "meta.bin"), dtype=np.int32)
     if graph_type == "HNSW":
         n, entry, md = int(meta[0]), int(meta[2]), int(meta[4])
     else:
         n, entry, md = int(meta[0]), int(meta[1]), int(meta[2])
-    links = np.fromfile(os.path.join(index_dir, "ground_links_1_chan_0.bin"), dtype=np.int32).reshape(n, link_stride(md))
-    vec = np.fromfile(os.path.join(index_dir, "ground_vectors_1_chan_0.bin"), dtype=np.float32).reshape(n, pad16(dim) + 16)
+    sets = fpga_channel_sets(index_dir)
+    nc = channels or (sets[0] if sets else 1)
+    links = np.empty((n, link_stride(md)), dtype=np.int32)
+    vec = np.empty((n, pad16(dim) + 16), dtype=np.float32)
+    for c in range(nc):
+        rows = (n - c + nc - 1) // nc
+        links[c::nc] = np.fromfile(os.path.join(index_dir, "ground_links_%d_chan_%d.bin" % (nc, c)),
+                                   dtype=np.int32).reshape(rows, link_stride(md))
+        vec[c::nc] = np.fromfile(os.path.join(index_dir, "ground_vectors_%d_chan_%d.bin" % (nc, c)),
+                                 dtype=np.float32).reshape(rows, pad16(dim) + 16)
     lp = os.path.join(index_dir, "ground_labels.bin")
     labels = np.fromfile(lp, dtype=np.int32) if (graph_type == "HNSW" and os.path.exists(lp)) else None
     return Graph(vec[:, :dim], links, md, entry, labels)

@@ -75,14 +75,32 @@ def _heuristic_prune(x, node_ids, cand, cand_d, max_degree):
     return out
 
 
+def _build_graph_cuda(xs, x, ids, max_degree):
+    """Steps 2-3 with the library's neighbour-selection kernel
+    (falcon_graph_prune, the same rule): forward prune of the kNN lists, then
+    forward + reverse candidates pruned again."""
+    from .nsg import prune, reverse_lists
+    adj, _ = prune(x, ids.to(torch.int32), max_degree)
+    rev = reverse_lists(adj, max_degree)
+    adj, _ = prune(x, torch.cat([adj, rev], 1), max_degree)
+    return adj
+
+
 def build_graph(vectors, max_degree, knn_k=None, device=None, batch=2048, verbose=False):
-    """Single-layer graph of max degree `max_degree` with medoid entry point."""
+    """Single-layer graph of max degree `max_degree` with medoid entry point.
+    On a GPU the neighbour selection runs in the library's prune kernel; on
+    the CPU in torch (same rule)."""
     dev = _device(device)
     xs = np.ascontiguousarray(vectors, dtype=np.float32)
     n = xs.shape[0]
     kk = min(knn_k or 2 * max_degree, n - 1)
     ids, dst = knn(xs, kk, device=dev)
     x = torch.from_numpy(xs).to(dev)
+    if dev.type == "cuda" and 4 * kk * (((xs.shape[1] + 3) // 4) + 4) <= 200 * 1024:
+        adj = _build_graph_cuda(xs, x, ids, max_degree)
+        mean = x.mean(0, keepdim=True)
+        entry = int(torch.argmin(((x - mean) ** 2).sum(1)).item())
+        return Graph.from_adjacency(xs, adj.cpu().numpy(), entry)
     fwd = torch.empty((n, max_degree), dtype=torch.int64, device=dev)
     for s in range(0, n, batch):
         e = min(n, s + batch)

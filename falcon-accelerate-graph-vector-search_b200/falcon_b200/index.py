@@ -41,6 +41,21 @@ def make_params(k=10, ef=64, mc=1, mg=1, cand_queue_size=32, bloom_bits=16, hash
     return p
 
 
+def params_array(per_query):
+    """A ctypes array of SearchParams from SearchParams or keyword dicts (one
+    per query); build it once and pass it to search(per_query=...) to keep the
+    conversion out of repeated calls."""
+    arr = (_lib.SearchParams * len(per_query))()
+    for i, p in enumerate(per_query):
+        arr[i] = p if isinstance(p, _lib.SearchParams) else make_params(**p)
+    return arr
+
+
+def max_k(arr):
+    ks = np.frombuffer(arr, dtype=np.int32).reshape(len(arr), ctypes.sizeof(_lib.SearchParams) // 4)[:, 0]
+    return int(ks.max())
+
+
 class SearchResult:
     def __init__(self, ids, dists, hops, visited, status):
         self.ids, self.dists, self.hops, self.visited, self.status = ids, dists, hops, visited, status
@@ -193,16 +208,14 @@ class FalconIndex:
                per_query=None, out_stride=None, stream=None):
         """Search host queries [nq, dim] (numpy) or device queries (torch CUDA tensor).
 
-        per_query: optional list/array of dicts or SearchParams, one per query
-        (mixed k/ef/mc in one launch).  Returns (ids, dists, hops, visited) with
+        per_query: optional list of dicts or SearchParams, one per query, or
+        a params_array (mixed k/ef/mc in one launch; host or device queries).  Returns (ids, dists, hops, visited) with
         ids/dists [nq, out_stride] best-first (out_stride = max k by default).
         """
         lib = _lib.load()
         if per_query is not None:
-            arr = (_lib.SearchParams * len(per_query))()
-            for i, p in enumerate(per_query):
-                arr[i] = p if isinstance(p, _lib.SearchParams) else make_params(**p)
-            params, pq, kmax = arr, 1, max(p.k for p in arr)
+            arr = per_query if isinstance(per_query, ctypes.Array) else params_array(per_query)
+            params, pq, kmax = arr, 1, max_k(arr)
         else:
             params, pq = make_params(k, ef, mc, mg, cand_queue_size, bloom_bits, hash_seed, mode, channels,
                                      precision, rerank, max_hops), 0
@@ -257,8 +270,6 @@ class FalconIndex:
     def _search_device(self, queries, params, pq, ostride, entry_points, stream):
         import torch
         lib = _lib.load()
-        if pq:
-            raise ValueError("per-query params with device queries: pass host queries")
         q = queries.contiguous().float()
         nq = q.shape[0]
         dev = q.device
@@ -270,8 +281,9 @@ class FalconIndex:
         if entry_points is not None:
             ep = entry_points.to(device=dev, dtype=torch.int32).contiguous()
         s = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+        pptr = ctypes.cast(params, ctypes.POINTER(_lib.SearchParams)) if pq else ctypes.byref(params)
         rc = lib.falcon_search(self._h, q.data_ptr(), nq, q.stride(0), ep.data_ptr() if ep is not None else None,
-                               ctypes.byref(params), 0, ids.data_ptr(), dists.data_ptr(), ostride, hops.data_ptr(),
+                               pptr, pq, ids.data_ptr(), dists.data_ptr(), ostride, hops.data_ptr(),
                                vis.data_ptr(), _lib.MEM_DEVICE, ctypes.c_void_p(s))
         _lib.check(rc)
         return SearchResult(ids, dists, hops, vis, rc)
@@ -308,4 +320,4 @@ def vadd(query_vectors_padded, entry_point_ids, db_vectors_ref, links_ref, num_d
     return out_id, out_dist, mem_debug
 
 
-__all__ = ["FalconIndex", "Graph", "make_params", "vadd", "storage_mask"]
+__all__ = ["FalconIndex", "Graph", "make_params", "params_array", "vadd", "storage_mask"]

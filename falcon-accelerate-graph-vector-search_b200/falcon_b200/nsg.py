@@ -15,9 +15,12 @@ equivalent single-layer graph of max degree R on one GPU:
      (falcon_graph_prune: hnswlib's / NSG's rule, alpha = 1);
   3. reverse edges: every kept edge u -> v offers u to v, and each node's
      forward and reverse candidates are pruned again;
-  4. optionally NSG's search step: every node is searched on the graph so far
-     (this library's own traversal kernel) and the ef best results join its
-     candidates for another prune + reverse round;
+  4. NSG's search step, repeated per pass: every node is searched on the
+     graph so far (this library's own traversal kernel, from the medoid) and
+     its ef best results join its candidates for another prune + reverse
+     round; a pass may prune with alpha > 1 (keep a candidate unless
+     alpha * d(kept, c) < d(c, node)), which keeps the longer edges that
+     high-dimensional data needs to stay navigable (DiskANN's second pass);
   5. the medoid (the point nearest the mean) as the entry point, and a
      breadth-first search from it; nodes it does not reach are attached to the
      first reached node of their candidate list, as NSG attaches unreached
@@ -171,38 +174,49 @@ def reachable(adj, entry):
     return seen
 
 
-def attach_unreached(adj, cnt, seen, cand, entry, rounds=8):
-    """Give every node the breadth-first search misses an in-edge from the
-    first reached node of its candidate list (else from the entry), into a
-    free slot or over that node's farthest edge; repeat until all are reached.
-    Returns the number of edges added."""
+def attach_unreached(adj, cnt, seen, cand, entry, rounds=16):
+    """Give every node the breadth-first search misses an in-edge: from the
+    first reached node of its candidate list that has a free slot, else from
+    any reached node with a free slot, else over the farthest edge of its
+    first reached candidate; repeat until all are reached.  adj/cnt are
+    updated in place.  Returns (edges added, reachability)."""
     added = 0
     R = adj.shape[1]
+    dev = adj.device
     for _ in range(rounds):
         un = torch.nonzero(~seen).flatten()
         if un.numel() == 0:
             break
         c = cand[un].to(torch.int64)
-        ok = (c >= 0) & seen[c.clamp_min(0)]
-        first = torch.argmax(ok.to(torch.int8), dim=1)
-        w = torch.where(ok.any(1), c[torch.arange(un.numel(), device=c.device), first],
-                        torch.full_like(un, int(entry)))
-        wn, un_h = w.cpu().numpy(), un.cpu().numpy()
-        cnt_h = cnt.cpu().numpy().copy()
-        rows = {}
-        for u, v in zip(un_h.tolist(), wn.tolist()):
-            if v not in rows:
-                rows[v] = adj[v].cpu().numpy().copy()
-            row = rows[v]
-            if cnt_h[v] < R:
-                row[cnt_h[v]] = u
-                cnt_h[v] += 1
-            else:
-                row[R - 1] = u
-            added += 1
-        for v, row in rows.items():
-            adj[v] = torch.from_numpy(row).to(adj.device)
-        cnt.copy_(torch.from_numpy(cnt_h).to(cnt.device))
+        cc = c.clamp_min(0)
+        reached = (c >= 0) & seen[cc]
+        free = reached & (cnt[cc] < R)
+        rows = torch.arange(un.numel(), device=dev)
+        w = torch.where(free.any(1), cc[rows, torch.argmax(free.to(torch.int8), 1)], torch.full_like(un, -1))
+        pool = torch.nonzero(seen & (cnt < R)).flatten()
+        miss = w < 0
+        if miss.any() and pool.numel():
+            w[miss] = pool[torch.arange(int(miss.sum()), device=dev) % pool.numel()]
+        # the rest replace the farthest edge of their first reached candidate (or the entry's)
+        miss = w < 0
+        if miss.any():
+            fr = torch.where(reached.any(1), cc[rows, torch.argmax(reached.to(torch.int8), 1)],
+                             torch.full_like(un, int(entry)))
+            adj[fr[miss], R - 1] = un[miss].to(adj.dtype)
+            added += int(miss.sum())
+        ok = w >= 0
+        wv, uv = w[ok], un[ok]
+        if wv.numel():
+            wv, o = torch.sort(wv, stable=True)
+            uv = uv[o]
+            first = torch.ones_like(wv, dtype=torch.bool)
+            first[1:] = wv[1:] != wv[:-1]
+            start = torch.cummax(torch.where(first, torch.arange(wv.numel(), device=dev), torch.zeros_like(wv)), 0).values
+            slot = cnt[wv].to(torch.int64) + (torch.arange(wv.numel(), device=dev) - start)
+            fit = slot < R
+            adj[wv[fit], slot[fit]] = uv[fit].to(adj.dtype)
+            cnt.index_add_(0, wv[fit], torch.ones_like(wv[fit], dtype=cnt.dtype))
+            added += int(fit.sum())
         seen = reachable(adj, entry)
     return added, seen
 
@@ -242,13 +256,15 @@ def knn_recall(x, xn, approx, sample=1000, seed=1):
     return float(hit)
 
 
-def build_nsg(vectors, max_degree=64, seed=1, knn_k=64, n_clusters=None, n_probe=24, alpha=1.0, search_ef=0,
+def build_nsg(vectors, max_degree=64, seed=1, knn_k=64, n_clusters=None, n_probe=24, alpha=1.0, search_passes=(),
               device=None, verbose=False, vectors_device=None, stats=None):
     """NSG-style single-layer graph of max degree `max_degree` over `vectors`
-    (host [n, d] float32), medoid entry point.  search_ef > 0 adds NSG's
-    search step (candidates from searching every node at that ef).
-    vectors_device: the same rows already on the GPU (optional).  Returns a
-    formats.Graph; `stats` (dict) receives timings and graph figures."""
+    (host [n, d] float32), medoid entry point.  search_passes: (ef, alpha)
+    pairs, each one round of NSG's search step (every node searched on the
+    graph so far at that ef; its results join its candidates) pruned with
+    that alpha.  vectors_device: the same rows already on the GPU (optional).
+    Returns a formats.Graph; `stats` (dict) receives timings and graph
+    figures."""
     st = stats if stats is not None else {}
     dev = torch.device(device or "cuda")
     t_all = time.time()
@@ -277,16 +293,20 @@ def build_nsg(vectors, max_degree=64, seed=1, knn_k=64, n_clusters=None, n_probe
     torch.cuda.synchronize(dev)
     st["prune_s"] = time.time() - t
     entry = medoid(x)
-    if search_ef > 0:
+    st["mean_degree_ivf"] = float(cnt.float().mean())
+    for i, (ef_s, alpha_s) in enumerate(search_passes):
         t = time.time()
-        cand = _search_candidates(xs, x, adj, entry, search_ef, dev)
-        adj2, _ = prune(x, torch.cat([cand, adj], 1), max_degree, alpha, order)
+        cand = _search_candidates(xs, x, adj, entry, int(ef_s), dev)
+        adj2, _ = prune(x, torch.cat([cand, adj], 1), max_degree, float(alpha_s), order)
         del cand
         rev = reverse_lists(adj2, max_degree)
-        adj, cnt = prune(x, torch.cat([adj2, rev], 1), max_degree, alpha, order)
+        adj, cnt = prune(x, torch.cat([adj2, rev], 1), max_degree, float(alpha_s), order)
         del adj2, rev
         torch.cuda.synchronize(dev)
-        st["search_step_s"] = time.time() - t
+        st["search_pass_%d_s" % i] = time.time() - t
+        st["mean_degree_pass_%d" % i] = float(cnt.float().mean())
+        _log(verbose, "search pass %d (ef %d, alpha %.2f): %.1fs, mean degree %.1f" % (
+            i, ef_s, alpha_s, time.time() - t, st["mean_degree_pass_%d" % i]))
     t = time.time()
     seen = reachable(adj, entry)
     st["unreached_before"] = int((~seen).sum())
@@ -301,7 +321,8 @@ def build_nsg(vectors, max_degree=64, seed=1, knn_k=64, n_clusters=None, n_probe
     torch.cuda.empty_cache()
     st["entry"] = int(entry)
     st["build_s"] = time.time() - t_all
-    st.update(dict(n_clusters=n_clusters, n_probe=n_probe, knn_k=knn_k, alpha=alpha, search_ef=search_ef, seed=seed))
+    st.update(dict(n_clusters=n_clusters, n_probe=n_probe, knn_k=knn_k, alpha=alpha,
+                   search_passes=[list(p) for p in search_passes], seed=seed))
     _log(verbose, "nsg build %.1fs: %s" % (st["build_s"], {k: (round(v, 3) if isinstance(v, float) else v)
                                                           for k, v in st.items()}))
     return Graph.from_adjacency(xs, adj_h, entry)
@@ -309,15 +330,16 @@ def build_nsg(vectors, max_degree=64, seed=1, knn_k=64, n_clusters=None, n_probe
 
 def _search_candidates(xs, x, adj, entry, ef, dev, chunk=1 << 21):
     """NSG's candidate acquisition: every node searched on the current graph
-    (FP32 inter-query traversal from the medoid, cand queue 64, 2^18-bit
-    filter); its ef results (itself excluded by the prune) as candidates."""
+    (FP32 inter-query traversal from the medoid, cand queue 64, 2^17-bit
+    filter in shared memory); its ef results (itself excluded by the prune)
+    as candidates."""
     from .index import FalconIndex
     g = Graph.from_adjacency(xs, adj.cpu().numpy(), entry)
     ix = FalconIndex(g, device=dev.index or 0)
     n = xs.shape[0]
     out = torch.empty((n, ef), dtype=torch.int32, device=dev)
     for s in range(0, n, chunk):
-        r = ix.search(x[s:s + chunk], k=ef, ef=ef, mc=1, mg=1, cand_queue_size=64, bloom_bits=18)
+        r = ix.search(x[s:s + chunk], k=ef, ef=ef, mc=1, mg=1, cand_queue_size=64, bloom_bits=17)
         out[s:s + chunk] = r.ids
     torch.cuda.synchronize(dev)
     ix.close()

@@ -117,10 +117,14 @@ void falcon_default_params(falcon_search_params *p);
    loading + buffer migration (host.cpp:201-713, 927). */
 int falcon_index_create(const falcon_index_desc *desc, falcon_index **out);
 
-/* Load the reference's FPGA index files (meta.bin, ground_links_1_chan_0.bin,
-   ground_vectors_1_chan_0.bin, ground_labels.bin written by
+/* Load the reference's FPGA index files (meta.bin, ground_links_{nc}_chan_{i}.bin,
+   ground_vectors_{nc}_chan_{i}.bin, ground_labels.bin written by
    vector_search_baselines/scripts_hnsw/hnsw.py:264-377 and
    scripts_nsg/nsg_to_FPGA.py:56-137; read as host.cpp:201-278 reads them).
+   The single-channel set is used when present, else the first complete set
+   of nc = 2, 4, 8 or 16 channel files, whose rows (node i is row i / nc of
+   channel i % nc, the writers' round robin) are put back in node order, as
+   the multi-channel hosts read them (intra v1.5 host.cpp:242-260).
    graph_type is "HNSW" or "NSG". */
 int falcon_index_load_fpga(const char *index_dir, const char *graph_type, int32_t dim, int32_t storage,
                            int32_t device, falcon_index **out);
@@ -192,7 +196,9 @@ int falcon_descend(falcon_index *ix, const float *queries, int64_t nq, int64_t q
  *                 point (the reference's multi-DDR host sets every query to
  *                 the global entry, host.cpp:711-713)
  *   params:       one falcon_search_params, or nq of them when
- *                 per_query_params != 0 (mixed k/ef/mc in one launch)
+ *                 per_query_params != 0 (mixed k/ef/mc in one launch);
+ *                 always host memory (validated on the host, then copied to
+ *                 the device on `stream`), whatever `memory` says
  *   out_ids/out_dists: nq rows of out_stride (>= every k); the first k of a
  *                 row are the results best-first, the rest -1 / 1e20
  *   out_hops/out_visited: per query (may be NULL); hops = 1 + popped

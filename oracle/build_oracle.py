@@ -122,13 +122,17 @@ def build_ref(force=False):
                   "-Wno-unknown-pragmas", "-pthread", "-DFALCON_REF_TRACE", "-I", shim, "-I", td, harness,
                   "-o", out + ".tmp"])
         os.replace(out + ".tmp", out)
-    out = os.path.join(REF_OUT, "libhnswlib_ref.so")
     src = os.path.join(HERE, "ref_harness", "hnswlib_ref.cpp")
-    if force or _stale(out, [src]):
-        # -mavx2 (not -march=native): the library travels to other x86 hosts.
-        _run(["g++", "-O3", "-mavx2", "-mfma", "-std=c++17", "-fPIC", "-shared", "-pthread", "-I", REF_HNSWLIB,
-              src, "-o", out + ".tmp"])
-        os.replace(out + ".tmp", out)
+    # The library travels to other x86 hosts, so it is built for two ISA
+    # levels and oracle.Hnsw loads the highest one the running CPU supports:
+    # AVX2 + FMA, and x86-64-v4 (AVX-512 F/BW/CD/DQ/VL, which turns on
+    # hnswlib's own AVX-512 distance, hnswlib.h:7-9).
+    for name, isa in (("libhnswlib_ref.so", ["-mavx2", "-mfma"]), ("libhnswlib_ref_v4.so", ["-march=x86-64-v4"])):
+        out = os.path.join(REF_OUT, name)
+        if force or _stale(out, [src, os.path.abspath(__file__)]):
+            _run(["g++", "-O3"] + isa + ["-std=c++17", "-fPIC", "-shared", "-pthread", "-I", REF_HNSWLIB,
+                  src, "-o", out + ".tmp"])
+            os.replace(out + ".tmp", out)
     out = os.path.join(REF_OUT, "murmur_golden")
     src = os.path.join(HERE, "ref_harness", "murmur_golden.cpp")
     if force or _stale(out, [src]):

@@ -360,10 +360,44 @@ class Hnsw:
     def __init__(self, handle, dim):
         self.h, self.dim = handle, dim
 
+    _lib_cache = None
+
+    @staticmethod
+    def isa():
+        """The ISA level of the hnswlib build this CPU runs: "x86-64-v4"
+        (AVX-512) when /proc/cpuinfo lists avx512 f/bw/cd/dq/vl and that
+        build exists, else "avx2"."""
+        try:
+            flags = set()
+            with open("/proc/cpuinfo") as f:
+                for line in f:
+                    if line.startswith("flags"):
+                        flags = set(line.split(":", 1)[1].split())
+                        break
+        except OSError:
+            flags = set()
+        v4 = {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"} <= flags
+        if v4 and os.path.exists(os.path.join(REF_DIR, "libhnswlib_ref_v4.so")):
+            return "x86-64-v4"
+        return "avx2"
+
+    @staticmethod
+    def cpu_model():
+        try:
+            with open("/proc/cpuinfo") as f:
+                for line in f:
+                    if line.startswith("model name"):
+                        return line.split(":", 1)[1].strip()
+        except OSError:
+            pass
+        return "unknown"
+
     @staticmethod
     def _L():
-        p = os.path.join(REF_DIR, "libhnswlib_ref.so")
-        L = ctypes.CDLL(p)
+        if Hnsw._lib_cache is not None:
+            return Hnsw._lib_cache
+        name = "libhnswlib_ref_v4.so" if Hnsw.isa() == "x86-64-v4" else "libhnswlib_ref.so"
+        L = ctypes.CDLL(os.path.join(REF_DIR, name))
         L.hnsw_build.restype = ctypes.c_void_p
         L.hnsw_build.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         L.hnsw_from_graph.restype = ctypes.c_void_p
@@ -379,6 +413,8 @@ class Hnsw:
         L.hnsw_upper_rows.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.hnsw_export_upper.argtypes = [ctypes.c_void_p] * 4
         L.hnsw_descend.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p]
+        L.hnsw_set_upper.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        Hnsw._lib_cache = L
         return L
 
     @classmethod
@@ -403,6 +439,36 @@ class Hnsw:
         obj = cls(h, v.shape[1])
         obj._keep = (v, adj, counts)
         return obj
+
+    def set_upper(self, upper):
+        """Give an index made by from_graph the HNSW upper layers of a
+        formats.UpperLayers (rows: count at [0], ids from [1]); searchKnn then
+        descends them first, as in an index hnswlib built itself."""
+        levels = np.ascontiguousarray(upper.levels, dtype=np.int32)
+        starts = np.ascontiguousarray(upper.row_start, dtype=np.int64)
+        rows = np.ascontiguousarray(upper.rows, dtype=np.int32)
+        rc = self._L().hnsw_set_upper(self.h, levels.ctypes.data, starts.ctypes.data, rows.ctypes.data,
+                                      rows.shape[1], 1, int(upper.max_level), int(upper.entry))
+        if rc != 0:
+            raise ValueError("upper-layer list longer than hnswlib's maxM_")
+        self._keep_upper = (levels, starts, rows)
+
+    def search_mixed(self, queries, ks, efs, threads, out_stride=None):
+        """searchKnn with per-query k and ef: the queries are grouped by
+        (ef, k) and each group is searched with setEf(ef) over all threads.
+        Returns labels / distances [nq, out_stride] (-1 / 1e20 padded)."""
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        ks, efs = np.asarray(ks), np.asarray(efs)
+        w = int(out_stride or ks.max())
+        lab = np.full((len(q), w), -1, dtype=np.int64)
+        d = np.full((len(q), w), 1e20, dtype=np.float32)
+        for ef in np.unique(efs):
+            for k in np.unique(ks):
+                sel = np.nonzero((efs == ef) & (ks == k))[0]
+                if sel.size:
+                    l_, d_ = self.search(q[sel], int(k), int(ef), threads)
+                    lab[sel, :k], d[sel, :k] = l_, d_
+        return lab, d
 
     def level0(self):
         L = self._L()

@@ -12,7 +12,8 @@
  *     loaded into the GPU index and the oracle;
  *   - the reference CPU search baseline: searchKnn with setEf(ef) over
  *     std::threads (hnswalg.h:1115-1160, 241-325), on any graph loaded through
- *     hnsw_from_graph (single layer, given entry point);
+ *     hnsw_from_graph (base layer, given entry point) and, for HNSW graphs,
+ *     hnsw_set_upper (the upper layers searchKnn descends first);
  *   - checking the hnswlib file reader (saveIndex, hnswalg.h:588-616, and the
  *     upper layers read through get_linklist) and the upper-layer descent
  *     (searchKnn's greedy part, hnswalg.h:514-541, with hnswlib's distance).
@@ -69,6 +70,39 @@ extern "C" void *hnsw_from_graph(int64_t n, int dim, int max_degree, const float
     ix->enterpoint_node_ = (hnswlib::tableint)entry;
     ix->maxlevel_ = 0;
     return h;
+}
+
+/* Upper layers for an index made by hnsw_from_graph, in hnswlib's own
+   arrangement (linkLists_ holds element_levels_[v] rows of maxM_ ids per
+   node, hnswalg.h:371-384): node v's level-l list (1 <= l <= levels[v]) is
+   rows[(row_start[v] + l - 1) * row_stride ..], the count at [0] and the ids
+   from [ids_offset].  maxlevel_ and enterpoint_node_ are set as given, so
+   searchKnn descends them as it does an index it built itself.  Returns -1
+   when a list is longer than maxM_. */
+extern "C" int hnsw_set_upper(void *hp, const int32_t *levels, const int64_t *row_start, const int32_t *rows,
+                              int64_t row_stride, int ids_offset, int max_level, int entry)
+{
+    hnsw_handle *h = (hnsw_handle *)hp;
+    auto *ix = h->index;
+    for (size_t i = 0; i < ix->cur_element_count; i++) {
+        const int lv = levels[i];
+        ix->element_levels_[i] = lv;
+        if (lv <= 0) continue;
+        ix->linkLists_[i] = (char *)calloc((size_t)lv, ix->size_links_per_element_);
+        if (!ix->linkLists_[i]) return -1;
+        for (int l = 1; l <= lv; l++) {
+            const int32_t *row = rows + (row_start[i] + l - 1) * row_stride;
+            const int c = row[0];
+            if (c < 0 || (size_t)c > ix->maxM_) return -1;
+            hnswlib::linklistsizeint *ll = ix->get_linklist((hnswlib::tableint)i, l);
+            ix->setListCount(ll, (unsigned short)c);
+            hnswlib::tableint *dst = (hnswlib::tableint *)(ll + 1);
+            for (int j = 0; j < c; j++) dst[j] = (hnswlib::tableint)row[ids_offset + j];
+        }
+    }
+    ix->maxlevel_ = max_level;
+    ix->enterpoint_node_ = (hnswlib::tableint)entry;
+    return 0;
 }
 
 extern "C" int hnsw_info(void *hp, int64_t *n, int *max_degree, int *entry, int *max_level)

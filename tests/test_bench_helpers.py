@@ -12,13 +12,42 @@ def test_algorithmic_bytes():
     import bench
     hops = np.array([10, 20])
     vis = np.array([100, 300])
+    ks = np.array([1, 100])
+    D, R = 128, 64
     # per query: visited * D * 4 + hops * (4 + 4 * degree) + D * 4 (query) + k * 8 (results)
-    per = lambda h, v: v * bench.DIM * 4 + h * (4 + 4 * bench.MAX_DEGREE) + bench.DIM * 4 + bench.K * 8
-    assert bench.algorithmic_bytes(hops, vis, 64) == per(10, 100) + per(20, 300)
-    # BF16 gathers half the bytes; the rerank reads ef FP32 vectors
-    b16 = bench.algorithmic_bytes(hops, vis, 64, elem_bytes=2, rerank=True)
-    assert b16 == sum(v * bench.DIM * 2 + h * (4 + 4 * bench.MAX_DEGREE) + 64 * bench.DIM * 4 + bench.DIM * 4
-                      + bench.K * 8 for h, v in ((10, 100), (20, 300)))
+    per = lambda h, v, k: v * D * 4 + h * (4 + 4 * R) + D * 4 + k * 8
+    assert bench.algorithmic_bytes(hops, vis, D, R, ks) == per(10, 100, 1) + per(20, 300, 100)
+    # BF16 gathers half the bytes; the rerank reads ef FP32 vectors; D=96 pads to 96
+    efs = np.array([64, 128])
+    b16 = bench.algorithmic_bytes(hops, vis, 96, R, ks, efs, elem_bytes=2, rerank=True)
+    assert b16 == sum(v * 96 * 2 + h * (4 + 4 * R) + ef * 96 * 4 + 96 * 4 + k * 8
+                      for h, v, k, ef in ((10, 100, 1, 64), (20, 300, 100, 128)))
+    # FP8: one byte per padded dimension plus a 4-byte scale per vector; D=100 pads to 112
+    f8 = bench.algorithmic_bytes(hops, vis, 100, R, ks, elem_bytes=1, scale_bytes=4)
+    assert f8 == sum(v * (112 + 4) + h * (4 + 4 * R) + 100 * 4 + k * 8 for h, v, k in ((10, 100, 1), (20, 300, 100)))
+
+
+def test_mixed_recall_groups():
+    import bench
+    gt = np.tile(np.arange(100), (4, 1))
+    ids = np.full((4, 100), -1)
+    ids[0, :10] = np.arange(10)          # k=10, all found
+    ids[1, :1] = [5]                     # k=1, wrong
+    ids[2, :100] = np.arange(100)        # k=100, all found
+    ids[3, :10] = np.arange(5, 15)       # k=10, half found
+    r = bench.mixed_recall(ids, gt, np.array([10, 1, 100, 10]))
+    assert r["recall@1_k=1"] == 0.0
+    assert r["recall@100_k=100"] == 1.0
+    assert abs(r["recall@10_k>=10"] - (10 + 10 + 5) / 30.0) < 1e-12
+
+
+def test_cfg2_params_seeded():
+    import bench
+    e1, k1, m1 = bench.cfg2_params(1000)
+    e2, k2, m2 = bench.cfg2_params(1000)
+    assert np.array_equal(e1, e2) and np.array_equal(k1, k2) and np.array_equal(m1, m2)
+    assert set(np.unique(k1)) == {1, 10, 100} and set(np.unique(m1)) == {1, 2, 4}
+    assert (e1 >= k1).all() and set(np.unique(e1)) <= {32, 64, 100, 128, 256}
 
 
 def test_distance_error_f64():

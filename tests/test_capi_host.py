@@ -88,6 +88,31 @@ def test_fpga_files_roundtrip(tmp_path):
         assert os.path.getsize(d / "ground_vectors_1_chan_0.bin") == 2000 * (512 + 64)
 
 
+def test_multichannel_fpga_files(tmp_path):
+    """The reference writers' round robin (hnsw.py:324-335, nsg_to_FPGA.py:
+    124-135): node j is row j // nc of channel j % nc; reading puts the rows
+    back in node order, whichever channel set is present."""
+    from falcon_b200.formats import fpga_channel_sets, read_fpga_index, write_fpga_index
+    g, _ = small_graph("sift", 1001, 128, 32, 4, seed=5)   # 1001 rows: uneven channels
+    d = tmp_path / "mc"
+    write_fpga_index(str(d), g, "NSG", num_channels=(2, 4))
+    assert fpga_channel_sets(str(d)) == [2, 4]
+    row_l, row_v = 64 + 2 * 64, 512 + 64
+    for nc in (2, 4):
+        for c in range(nc):
+            rows = (1001 - c + nc - 1) // nc
+            assert os.path.getsize(d / ("ground_links_%d_chan_%d.bin" % (nc, c))) == rows * row_l
+            assert os.path.getsize(d / ("ground_vectors_%d_chan_%d.bin" % (nc, c))) == rows * row_v
+        # row 3 of channel 1 is node 3 * nc + 1
+        raw = np.fromfile(d / ("ground_links_%d_chan_1.bin" % nc), dtype=np.int32).reshape(-1, row_l // 4)
+        assert raw[3, 0] == g.counts()[3 * nc + 1]
+        assert np.array_equal(raw[3, 16:16 + raw[3, 0]], g.adjacency()[3 * nc + 1, :raw[3, 0]])
+        r = read_fpga_index(str(d), "NSG", 128, channels=nc)
+        assert np.array_equal(r.vectors, g.vectors) and np.array_equal(r.adjacency(), g.adjacency())
+    r = read_fpga_index(str(d), "NSG", 128)
+    assert np.array_equal(r.adjacency(), g.adjacency())
+
+
 def test_graph_builder_properties():
     g, _ = small_graph("unit", 2000, 96, 64, 4, seed=5)
     adj = g.adjacency()

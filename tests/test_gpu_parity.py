@@ -168,6 +168,19 @@ def test_load_fpga_files_and_labels(tmp_path):
     assert np.array_equal(h.hops, mem.hops)
 
 
+def test_load_multichannel_fpga_files(tmp_path):
+    """A directory holding only the 4-channel set (the layout of the
+    reference's 4-channel FPGA builds) loads and searches like the graph."""
+    from falcon_b200 import FalconIndex
+    from falcon_b200.formats import write_fpga_index
+    g, q = small_graph("sift", 6001, 128, 32, 32, seed=9)
+    write_fpga_index(str(tmp_path / "n4"), g, "NSG", num_channels=(4,))
+    mem = _index(g).search(q, k=10, ef=64, mc=2, mg=2)
+    r = FalconIndex.load_fpga(str(tmp_path / "n4"), "NSG", 128).search(q, k=10, ef=64, mc=2, mg=2)
+    assert _same(r.ids, r.dists, mem.ids, mem.dists)
+    assert np.array_equal(r.hops, mem.hops) and np.array_equal(r.visited, mem.visited)
+
+
 def test_device_memory_path_matches_host():
     import torch
     g, q = small_graph("unit", 6000, 96, 64, 96, seed=7)

@@ -91,7 +91,7 @@ def test_build_nsg_small_graph_searchable():
     x = sift_like(20000, 32, seed=3)
     q = sift_like(200, 32, seed=4)
     st = {}
-    g = build_nsg(x, max_degree=32, seed=1, knn_k=48, n_clusters=40, n_probe=8, stats=st)
+    g = build_nsg(x, max_degree=32, seed=1, knn_k=48, n_clusters=40, n_probe=8, search_passes=[(64, 1.0), (64, 1.2)], stats=st)
     assert st["unreached_after"] == 0
     adj = g.adjacency()
     assert adj.shape == (20000, 32) and adj.max() < 20000
