@@ -5,6 +5,10 @@ Outputs:
   oracle/_ref/libfalcon_ref_d{D}.so the reference's own v1.3 HLS kernel headers
                                     compiled as plain C++ through the harness
                                     in oracle/ref_harness/ (one per dimension D)
+  oracle/_ref/libfalcon_ref_intra_d96_c{2,4}.so
+                                    the reference's intra-query v1.5 kernel
+                                    headers through ref_intra_harness.cpp
+                                    (2 and 4 channels, D = 96)
   oracle/_ref/libfalcon_ref_trace_d128.so
                                     the same harness over the reference's trace
                                     variant (eval_trace_FPGA_inter_query_v1.3)
@@ -32,6 +36,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_ROOT = "/root/reference"
 REF_V13 = os.path.join(REF_ROOT, "FPGA_multi_DDR", "FPGA_inter_query_v1.3_longer_FIFO_alt_PR", "src")
 REF_TRACE = os.path.join(REF_ROOT, "FPGA_multi_DDR", "eval_trace_FPGA_inter_query_v1.3", "src")
+REF_V15 = os.path.join(REF_ROOT, "FPGA_multi_DDR", "FPGA_intra_query_v1.5_support_batching_longer_FIFO", "src")
+REF_INTRA_VARIANTS = ((96, 2), (96, 4))   # (D, N_CHANNEL) of the intra-query v1.5 builds
 REF_HNSWLIB = os.path.join(REF_ROOT, "networked_FPGA", "CPU_programs_oldest", "hnswlib")
 REF_MURMUR = os.path.join(REF_ROOT, "unit_tests", "bloom_and_hash", "sw_murmur2", "murmur2.cpp")
 REF_SWBLOOM = os.path.join(REF_ROOT, "unit_tests", "bloom_and_hash", "sw_bloom")
@@ -74,11 +80,18 @@ _EDITS = [
 ]
 
 
-def _patched_v13_copy(dst, dim, src=None):
+def _patched_v13_copy(dst, dim, src=None, channels=None):
     names = ["constants.hpp", "types.hpp", "utils.hpp", "priority_queue.hpp", "bloom_filter.hpp",
              "compute.hpp", "DRAM_utils.hpp", "scheduler.hpp"]
     for n in names:
         shutil.copy(os.path.join(src or REF_V13, n), os.path.join(dst, n))
+    if channels is not None:   # the intra-query v1.5 headers: channel count of the variant
+        p = os.path.join(dst, "constants.hpp")
+        s = open(p).read()
+        s2, k = re.subn(r"#define N_CHANNEL \d+", "#define N_CHANNEL %d" % channels, s)
+        if k != 1:
+            raise RuntimeError("could not set N_CHANNEL in constants.hpp")
+        open(p, "w").write(s2)
     for fname, pat, rep in _EDITS:
         p = os.path.join(dst, fname)
         s = open(p).read()
@@ -111,6 +124,18 @@ def build_ref(force=False):
             _patched_v13_copy(td, dim)
             _run(["g++", "-O1", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math",
                   "-Wno-unknown-pragmas", "-pthread", "-I", shim, "-I", td, harness, "-o", out + ".tmp"])
+        os.replace(out + ".tmp", out)
+    # the intra-query v1.5 kernel, one build per (D, N_CHANNEL)
+    intra = os.path.join(HERE, "ref_harness", "ref_intra_harness.cpp")
+    for dim, ch in REF_INTRA_VARIANTS:
+        out = os.path.join(REF_OUT, "libfalcon_ref_intra_d%d_c%d.so" % (dim, ch))
+        srcs = [intra] + [os.path.join(shim, f) for f in os.listdir(shim)] + [os.path.abspath(__file__)]
+        if not force and not _stale(out, srcs):
+            continue
+        with tempfile.TemporaryDirectory() as td:
+            _patched_v13_copy(td, dim, REF_V15, channels=ch)
+            _run(["g++", "-O1", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math",
+                  "-Wno-unknown-pragmas", "-pthread", "-I", shim, "-I", td, intra, "-o", out + ".tmp"])
         os.replace(out + ".tmp", out)
     # the trace variant of the same kernel (eval_trace_FPGA_inter_query_v1.3), D = 128
     out = os.path.join(REF_OUT, "libfalcon_ref_trace_d128.so")

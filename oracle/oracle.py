@@ -353,6 +353,43 @@ def ref_inter_search(vectors, links_ref, max_degree, queries, entries, ef=64, ca
     return oid, od, dbg[:, 0].copy(), dbg[:, 1].copy()
 
 
+def ref_intra_available(dim, channels):
+    return os.path.exists(os.path.join(REF_DIR, "libfalcon_ref_intra_d%d_c%d.so" % (dim, channels)))
+
+
+def ref_intra_search(vectors, links_ref, max_degree, queries, entries, channels, ef=64, cand_queue_size=32, mc=1,
+                     mg=1, bloom_bits=16, hash_seed=1, burst=16):
+    """Run the reference's intra-query v1.5 kernel pipeline (N channels, the
+    nodes spread round robin over them) on node-ordered reference-layout data.
+    Returns ids, dists, hops (v1.5 reports no visited count)."""
+    n, dim = vectors.shape
+    key = ("intra", dim, channels)
+    if key not in _ref_libs:
+        L = ctypes.CDLL(os.path.join(REF_DIR, "libfalcon_ref_intra_d%d_c%d.so" % (dim, channels)))
+        L.ref_intra_search.restype = ctypes.c_int
+        L.ref_intra_search.argtypes = [ctypes.c_int] * 6 + [ctypes.c_uint, ctypes.c_int, ctypes.c_int,
+                                                            ctypes.c_int64] + [ctypes.c_void_p] * 7
+        _ref_libs[key] = L
+    L = _ref_libs[key]
+    dp = pad16(dim)
+    db = np.zeros((n, dp + 16), dtype=np.float32)
+    db[:, :dim] = vectors
+    q = np.zeros((len(queries), dp), dtype=np.float32)
+    q[:, :dim] = queries
+    nq = len(queries)
+    e = np.ascontiguousarray(np.broadcast_to(np.asarray(entries, dtype=np.int32), (nq,)))
+    lk = np.ascontiguousarray(links_ref, dtype=np.int32)
+    oid = np.empty((nq, ef), dtype=np.int32)
+    od = np.empty((nq, ef), dtype=np.float32)
+    dbg = np.empty((nq, 1), dtype=np.int32)
+    rc = L.ref_intra_search(nq, ef, cand_queue_size, mc, mg, bloom_bits, hash_seed, burst, max_degree, n,
+                            e.ctypes.data, q.ctypes.data, db.ctypes.data, lk.ctypes.data, oid.ctypes.data,
+                            od.ctypes.data, dbg.ctypes.data)
+    if rc != 0:
+        raise ValueError("reference harness rejected arguments")
+    return oid, od, dbg[:, 0].copy()
+
+
 # ---------------------------------------------------------------------------
 # Reference hnswlib
 # ---------------------------------------------------------------------------

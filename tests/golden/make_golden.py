@@ -11,9 +11,15 @@ expected value comes from the reference's own code:
                          (oracle/_ref/libfalcon_ref_d{D}.so) on a seeded graph:
                          ids, distances, hops and visited per query and
                          parameter set.
+  intra_v15_d96_md64.npz the intra-query v1.5 HLS kernel pipeline run as C++
+                         (oracle/_ref/libfalcon_ref_intra_d96_c{2,4}.so, the
+                         nodes spread round robin over 2 or 4 channels) on a
+                         seeded unit-normal graph (no repeated distances, so the
+                         readiness-order channel merge is schedule independent):
+                         ids, distances and hops per query and parameter set.
 The graph is stored in the fixture (int16 adjacency); vectors and queries are
-integer-valued and regenerated from their seeds, so the fixtures stay small
-and exact on any host.
+regenerated from their seeds (integer-valued for the traversal fixtures), so
+the fixtures stay small.
 
 usage: python tests/golden/make_golden.py
 """
@@ -32,7 +38,7 @@ sys.path.insert(0, os.path.join(REPO, "oracle"))
 import build_oracle  # noqa: E402
 import oracle  # noqa: E402
 from falcon_b200.graph import build_graph  # noqa: E402
-from falcon_b200.synthetic import sift_like  # noqa: E402
+from falcon_b200.synthetic import sift_like, unit_normal  # noqa: E402
 
 TRAVERSAL_CASES = [
     # name, n, dim, max_degree, n_queries, parameter sets (ef, mc, mg, cand_queue_size, bloom_bits)
@@ -41,6 +47,10 @@ TRAVERSAL_CASES = [
     ("traversal_d96_md64", 1500, 96, 64, 16,
      [(64, 1, 1, 32, 16), (64, 2, 5, 32, 16), (48, 1, 2, 24, 14)]),
 ]
+
+INTRA_CASE = ("intra_v15_d96_md64", 1500, 96, 64, 16,
+              # channels, ef, mc, mg, bloom_bits
+              [(2, 64, 1, 1, 15), (4, 64, 2, 6, 14), (4, 128, 4, 3, 15), (2, 32, 2, 2, 16)])
 
 
 def main():
@@ -70,6 +80,21 @@ def main():
                             n=np.int32(n), dim=np.int32(dim), max_degree=np.int32(md), n_queries=np.int32(nq),
                             params=np.array(psets, dtype=np.int32), **res)
         print(name, "written")
+    name, n, dim, md, nq, psets = INTRA_CASE
+    x = unit_normal(n, dim, seed=13)
+    q = unit_normal(nq, dim, seed=14)
+    g = build_graph(x, md, device="cpu")
+    adj = g.adjacency()
+    res = {}
+    for i, (ch, ef, mc, mg, bits) in enumerate(psets):
+        ids, d, hops = oracle.ref_intra_search(g.vectors, g.links, md, q, g.entry_point, ch, ef=ef, mc=mc, mg=mg,
+                                               bloom_bits=bits)
+        res["ids_%d" % i], res["dists_%d" % i], res["hops_%d" % i] = ids, d, hops
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), adjacency=adj.astype(np.int16),
+                        entry=np.int32(g.entry_point), data_seed=np.int32(13), query_seed=np.int32(14),
+                        n=np.int32(n), dim=np.int32(dim), max_degree=np.int32(md), n_queries=np.int32(nq),
+                        params=np.array(psets, dtype=np.int32), **res)
+    print(name, "written")
 
 
 if __name__ == "__main__":
