@@ -209,6 +209,17 @@ def cfg2_workload(dev, rank=0, timings=None):
     x = sift_like_blocks(CFG2["n"], CFG2["dim"], seed=CFG2["seed_data"])
     q = sift_like_blocks(CFG2["nq"], CFG2["dim"], seed=CFG2["seed_query"] + 1000 * rank)
     tm["data_s"] = time.time() - t
+    cache = CFG2.get("graph_cache")
+    if cache and os.path.exists(cache):
+        # a graph and ground truth saved by an earlier run of the same workload (profiling runs)
+        from falcon_b200.formats import Graph
+        z = np.load(cache)
+        st = json.loads(str(z["stats"]))
+        g = Graph(x, z["links"], CFG2["degree"], int(z["entry"]))
+        gt = z["gt"]
+        tm["graph_cache"] = cache
+        log("cfg2 workload from %s" % cache)
+        return x, q, g, gt, st
     xd = torch.from_numpy(x).to(dev)
     st = {}
     t = time.time()
@@ -218,6 +229,8 @@ def cfg2_workload(dev, rank=0, timings=None):
     t = time.time()
     gt, _ = shortlist_f64_tiled(x, q[:CFG2["ngt"]], 100, shortlist=128, base_device=xd, device=dev)
     tm["ground_truth_s"] = time.time() - t
+    if cache:
+        np.savez(cache, links=g.links, entry=g.entry_point, gt=gt, stats=json.dumps(st))
     del xd
     torch.cuda.empty_cache()
     log("cfg2 workload: %s" % rounded(tm))
@@ -467,19 +480,24 @@ def run_cfg1(args, dev, local, out):
     ix.set_upper_layers(upper)
     dq = torch.from_numpy(q).to(dev)
     build_s = time.time() - t0
-    sweep = [(64, 1, 1, 32, 16), (128, 1, 1, 32, 16), (256, 1, 1, 32, 16), (256, 2, 4, 32, 16),
-             (512, 1, 1, 64, 20), (1024, 1, 1, 256, 19), (1024, 2, 4, 256, 19), (1024, 1, 4, 256, 19)]
-    pts = []
-    for ef, mc, mg, cq, bits in sweep:
-        ms, r = timed(lambda: ix.search(dq, k=k, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits), 2)
-        rec = recall_at_k(r.ids.cpu().numpy(), gt, k)
-        pts.append(dict(ef=ef, mc=mc, mg=mg, cq=cq, bits=bits, recall=rec, qps=nq / ms * 1e3, ms=ms,
-                        hops=float(r.hops.float().mean()), visited=float(r.visited.float().mean())))
-        log("cfg1 sweep %s" % rounded(pts[-1]))
-    ok = [p for p in pts if p["recall"] >= RECALL_TARGET]
-    sel = max(ok, key=lambda p: p["qps"]) if ok else max(pts, key=lambda p: p["recall"])
-    ef, mc, mg, cq, bits = sel["ef"], sel["mc"], sel["mg"], sel["cq"], sel["bits"]
-    P = dict(k=k, ef=ef, mc=mc, mg=mg, cand_queue_size=cq, bloom_bits=bits)
+    # operating point from the autotuner (falcon_b200.autotune): per ef, Bloom
+    # size from the visited count, then candidate queue and (mc, mg) for
+    # throughput at the recall target, on a 2000-query sample
+    from falcon_b200.autotune import best_for_recall, pick, tune
+    prof = tune(ix, q[:2000], gt[:2000], dim, 64, ef_list=(256, 512, 1024), k=k, recall_target=RECALL_TARGET,
+                cq_grid=(64, 256), mcmg_grid=((1, 1), (2, 4), (1, 4)), latency_channels=(4,),
+                log=lambda m: log("cfg1 " + m))
+    key, entry = best_for_recall(prof, RECALL_TARGET)
+    P = pick(prof, dim, 64, entry["throughput"]["params"]["ef"])
+    P.pop("mode", None)
+    ef, mc, mg, cq, bits = P["ef"], P["mc"], P["mg"], P["cand_queue_size"], P["bloom_bits"]
+    ms, r = timed(lambda: ix.search(dq, **P), 3)
+    sel = dict(ef=ef, mc=mc, mg=mg, cq=cq, bits=bits, recall=recall_at_k(r.ids.cpu().numpy(), gt, k),
+               qps=nq / ms * 1e3, ms=ms, hops=float(r.hops.float().mean()), visited=float(r.visited.float().mean()),
+               profile_key=key)
+    ok = sel["recall"] >= RECALL_TARGET
+    pts = [rounded({kk: v for kk, v in row.items()}) for e in prof.values() for row in e["grid"]]
+    log("cfg1 selected by the autotuner: %s" % rounded(sel))
     ms_b, rb = timed(lambda: ix.search(dq, precision="bf16", rerank=True, **P))
     ms_f, rf = timed(lambda: ix.search(dq, precision="fp8", rerank=True, **P))
     r = ix.search(dq, **P)
@@ -509,14 +527,15 @@ def run_cfg1(args, dev, local, out):
         pl.update(extra)
         p50, p99 = batch1_latency(ix, dq, args.latency_samples, **pl)
         lat_sel[mode] = {"p50_ms": p50, "p99_ms": p99}
-    served = None if args.no_serve else serve_cfg1(ix, q, gt, P, nq / (ms_b / 1e3))
+    served = None if args.no_serve else serve_cfg1(ix, q, gt, prof, ef, nq / (ms_b / 1e3))
     ix.close()
     out["cfg1"] = {
         "workload": "deep1m_hnsw_m32: 1M x 96 unit-normal (seeded Deep1M stand-in), HNSW-style M=32 graph (exact "
                     "kNN + hnswlib's neighbour heuristic + reverse edges, upper layers with hnswlib's level "
                     "distribution), 10k queries, k=10; searches descend the upper layers",
-        "n_base": n, "build_s": build_s, "sweep": [rounded(p) for p in pts], "selected": rounded(sel),
+        "n_base": n, "build_s": build_s, "autotuner_grid": pts, "selected": rounded(sel),
         "recall_target_reached": bool(ok),
+        "latency_pick": {kk: v for kk, v in entry["latency"].items()},
         "bf16_rerank": {"value": nq / (ms_b / 1e3), "unit": "queries/s",
                         "recall@10": recall_at_k(rb.ids.cpu().numpy(), gt, k)},
         "fp8_rerank": {"value": nq / (ms_f / 1e3), "unit": "queries/s",
@@ -525,19 +544,19 @@ def run_cfg1(args, dev, local, out):
         "served": served}
 
 
-def serve_cfg1(ix, q, gt, P, batched_bf16_qps):
+def serve_cfg1(ix, q, gt, prof, ef, batched_bf16_qps):
     """Continuous batching of single-query requests (BF16 traversal + exact
     FP32 rerank) with Poisson arrivals at 50 %, 80 % of the batched BF16 rate
-    and at saturation."""
-    from falcon_b200 import make_params
+    and at saturation; each request's parameters come from the autotuner's
+    profile for its ef (FalconServer.auto_params)."""
     from falcon_b200.groundtruth import recall_at_k
     from falcon_b200.serving import FalconServer, poisson_arrivals
-    k = P["k"]
-    sv = FalconServer(ring_capacity=65536, max_k=k, ef_max=P["ef"], cand_queue_max=P["cand_queue_size"],
-                      bloom_bits_max=P["bloom_bits"], mc_max=max(P["mc"], 1), mg_max=max(P["mg"], 1), dim_max=96,
-                      idle_exit_us=5000)
+    k = 10
+    sv = FalconServer(ring_capacity=65536, max_k=k, ef_max=ef, cand_queue_max=256, bloom_bits_max=20, mc_max=4,
+                      mg_max=4, dim_max=96, idle_exit_us=5000)
     iid = sv.add_index(ix)
-    p = make_params(precision="bf16", rerank=True, **P)
+    sv.set_profile(prof)
+    p = sv.auto_params(iid, k=k, ef=ef, precision="bf16", rerank=True)
     n = 2 * len(q)
     qq = np.concatenate([q, q])
     out = {"precision": "bf16+fp32 rerank", "requests_per_point": n, "points": [],
@@ -716,7 +735,7 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
     threads = os.cpu_count() or 1
-    cfgs = [int(c) for c in args.configs.split(",") if c.strip()]
+    cfgs = [int(c) for c in args.configs.split(",") if c.strip().isdigit()]
     out = {}
     t0 = time.time()
     H2 = headline_cfg2(args, dev, local, rank, ws, out)
@@ -821,6 +840,9 @@ def main():
     ap.add_argument("--cfg3-n", type=int, default=1_000_000)
     ap.add_argument("--latency-samples", type=int, default=200)
     ap.add_argument("--ref-queries", type=int, default=4000, help="reference arm: queries per step")
+    ap.add_argument("--graph-cache", default=None,
+                    help="configs[2]: load the graph and ground truth from this .npz if it exists, else save them "
+                         "there (for repeated profiling runs of one workload)")
     ap.add_argument("--profile-region", action="store_true",
                     help="bracket only the timed headline steps with cudaProfilerStart/Stop and exit after them")
     args = ap.parse_args()
@@ -828,6 +850,7 @@ def main():
         args.warmup = 3
     if args.n_base:
         CFG2["n"] = args.n_base
+    CFG2["graph_cache"] = args.graph_cache
     if args.n_queries:
         CFG2["nq"] = args.n_queries
         CFG2["ngt"] = min(CFG2["ngt"], args.n_queries)

@@ -64,6 +64,7 @@ struct DescendLaunch {
     int32_t *out_entry;
     int64_t out_entry_stride;       // int32 units between queries' entries (0: contiguous)
     int32_t *out_hops;              // may be null
+    const int32_t *rows;            // may be null: query i is row rows[i] of queries and of out_entry
 };
 
 // Per-query search parameters as the kernels read them.
@@ -136,7 +137,8 @@ struct ServeDesc {
 // and the 16-byte register rows per lane its vectors take: FP32 1..4, BF16
 // 1..2, FP8 1.  One kernel holding several traversal variants (called or
 // inlined) spills inside the hop loop, so each class has its own kernel and
-// its own claim queue, and the host runs one class kernel at a time.
+// its own claim queue; the kernels of the classes with work run at the same
+// time, each on its own stream over a share of the SMs.
 constexpr int kServeClasses = 7;
 
 __host__ __device__ constexpr int serve_class(int precision, int vrows)
@@ -153,10 +155,10 @@ __host__ __device__ constexpr int serve_vrows(int dpad, int precision)
 struct ServeCtl {
     unsigned long long head[kServeClasses];   // per class queue: requests claimed by warps
     unsigned long long tail[kServeClasses];   // per class queue: requests published by the host
-    long long last_active_ns;       // last claim or completion (globaltimer)
+    long long last_active_ns[kServeClasses];  // per class: last claim or completion (globaltimer)
+    uint32_t yield_epoch[kServeClasses];      // host: class c's launch with this epoch leaves between requests
     int32_t stop;                   // host: leave when idle
     int32_t error;
-    uint32_t yield_epoch;           // host: the launch with this epoch leaves between requests
 };
 
 struct ServeLaunch {
@@ -165,7 +167,7 @@ struct ServeLaunch {
     const ServeDesc *ring;
     int32_t ring_cap;
     const int32_t *class_slots;     // kServeClasses x ring_cap: ring entries in each class's claim order
-    const uint32_t *run_epoch;      // host-mapped: epoch of the current launch, read once at start
+    const uint32_t *run_epoch;      // host-mapped, per class: epoch of its current launch, read once at start
     const float *qpool;             // ring_cap x qstride (device)
     int32_t qstride;
     int32_t *out_ids;               // ring_cap x out_stride (host-mapped)
@@ -181,16 +183,30 @@ struct ServeLaunch {
     int32_t *cand_ids;              // per warp ef_max (rerank candidates)
     float *cand_d;
     long long idle_ns;
+    int32_t warp_base;              // first per-warp scratch slot (Bloom, rerank) of this launch
 };
 
+// Rerank scratch of a serving warp without the bucketed list: ef_max
+// distances and ids.
+__host__ __device__ inline size_t serve_rerank_bytes(int ef_max)
+{
+    return ((size_t)ef_max * (sizeof(float) + sizeof(int)) + 15) & ~(size_t)15;
+}
+
+// Shared memory of one serving warp: the traversal's (Bloom filter when it
+// fits, bucketed result list of heap_cap slots or sorted lists of list_r +
+// list_c slots, group FIFO, staged ids), then the rerank scratch unless the
+// rerank reuses the bucketed list's space.
 __host__ __device__ inline size_t serve_warp_smem_bytes(int bloom_bits_max, int mc_max, int mg_max, int heap_cap,
-                                                        int ef_max)
+                                                        int list_r, int list_c, int ef_max)
 {
     size_t b = (bloom_bits_max <= kMaxSmemBloomBits) ? ((size_t)1 << (bloom_bits_max - 3)) : 0;
     b += (size_t)heap_cap * (sizeof(uint64_t) + sizeof(int));
-    if (heap_cap == 0) b += (size_t)ef_max * (sizeof(float) + sizeof(int));   // else the heap is reused
+    b += (size_t)(list_r + list_c) * (sizeof(float) + sizeof(int));
     b += sizeof(int) * (size_t)(mc_max * mg_max + mg_max + kSidsPerWarp);
-    return (b + 15) & ~(size_t)15;
+    b = (b + 15) & ~(size_t)15;
+    if (heap_cap == 0) b += serve_rerank_bytes(ef_max);
+    return b;
 }
 
 // Serving kernel of request class `cls` for entries-per-lane `epl` (8 or 32).

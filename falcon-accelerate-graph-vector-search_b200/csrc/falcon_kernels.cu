@@ -615,6 +615,158 @@ __device__ __forceinline__ void trace_batch(const TraceIO *tr, int &n, bool rec,
     n += __popc(m);
 }
 
+// ---------------------------------------------------------------------------
+// Batch merge (intra-query kernel, ef <= 256: both queues sorted in shared
+// memory, merged by warp 0 while the channel warps wait for the group).
+//
+// In the sorted-list model above, inserting x_1..x_m one at a time (x_j kept
+// iff its distance is below the result list's current maximum, then forwarded
+// to the candidate list iff also below that list's maximum) has a closed
+// form, because a maximum only ever decreases while results are collected:
+//   * the result list afterwards holds the ef smallest keys (distance, age)
+//     of the old list and x_1..x_m, and x_j is kept iff fewer than ef of
+//     {old entries, x_1..x_{j-1}} have a distance <= d_j (an x_i rejected
+//     earlier with d_i <= d_j implies d_j is rejected too, so counting it
+//     changes nothing);
+//   * x_j is forwarded iff it is kept and fewer than cq of {old candidate
+//     entries, kept x_i with i < j} have a distance <= d_j (a kept x_i that
+//     was not forwarded had d_i >= the candidate maximum, so again counting it
+//     changes nothing);
+//   * the merged order is by (distance, age): old entries before new ones of
+//     equal distance, new ones in stream order.
+// So a window of up to 32 stream slots (lane j = slot j) is merged at once
+// (in the one-warp kernels few slots per window pass the threshold at these
+// ef, and inserting them one at a time in registers measured faster):
+// each lane counts the old entries <= its distance by binary search, the
+// earlier slots by a ballot loop, and the lists are rewritten in place with
+// every entry at its merged position.  The outcome is the one-at-a-time
+// insertion's, entry for entry.
+// ---------------------------------------------------------------------------
+struct SmemLists {
+    float *rd;    // result list distances [0, ef)
+    int *ri;
+    float *cd;    // candidate list distances [0, cq)
+    int *ci;
+};
+
+// Entries of the ascending a[0..n) that are <= x.
+__device__ __forceinline__ int count_le(const float *a, int n, float x)
+{
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] <= x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Rewrite the ascending list a/ai[0..n) (PER entries per lane at p = lane +
+// 32 e) merged with the lanes of mask m, each at its merged position newpos:
+// an old entry moves right by the number of new entries with a smaller
+// distance; entries pushed to position n or beyond drop out.
+template <int PER>
+__device__ __forceinline__ void list_merge_rewrite(float *a, int *ai, int n, unsigned m, float d, int id, int newpos,
+                                                   int lane)
+{
+    float od[PER];
+    int oi[PER], sh[PER];
+#pragma unroll
+    for (int e = 0; e < PER; e++) {
+        const int p = lane + 32 * e;
+        od[e] = (p < n) ? a[p] : 0.0f;
+        oi[e] = (p < n) ? ai[p] : -1;
+        sh[e] = 0;
+    }
+    for (unsigned mm = m; mm; mm &= mm - 1) {
+        const float dj = __shfl_sync(kFull, d, __ffs(mm) - 1);
+#pragma unroll
+        for (int e = 0; e < PER; e++) sh[e] += (dj < od[e]) ? 1 : 0;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < PER; e++) {
+        const int p = lane + 32 * e, q = p + sh[e];
+        if (p < n && q < n) {
+            a[q] = od[e];
+            ai[q] = oi[e];
+        }
+    }
+    if (((m >> lane) & 1u) && newpos < n) {
+        a[newpos] = d;
+        ai[newpos] = id;
+    }
+    __syncwarp();
+}
+
+// Merge the window (lane j: slot j, `valid` lanes only) into both lists.
+template <int EPL, int CPL>
+__device__ __forceinline__ void merge_window(const SmemLists &L, int ef, int cq, float d, int id, bool valid, int lane,
+                                             float &rmax, float &cmax)
+{
+    const unsigned vm = __ballot_sync(kFull, valid && d < rmax);
+    if (vm == 0) return;
+    const bool in = (vm >> lane) & 1u;
+    const int r_le = in ? count_le(L.rd, ef, d) : ef;
+    int b_le = 0;
+    for (unsigned m = vm; m; m &= m - 1) {
+        const int i = __ffs(m) - 1;
+        const float di = __shfl_sync(kFull, d, i);
+        b_le += (i < lane && di <= d) ? 1 : 0;
+    }
+    const bool kept = in && r_le + b_le < ef;
+    const unsigned km = __ballot_sync(kFull, kept);
+    int k_before = 0, k_le = 0;
+    for (unsigned m = km; m; m &= m - 1) {
+        const int i = __ffs(m) - 1;
+        const float di = __shfl_sync(kFull, d, i);
+        k_before += (di < d || (di == d && i < lane)) ? 1 : 0;
+        k_le += (i < lane && di <= d) ? 1 : 0;
+    }
+    const int c_le = kept ? count_le(L.cd, cq, d) : cq;
+    const bool fwd = kept && c_le + k_le < cq;
+    const unsigned fm = __ballot_sync(kFull, fwd);
+    int f_before = 0;
+    for (unsigned m = fm; m; m &= m - 1) {
+        const int i = __ffs(m) - 1;
+        const float di = __shfl_sync(kFull, d, i);
+        f_before += (di < d || (di == d && i < lane)) ? 1 : 0;
+    }
+    list_merge_rewrite<EPL>(L.rd, L.ri, ef, km, d, id, r_le + k_before, lane);
+    rmax = L.rd[ef - 1];
+    if (fm) {
+        list_merge_rewrite<CPL>(L.cd, L.ci, cq, fm, d, id, c_le + f_before, lane);
+        cmax = L.cd[cq - 1];
+    }
+}
+
+// pop_top of the candidate list in shared memory: the best entry leaves, the
+// rest move up one, a +large placeholder enters at position cq - 1.
+template <int CPL>
+__device__ __forceinline__ int list_pop(float *cd, int *ci, int cq, int lane)
+{
+    const int pid = ci[0];
+    float t[CPL];
+    int ti[CPL];
+#pragma unroll
+    for (int e = 0; e < CPL; e++) {
+        const int nx = lane + 32 * e + 1;
+        t[e] = (nx < cq) ? cd[nx] : kLarge;
+        ti[e] = (nx < cq) ? ci[nx] : -1;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < CPL; e++) {
+        const int p = lane + 32 * e;
+        if (p < cq) {
+            cd[p] = t[e];
+            ci[p] = ti[e];
+        }
+    }
+    __syncwarp();
+    return pid;
+}
+
 // ROW selects the whole-row Bloom path for degrees <= 64; instances whose
 // vector registers leave no room for it keep the per-32-id path.
 template <int ELEM, int EPL, int VROWS, bool ROW, bool TRACE = false>
@@ -885,32 +1037,89 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
     }
 }
 
-__host__ __device__ __forceinline__ size_t warp_smem_bytes(int bloom_bits_max, int mc_max, int mg_max, int heap_cap)
+// Shared memory of one warp: Bloom filter (when it fits), the bucketed
+// result list (heap_cap slots) or the two sorted lists (list_r + list_c
+// slots), the group FIFO and the staged neighbour ids.
+__host__ __device__ __forceinline__ size_t warp_smem_bytes(int bloom_bits_max, int mc_max, int mg_max, int heap_cap,
+                                                           int list_r, int list_c)
 {
     size_t b = (bloom_bits_max <= kMaxSmemBloomBits) ? ((size_t)1 << (bloom_bits_max - 3)) : 0;
     b += (size_t)heap_cap * (sizeof(uint64_t) + sizeof(int));
+    b += (size_t)(list_r + list_c) * (sizeof(float) + sizeof(int));
     b += sizeof(int) * (size_t)(mc_max * mg_max + mg_max + kSidsPerWarp);
     return (b + 15) & ~(size_t)15;
 }
 
+// Pointers into one warp's shared memory (layout of warp_smem_bytes).
+struct WarpSmem {
+    uint32_t *bloom;
+    uint64_t *hkey;
+    int *hid;
+    SmemLists lists;
+    int *fifo, *fifo_len, *sids;
+};
+
+__device__ __forceinline__ WarpSmem carve_warp_smem(unsigned char *wbase, uint32_t *bloom_global, bool smem_bloom,
+                                                    size_t bloom_bytes, int heap_cap, int list_r, int list_c,
+                                                    int mc_max, int mg_max)
+{
+    WarpSmem w;
+    w.bloom = smem_bloom ? reinterpret_cast<uint32_t *>(wbase) : bloom_global;
+    unsigned char *p = wbase + (smem_bloom ? bloom_bytes : 0);
+    w.hkey = reinterpret_cast<uint64_t *>(p);
+    p += sizeof(uint64_t) * heap_cap;
+    w.hid = reinterpret_cast<int *>(p);
+    p += sizeof(int) * heap_cap;
+    w.lists.rd = reinterpret_cast<float *>(p);
+    p += sizeof(float) * list_r;
+    w.lists.ri = reinterpret_cast<int *>(p);
+    p += sizeof(int) * list_r;
+    w.lists.cd = reinterpret_cast<float *>(p);
+    p += sizeof(float) * list_c;
+    w.lists.ci = reinterpret_cast<int *>(p);
+    p += sizeof(int) * list_c;
+    w.fifo = reinterpret_cast<int *>(p);
+    w.fifo_len = w.fifo + mc_max * mg_max;
+    w.sids = w.fifo_len + mg_max;
+    return w;
+}
+
+// Shared-memory list capacities: the bucketed result list for ef > 256 (all
+// kernels), and the sorted lists for ef <= 256 (the intra-query kernel only;
+// the one-warp traversal keeps those lists in registers).
+template <int EPL, bool SORTED_LISTS = false> struct ListCaps {
+    static constexpr int heap = (EPL > 8) ? 32 * EPL : 0;
+    static constexpr int r = (EPL > 8 || !SORTED_LISTS) ? 0 : 32 * EPL;
+    static constexpr int c = (EPL > 8 || !SORTED_LISTS) ? 0 : 32 * CandPerLane<EPL>::value;
+};
+
+// Resident blocks of 4 warps the one-warp traversal is compiled for.  3 (168
+// registers) keeps the gather batch and the lists in registers without
+// spilling.  FP32 rows of one 512-byte segment row (D <= 128) at ef <= 256
+// run 4 (128 registers): the 16 warps per SM hide more gather latency than
+// the ~100 bytes of spilled loop state cost (913.6k -> 985.5k queries/s on
+// the 10M x 128 mixed-parameter workload).  FALCON_INTER_BLOCKS_SMALL_EF
+// overrides that choice.
+#ifndef FALCON_INTER_BLOCKS_SMALL_EF
+#define FALCON_INTER_BLOCKS_SMALL_EF 4
+#endif
+template <int ELEM, int EPL, int VROWS> struct InterBlocks {
+    static constexpr int value = (ELEM == kF32 && VROWS == 1 && EPL <= 8) ? FALCON_INTER_BLOCKS_SMALL_EF : 3;
+};
+
 template <int ELEM, int EPL, int VROWS, bool TRACE>
-__global__ void __launch_bounds__(128, 3) inter_kernel(const SearchLaunch A)
+__global__ void __launch_bounds__(128, (InterBlocks<ELEM, EPL, VROWS>::value)) inter_kernel(const SearchLaunch A)
 {
     extern __shared__ uint4 smem_u4[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    constexpr int HEAP_CAP = (EPL > 8) ? 32 * EPL : 0;
-    const size_t wbytes = warp_smem_bytes(A.bloom_bits_max, A.mc_max, A.mg_max, HEAP_CAP);
+    using Caps = ListCaps<EPL>;
+    const size_t wbytes = warp_smem_bytes(A.bloom_bits_max, A.mc_max, A.mg_max, Caps::heap, Caps::r, Caps::c);
     unsigned char *wbase = reinterpret_cast<unsigned char *>(smem_u4) + wbytes * warp;
     const bool smem_bloom = A.bloom_bits_max <= kMaxSmemBloomBits;
     const size_t bloom_bytes = (size_t)1 << (A.bloom_bits_max - 3);
-    uint32_t *bloom = smem_bloom ? reinterpret_cast<uint32_t *>(wbase)
-                                 : A.bloom_global + ((size_t)blockIdx.x * 4 + warp) * (bloom_bytes / 4);
-    unsigned char *after_bloom = wbase + (smem_bloom ? bloom_bytes : 0);
-    uint64_t *hkey = reinterpret_cast<uint64_t *>(after_bloom);
-    int *hid = reinterpret_cast<int *>(after_bloom + sizeof(uint64_t) * HEAP_CAP);
-    int *fifo = reinterpret_cast<int *>(after_bloom + (sizeof(uint64_t) + sizeof(int)) * HEAP_CAP);
-    int *fifo_len = fifo + A.mc_max * A.mg_max;
-    int *sids = fifo_len + A.mg_max;
+    uint32_t *gbloom = smem_bloom ? nullptr : A.bloom_global + ((size_t)blockIdx.x * 4 + warp) * (bloom_bytes / 4);
+    const WarpSmem W = carve_warp_smem(wbase, gbloom, smem_bloom, bloom_bytes, Caps::heap, Caps::r, Caps::c, A.mc_max,
+                                       A.mg_max);
     for (;;) {
         unsigned long long qi = 0;
         if (lane == 0) qi = atomicAdd(reinterpret_cast<unsigned long long *>(A.work_counter), 1ull);
@@ -936,11 +1145,11 @@ __global__ void __launch_bounds__(128, 3) inter_kernel(const SearchLaunch A)
             tio.id = A.trace_id + (int64_t)qi * A.trace_cap;
             tio.cap = A.trace_cap;
             tio.counts = A.trace_counts + 3 * (int64_t)qi;
-            search_one_inter<ELEM, EPL, VROWS, kRowBloom<ELEM, VROWS>, true>(A.g, P, io, bloom, fifo, fifo_len, sids,
-                                                                             hkey, hid, lane, &tio);
+            search_one_inter<ELEM, EPL, VROWS, kRowBloom<ELEM, VROWS>, true>(A.g, P, io, W.bloom, W.fifo, W.fifo_len,
+                                                                             W.sids, W.hkey, W.hid, lane, &tio);
         } else {
-            search_one_inter<ELEM, EPL, VROWS, kRowBloom<ELEM, VROWS>>(A.g, P, io, bloom, fifo, fifo_len, sids, hkey,
-                                                                       hid, lane);
+            search_one_inter<ELEM, EPL, VROWS, kRowBloom<ELEM, VROWS>>(A.g, P, io, W.bloom, W.fifo, W.fifo_len, W.sids,
+                                                                       W.hkey, W.hid, lane);
         }
         __syncwarp();
     }
@@ -948,15 +1157,21 @@ __global__ void __launch_bounds__(128, 3) inter_kernel(const SearchLaunch A)
 
 // ---------------------------------------------------------------------------
 // Intra-query mode (reference intra-query v1.5): one thread block per query,
-// `channels` warps.  Per retired group the block
+// `channels` channels of W warps each (W only spreads the work; results do
+// not depend on it).  Per retired group the block
 //   1. routes the group's neighbour ids to channel id & (channels-1) keeping
-//      stream order (utils.hpp:396-495, split_tasks_to_channels),
-//   2. lets warp c run its own Bloom filter, gather and L2 over channel c
-//      (the reference's per-channel bloom/fetch/compute PEs),
-//   3. merges the channels in channel order into the queues in warp 0
+//      stream order (utils.hpp:396-495, split_tasks_to_channels), and the
+//      channel's first warp runs the channel's Bloom filter over them
+//      (the reference's per-channel bloom PE), keeping the new ids in order;
+//   2. the channel's W warps gather the new vectors and form their distances
+//      (the per-channel fetch/compute PEs), batches dealt round robin;
+//   3. warp 0 merges the channels in channel order into the queues
 //      (gather_distances_from_channels, utils.hpp:497-569, merges in
-//      readiness order; channel order is one of its schedules), then the
-//      scheduler refills the group FIFO (v1.5 scheduler.hpp:94-146).
+//      readiness order; channel order is one of its schedules; a whole
+//      group is merged before the scheduler acts, so on distinct distances
+//      the order cannot change the outcome), then the scheduler refills the
+//      group FIFO (v1.5 scheduler.hpp:94-146) and prefetches the rows of the
+//      candidates it popped.
 // The stale-threshold prefilter of v1.5 (utils.hpp:277-347) is omitted: it
 // only drops distances that the result queue would reject anyway.
 // ---------------------------------------------------------------------------
@@ -967,17 +1182,21 @@ struct IntraSmem {
     int chan_visited[kMaxChannels];
 };
 
+// Most warps an intra-query block uses (channels x warps per channel).
+constexpr int kIntraMaxWarps = 16;
+
 template <int ELEM, int EPL, int VROWS>
-__global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
+__global__ void __launch_bounds__(32 * kIntraMaxWarps) intra_kernel(const SearchLaunch A)
 {
     extern __shared__ uint4 smem_u4[];
     constexpr int EPS = ET<ELEM>::EPS;
     constexpr int NB = (VROWS == 1) ? 8 : 4;
     constexpr bool HEAP = EPL > 8;
-    constexpr int REPL = HEAP ? 1 : EPL;
     constexpr int HEAP_CAP = HEAP ? 32 * EPL : 0;
-    const int C = blockDim.x >> 5;
+    const int C = A.channels;
+    const int W = (blockDim.x >> 5) / C;                  // warps per channel
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int chan = warp / W, sub = warp - chan * W;
     const GraphView &g = A.g;
     const int nseg = g.dpad * ET<ELEM>::BYTES / 16;
     unsigned char *base_ptr = reinterpret_cast<unsigned char *>(smem_u4);
@@ -985,10 +1204,10 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
     size_t off = (sizeof(IntraSmem) + 15) & ~(size_t)15;
     const size_t bloom_bytes = (size_t)1 << (A.bloom_bits_max - 3);
     const bool smem_bloom = A.bloom_bits_max <= kMaxSmemBloomBits;
-    uint32_t *bloom = smem_bloom ? reinterpret_cast<uint32_t *>(base_ptr + off + bloom_bytes * warp)
-                                 : A.bloom_global + ((size_t)blockIdx.x * C + warp) * (bloom_bytes / 4);
+    uint32_t *bloom = smem_bloom ? reinterpret_cast<uint32_t *>(base_ptr + off + bloom_bytes * chan)
+                                 : A.bloom_global + ((size_t)blockIdx.x * C + chan) * (bloom_bytes / 4);
     if (smem_bloom) off += bloom_bytes * C;
-    // channel c's ids (then its surviving ids and distances) of the current
+    // channel c's ids (then its new ids and their distances) of the current
     // group: lcap slots at c * lcap
     const int lcap = A.mc_max * g.max_degree;
     int *list_id = reinterpret_cast<int *>(base_ptr + off);
@@ -999,20 +1218,26 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
     off += sizeof(int) * (size_t)(A.mc_max * A.mg_max);
     int *fifo_len = reinterpret_cast<int *>(base_ptr + off);
     off += sizeof(int) * (size_t)A.mg_max;
-    int *sids = reinterpret_cast<int *>(base_ptr + off) + 32 * warp;
-    off += sizeof(int) * 32 * C;
     off = (off + 15) & ~(size_t)15;
     uint64_t *hkey = reinterpret_cast<uint64_t *>(base_ptr + off);
     int *hid = reinterpret_cast<int *>(base_ptr + off + sizeof(uint64_t) * HEAP_CAP);
+    off += (sizeof(uint64_t) + sizeof(int)) * HEAP_CAP;
+    using Caps = ListCaps<EPL, true>;
+    SmemLists L;   // sorted lists for ef <= 256, used by warp 0
+    L.rd = reinterpret_cast<float *>(base_ptr + off);
+    L.ri = reinterpret_cast<int *>(L.rd + Caps::r);
+    L.cd = reinterpret_cast<float *>(L.ri + Caps::r);
+    L.ci = reinterpret_cast<int *>(L.cd + Caps::c);
     // lane groups and gather batches as in search_one_inter
     const uint32_t vbytes = (uint32_t)nseg * 16u;
+    const uint32_t rbytes = (uint32_t)(g.ids_off + g.max_degree) * 4u;
     const int lg = lane_group_log2<VROWS, NB>(nseg);
     const int BS = (32 >> lg) * NB;
     const int gmask = (1 << lg) - 1;
     const bool rep_lane = (lane & gmask) < NB;
     const int my_slot = (lane >> lg) * NB + (lane & gmask);
-    int *my_ids = list_id + (size_t)lcap * warp;
-    float *my_d = list_d + (size_t)lcap * warp;
+    int *my_ids = list_id + (size_t)lcap * chan;
+    float *my_d = list_d + (size_t)lcap * chan;
 
     for (;;) {
         if (threadIdx.x == 0) S->qi = atomicAdd(reinterpret_cast<unsigned long long *>(A.work_counter), 1ull);
@@ -1034,31 +1259,29 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
                 }
             }
         }
-        {
+        if (sub == 0) {
             const int nvec = 1 << (P.bloom_bits - 7);
             uint4 *b4 = reinterpret_cast<uint4 *>(bloom);
             for (int i = lane; i < nvec; i += 32) b4[i] = make_uint4(0, 0, 0, 0);
         }
         const uint32_t bmask = (1u << P.bloom_bits) - 1u;
         int visited = 0;
-        // queues live in warp 0
-        float rd[REPL];
-        int ri[REPL];
-#pragma unroll
-        for (int e = 0; e < REPL; e++) {
-            rd[e] = (lane * EPL + e < P.ef) ? kLarge : __int_as_float(0x7f800000);
-            ri[e] = -1;
-        }
+        // queues live in warp 0: the bucketed list + register candidate list
+        // for ef > 256, else the sorted lists L in shared memory
         uint32_t age = 0;
         BucketMax BM;
+        constexpr int CPL = CandPerLane<EPL>::value;
+        float cd[HEAP ? CPL : 1];
+        int ci[HEAP ? CPL : 1];
         if constexpr (HEAP) {
             if (warp == 0) bucket_init<EPL>(BM, hkey, hid, P.ef, lane);
-        }
-        constexpr int CPL = CandPerLane<EPL>::value;
-        float cd[CPL];
-        int ci[CPL];
 #pragma unroll
-        for (int e = 0; e < CPL; e++) { cd[e] = kLarge; ci[e] = -1; }
+            for (int e = 0; e < CPL; e++) { cd[e] = kLarge; ci[e] = -1; }
+        } else if (warp == 0) {
+            for (int p = lane; p < P.ef; p += 32) { L.rd[p] = kLarge; L.ri[p] = -1; }
+            for (int p = lane; p < P.cq; p += 32) { L.cd[p] = kLarge; L.ci[p] = -1; }
+            __syncwarp();
+        }
         float rmax = kLarge, cmax = kLarge;
         if (threadIdx.x == 0) {
             int entry = A.entries ? A.entries[qi] : A.default_entry;
@@ -1079,47 +1302,55 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
         while (S->inflight > 0) {
             const int head = S->head;
             const int glen = fifo_len[head];
-            // 1. route: this channel's ids of the group's rows, in stream order
-            int count = 0;
-            for (int b = 0; b < glen; b++) {
-                const int32_t *row = g.links + (int64_t)fifo[head * mc + b] * g.lstride;
-                const int cnt = ld_nc_s32(row);
-                for (int c0 = 0; c0 < cnt; c0 += 32) {
-                    const int nb = (c0 + lane < cnt) ? ld_nc_s32(row + g.ids_off + c0 + lane) : -1;
-                    const bool mine = nb >= 0 && (nb & (C - 1)) == warp;
-                    const unsigned mm = __ballot_sync(kFull, mine);
-                    if (mine) my_ids[count + __popc(mm & ((1u << lane) - 1u))] = nb;
-                    count += __popc(mm);
-                }
-            }
-            __syncwarp();
-            // 2. this channel: Bloom, gather, distances; survivors compacted in place
-            int nvalid = 0;
-            for (int c0 = 0; c0 < count; c0 += 32) {
-                const bool act = c0 + lane < count;
-                const int nb = act ? my_ids[c0 + lane] : -1;
-                const bool valid = bloom_chunk(bloom, bmask, P.seed, nb, act, lane);
-                const unsigned vm = __ballot_sync(kFull, valid);
-                const int V = __popc(vm);
-                visited += V;
-                if (valid) sids[__popc(vm & ((1u << lane) - 1u))] = nb;
-                if (valid) prefetch_l2(g.vecs + (int64_t)nb * g.vstride_bytes, vbytes);
-                __syncwarp();
-                uint4 raw[NB][VROWS];
-                float scale[NB];
-                if (V > 0) gather_batch<ELEM, VROWS, NB>(g, sids, 0, V, nseg, lane, lg, raw, scale);
-                for (int b0 = 0; b0 < V; b0 += BS) {
-                    const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane, lg);
-                    if (b0 + BS < V) gather_batch<ELEM, VROWS, NB>(g, sids, b0 + BS, V, nseg, lane, lg, raw, scale);
-                    if (rep_lane && b0 + my_slot < V) {
-                        my_ids[nvalid + b0 + my_slot] = sids[b0 + my_slot];
-                        my_d[nvalid + b0 + my_slot] = dist;
+            // 1. the channel's first warp: its ids of the group's rows in stream
+            //    order, then its Bloom filter; the new ids are compacted in place
+            if (sub == 0) {
+                int count = 0;
+                for (int b = 0; b < glen; b++) {
+                    const int32_t *row = g.links + (int64_t)fifo[head * mc + b] * g.lstride;
+                    const int cnt = ld_nc_s32(row);
+                    for (int c0 = 0; c0 < cnt; c0 += 32) {
+                        const int nb = (c0 + lane < cnt) ? ld_nc_s32(row + g.ids_off + c0 + lane) : -1;
+                        const bool mine = nb >= 0 && (nb & (C - 1)) == chan;
+                        const unsigned mm = __ballot_sync(kFull, mine);
+                        if (mine) my_ids[count + __popc(mm & ((1u << lane) - 1u))] = nb;
+                        count += __popc(mm);
                     }
                 }
-                nvalid += V;
                 __syncwarp();
+                int nvalid = 0;
+                for (int c0 = 0; c0 < count; c0 += 32) {
+                    const bool act = c0 + lane < count;
+                    const int nb = act ? my_ids[c0 + lane] : -1;
+                    const bool valid = bloom_chunk(bloom, bmask, P.seed, nb, act, lane);
+                    const unsigned vm = __ballot_sync(kFull, valid);
+                    // written at or below the chunk just read: the in-place compaction is safe
+                    if (valid) {
+                        my_ids[nvalid + __popc(vm & ((1u << lane) - 1u))] = nb;
+                        prefetch_l2(g.vecs + (int64_t)nb * g.vstride_bytes, vbytes);
+                    }
+                    nvalid += __popc(vm);
+                    __syncwarp();
+                }
+                visited += nvalid;
+                if (lane == 0) S->chan_valid[chan] = nvalid;
             }
-            if (lane == 0) S->chan_valid[warp] = nvalid;
+            __syncthreads();
+            // 2. the channel's warps: gathers and distances, batch b by warp b mod W
+            {
+                const int nvalid = S->chan_valid[chan];
+                const int step = BS * W;
+                int b0 = BS * sub;
+                uint4 raw[NB][VROWS];
+                float scale[NB];
+                if (b0 < nvalid) gather_batch<ELEM, VROWS, NB>(g, my_ids, b0, nvalid, nseg, lane, lg, raw, scale);
+                for (; b0 < nvalid; b0 += step) {
+                    const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane, lg);
+                    if (b0 + step < nvalid)
+                        gather_batch<ELEM, VROWS, NB>(g, my_ids, b0 + step, nvalid, nseg, lane, lg, raw, scale);
+                    if (rep_lane && b0 + my_slot < nvalid) my_d[b0 + my_slot] = dist;
+                }
+            }
             __syncthreads();
             // 3. warp 0 merges channels in order and runs the scheduler
             if (warp == 0) {
@@ -1127,25 +1358,26 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
                     const int o = c * lcap;
                     const int nv = S->chan_valid[c];
                     for (int j0 = 0; j0 < nv; j0 += 32) {
-                        const float dl = (j0 + lane < nv) ? list_d[o + j0 + lane] : kLarge;
-                        unsigned m = __ballot_sync(kFull, j0 + lane < nv && dl < rmax);
-                        while (m) {
-                            const int t = __ffs(m) - 1;
-                            m &= m - 1;
-                            const float dd = __shfl_sync(kFull, dl, t);
-                            if (dd < rmax) {
-                                const int id = list_id[o + j0 + t];
-                                if constexpr (HEAP) {
+                        const bool v = j0 + lane < nv;
+                        const float dl = v ? list_d[o + j0 + lane] : kLarge;
+                        if constexpr (HEAP) {
+                            unsigned m = __ballot_sync(kFull, v && dl < rmax);
+                            while (m) {
+                                const int t = __ffs(m) - 1;
+                                m &= m - 1;
+                                const float dd = __shfl_sync(kFull, dl, t);
+                                if (dd < rmax) {
+                                    const int id = list_id[o + j0 + t];
                                     rmax = bucket_replace_max<EPL>(BM, hkey, hid, heap_key(dd, ++age), id, lane);
-                                } else {
-                                    rl_insert<EPL>(rd, ri, lane, dd, id);
-                                    rmax = rl_get<EPL>(rd, P.ef - 1);
-                                }
-                                if (dd < cmax) {
-                                    cl_insert<CPL>(cd, ci, lane, P.cq, dd, id);
-                                    cmax = rl_get<CPL>(cd, P.cq - 1);
+                                    if (dd < cmax) {
+                                        cl_insert<CPL>(cd, ci, lane, P.cq, dd, id);
+                                        cmax = rl_get<CPL>(cd, P.cq - 1);
+                                    }
                                 }
                             }
+                        } else {
+                            const int idl = v ? list_id[o + j0 + lane] : -1;
+                            merge_window<EPL, CPL>(L, P.ef, P.cq, dl, idl, v, lane, rmax, cmax);
                         }
                     }
                 }
@@ -1159,10 +1391,16 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
                     if (slot >= mg) slot -= mg;
                     int n = 0;
                     for (int bb = 0; bb < mc; bb++) {
-                        const float best = __shfl_sync(kFull, cd[0], 0);
+                        float best;
+                        if constexpr (HEAP) best = __shfl_sync(kFull, cd[0], 0);
+                        else best = L.cd[0];
                         if (!(best <= thr && best < kLarge)) break;
                         if (P.max_hops > 0 && hops >= P.max_hops) { truncated = true; break; }
-                        const int pid = cl_pop<CPL>(cd, ci, lane, P.cq);
+                        int pid;
+                        if constexpr (HEAP) pid = cl_pop<CPL>(cd, ci, lane, P.cq);
+                        else pid = list_pop<CPL>(L.cd, L.ci, P.cq, lane);
+                        // the popped candidate's row is read as soon as its group is the oldest
+                        if (lane == n) prefetch_l2(g.links + (int64_t)pid * g.lstride, rbytes);
                         if (lane == 0) fifo[slot * mc + n] = pid;
                         n++;
                         hops++;
@@ -1171,7 +1409,8 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
                     if (lane == 0) fifo_len[slot] = n;
                     inflight++;
                 }
-                cmax = rl_get<CPL>(cd, P.cq - 1);
+                if constexpr (HEAP) cmax = rl_get<CPL>(cd, P.cq - 1);
+                else cmax = L.cd[P.cq - 1];
                 if (lane == 0) {
                     S->head = h;
                     S->inflight = inflight;
@@ -1181,7 +1420,7 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
             }
             __syncthreads();
         }
-        if (lane == 0) S->chan_visited[warp] = visited;
+        if (sub == 0 && lane == 0) S->chan_visited[chan] = visited;
         __syncthreads();
         if (warp == 0) {
             const int nwrite = A.write_all_ef ? P.ef : P.k;
@@ -1201,15 +1440,11 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
                 }
                 __syncwarp();
             } else {
-#pragma unroll
-                for (int e = 0; e < REPL; e++) {
-                    const int i = lane * EPL + e;
-                    if (i < nwrite) {
-                        int id = ri[e];
-                        if (!A.write_all_ef && g.labels && id >= 0) id = g.labels[id];
-                        oid_row[i] = id;
-                        od_row[i] = rd[e];
-                    }
+                for (int i = lane; i < nwrite; i += 32) {
+                    int id = L.ri[i];
+                    if (!A.write_all_ef && g.labels && id >= 0) id = g.labels[id];
+                    oid_row[i] = id;
+                    od_row[i] = L.rd[i];
                 }
             }
             for (int i = nwrite + lane; i < A.out_stride; i += 32) { oid_row[i] = -1; od_row[i] = kLarge; }
@@ -1225,15 +1460,15 @@ __global__ void __launch_bounds__(256) intra_kernel(const SearchLaunch A)
     }
 }
 
-size_t intra_smem_bytes(const SearchLaunch &a, int channels, int heap_cap)
+size_t intra_smem_bytes(const SearchLaunch &a, int channels, int heap_cap, int list_r, int list_c)
 {
     size_t b = (sizeof(IntraSmem) + 15) & ~(size_t)15;
     if (a.bloom_bits_max <= kMaxSmemBloomBits) b += ((size_t)1 << (a.bloom_bits_max - 3)) * channels;
     b += 2 * sizeof(int) * (size_t)a.mc_max * a.g.max_degree * channels;
     b += sizeof(int) * (size_t)(a.mc_max * a.mg_max + a.mg_max);
-    b += sizeof(int) * 32 * channels;
     b = (b + 15) & ~(size_t)15;
     b += (size_t)heap_cap * (sizeof(uint64_t) + sizeof(int));
+    b += (size_t)(list_r + list_c) * (sizeof(float) + sizeof(int));
     return (b + 15) & ~(size_t)15;
 }
 
@@ -1265,7 +1500,8 @@ __global__ void __launch_bounds__(128) descend_kernel(const DescendLaunch A)
     const bool rep_lane = (lane & gmask) < NB;
     const int my_slot = (lane >> lg) * NB + (lane & gmask);
     const int64_t nwarps = (int64_t)gridDim.x * 4;
-    for (int64_t qi = (int64_t)blockIdx.x * 4 + warp; qi < A.nq; qi += nwarps) {
+    for (int64_t qn = (int64_t)blockIdx.x * 4 + warp; qn < A.nq; qn += nwarps) {
+        const int64_t qi = A.rows ? (int64_t)A.rows[qn] : qn;   // the query's row
         float q[VROWS][4];
         const float *Q = A.queries + qi * A.qstride;
 #pragma unroll
@@ -1325,7 +1561,7 @@ __global__ void __launch_bounds__(128) descend_kernel(const DescendLaunch A)
         }
         if (lane == 0) {
             A.out_entry[qi * (A.out_entry_stride > 0 ? A.out_entry_stride : 1)] = cur;
-            if (A.out_hops) A.out_hops[qi] = hops;
+            if (A.out_hops) A.out_hops[qn] = hops;
         }
     }
 }
@@ -1422,10 +1658,11 @@ __global__ void __launch_bounds__(128) rerank_kernel(const RerankLaunch A)
 // per-entry done word (seq + 1) is released to the host.  Claiming uses
 // compare-and-swap so no request is ever claimed before it is published.
 // Every wait is bounded: a warp that finds no work sleeps and leaves after
-// `idle_ns` of idleness (or at once when `stop` is set), and every warp
-// leaves between requests once the host sets yield_epoch to this launch's
-// epoch (another class is waiting); the host relaunches a class kernel when
-// work is waiting.
+// its class has had no claim or completion for `idle_ns` (or at once when
+// `stop` is set), and every warp leaves between requests once the host sets
+// its class's yield_epoch to this launch's epoch (the host re-partitions the
+// SMs between the classes with work); the host relaunches a class kernel when
+// its class has work waiting.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ unsigned long long load_acquire_u64(const unsigned long long *p)
 {
@@ -1456,7 +1693,7 @@ __device__ __forceinline__ void serve_rerank(const ServeLaunch &S, int e, float 
         for (int w = 0; w < (int)(sizeof(ServeDesc) / sizeof(int)); w++) dst[w] = __ldcg(src + w);
     }
     const GraphView &v = S.views[D.index];
-    const int32_t *cand_ids = S.cand_ids + ((size_t)blockIdx.x * 4 + (threadIdx.x >> 5)) * S.ef_max;
+    const int32_t *cand_ids = S.cand_ids + ((size_t)S.warp_base + (size_t)blockIdx.x * 4 + (threadIdx.x >> 5)) * S.ef_max;
     const float *query = S.qpool + (int64_t)e * S.qstride;
     int32_t *orow = S.out_ids + (int64_t)e * S.out_stride;
     float *drow = S.out_d + (int64_t)e * S.out_stride;
@@ -1478,55 +1715,50 @@ __global__ void __launch_bounds__(128, 3) serve_kernel(const ServeLaunch S)
 {
     extern __shared__ uint4 smem_u4[];
     constexpr int CLS = serve_class(ELEM, VROWS);
-    constexpr int HEAP_CAP = (EPL > 8) ? 32 * EPL : 0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const size_t wbytes = serve_warp_smem_bytes(S.bloom_bits_max, S.mc_max, S.mg_max, HEAP_CAP, S.ef_max);
+    using Caps = ListCaps<EPL>;
+    const size_t wbytes =
+        serve_warp_smem_bytes(S.bloom_bits_max, S.mc_max, S.mg_max, Caps::heap, Caps::r, Caps::c, S.ef_max);
     unsigned char *wbase = reinterpret_cast<unsigned char *>(smem_u4) + wbytes * warp;
     const bool smem_bloom = S.bloom_bits_max <= kMaxSmemBloomBits;
     const size_t bloom_bytes = (size_t)1 << (S.bloom_bits_max - 3);
-    uint32_t *bloom = smem_bloom ? reinterpret_cast<uint32_t *>(wbase)
-                                 : S.bloom_global + ((size_t)blockIdx.x * 4 + warp) * (bloom_bytes / 4);
-    unsigned char *p = wbase + (smem_bloom ? bloom_bytes : 0);
-    uint64_t *hkey = reinterpret_cast<uint64_t *>(p);
-    p += sizeof(uint64_t) * HEAP_CAP;
-    int *hid = reinterpret_cast<int *>(p);
-    p += sizeof(int) * HEAP_CAP;
-    // rerank scratch: the heap's space once the traversal has written its results
-    float *rsd = HEAP_CAP ? reinterpret_cast<float *>(hkey) : reinterpret_cast<float *>(p);
-    int *rsi = HEAP_CAP ? reinterpret_cast<int *>(hkey) + S.ef_max : reinterpret_cast<int *>(p) + S.ef_max;
-    if (!HEAP_CAP) p += (sizeof(float) + sizeof(int)) * S.ef_max;
-    int *fifo = reinterpret_cast<int *>(p);
-    int *fifo_len = fifo + S.mc_max * S.mg_max;
-    int *sids = fifo_len + S.mg_max;
-    const size_t gw = (size_t)blockIdx.x * 4 + warp;
+    const size_t gw = (size_t)S.warp_base + (size_t)blockIdx.x * 4 + warp;   // this warp's scratch slot
+    uint32_t *gbloom = smem_bloom ? nullptr : S.bloom_global + gw * (bloom_bytes / 4);
+    const WarpSmem W = carve_warp_smem(wbase, gbloom, smem_bloom, bloom_bytes, Caps::heap, Caps::r, Caps::c, S.mc_max,
+                                       S.mg_max);
+    // rerank scratch: the bucketed list's space once the traversal has written
+    // its results, else ef_max slots after the warp's traversal state
+    float *rsd = Caps::heap ? reinterpret_cast<float *>(W.hkey)
+                            : reinterpret_cast<float *>(wbase + wbytes - serve_rerank_bytes(S.ef_max));
+    int *rsi = Caps::heap ? reinterpret_cast<int *>(W.hkey) + S.ef_max : reinterpret_cast<int *>(rsd + S.ef_max);
     int32_t *cand_ids = S.cand_ids + gw * S.ef_max;
     float *cand_d = S.cand_d + gw * S.ef_max;
     const int32_t *slots = S.class_slots + (size_t)CLS * S.ring_cap;
     uint32_t epoch = 0;
-    if (lane == 0) epoch = *reinterpret_cast<const volatile uint32_t *>(S.run_epoch);
+    if (lane == 0) epoch = reinterpret_cast<const volatile uint32_t *>(S.run_epoch)[CLS];
 
     for (;;) {
         unsigned long long h = ~0ull;
         int yielded = 0;
         if (lane == 0) {
             // the host hands the GPU to another class: leave between requests
-            yielded = *reinterpret_cast<volatile uint32_t *>(&S.ctl->yield_epoch) == epoch;
+            yielded = *reinterpret_cast<volatile uint32_t *>(&S.ctl->yield_epoch[CLS]) == epoch;
             for (int tries = 0; !yielded && tries < 256; tries++) {
                 const unsigned long long hd = atomicAdd(&S.ctl->head[CLS], 0ull);
                 const unsigned long long tl = load_acquire_u64(&S.ctl->tail[CLS]);
                 if (hd >= tl) break;
                 if (atomicCAS(&S.ctl->head[CLS], hd, hd + 1) == hd) { h = hd; break; }
             }
-            if (h != ~0ull) atomicMax(&S.ctl->last_active_ns, global_ns());
+            if (h != ~0ull) atomicMax(&S.ctl->last_active_ns[CLS], global_ns());
         }
         if (__shfl_sync(kFull, yielded, 0)) break;
         h = __shfl_sync(kFull, h, 0);
         if (h == ~0ull) {
-            // leave only when the whole server has been idle for idle_ns
+            // leave only when this class has been idle for idle_ns
             int leave = 0;
             if (lane == 0) {
                 const int stop = *reinterpret_cast<volatile int *>(&S.ctl->stop);
-                const long long last = *reinterpret_cast<volatile long long *>(&S.ctl->last_active_ns);
+                const long long last = *reinterpret_cast<volatile long long *>(&S.ctl->last_active_ns[CLS]);
                 leave = stop || (global_ns() - last > S.idle_ns);
             }
             if (__shfl_sync(kFull, leave, 0)) break;
@@ -1553,8 +1785,8 @@ __global__ void __launch_bounds__(128, 3) serve_kernel(const ServeLaunch S)
         io.hops = S.out_hops + e;
         io.visited = S.out_visited + e;
         io.status = S.status;
-        search_one_inter<ELEM, EPL, VROWS, kRowBloom<ELEM, VROWS>>(v, D.p, io, bloom, fifo, fifo_len, sids, hkey, hid,
-                                                                   lane);
+        search_one_inter<ELEM, EPL, VROWS, kRowBloom<ELEM, VROWS>>(v, D.p, io, W.bloom, W.fifo, W.fifo_len, W.sids,
+                                                                   W.hkey, W.hid, lane);
         if constexpr (ELEM != kF32) {
             if (rerank) {
                 __syncwarp();
@@ -1565,7 +1797,7 @@ __global__ void __launch_bounds__(128, 3) serve_kernel(const ServeLaunch S)
         if (lane == 0) {
             __threadfence_system();
             *reinterpret_cast<volatile unsigned long long *>(S.done + e) = D.seq + 1;
-            atomicMax(&S.ctl->last_active_ns, global_ns());
+            atomicMax(&S.ctl->last_active_ns[CLS], global_ns());
         }
         __syncwarp();
     }
@@ -1613,7 +1845,8 @@ cudaError_t launch_inter(const SearchLaunch &a, size_t, int num_sms, cudaStream_
     constexpr bool kTrace = (ELEM == kF32);
     auto kern = (kTrace && a.trace_counts) ? inter_kernel<ELEM, EPL, VROWS, kTrace> : inter_kernel<ELEM, EPL, VROWS, false>;
     if (a.trace_counts && !kTrace) return cudaErrorInvalidValue;
-    const size_t smem_block = warp_smem_bytes(a.bloom_bits_max, a.mc_max, a.mg_max, (EPL > 8) ? 32 * EPL : 0) * 4;
+    using Caps = ListCaps<EPL>;
+    const size_t smem_block = warp_smem_bytes(a.bloom_bits_max, a.mc_max, a.mg_max, Caps::heap, Caps::r, Caps::c) * 4;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_block);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -1636,11 +1869,17 @@ template <int ELEM, int EPL, int VROWS>
 cudaError_t launch_intra(const SearchLaunch &a, int channels, int num_sms, cudaStream_t s, int64_t *slots)
 {
     auto kern = intra_kernel<ELEM, EPL, VROWS>;
-    const size_t smem = intra_smem_bytes(a, channels, (EPL > 8) ? 32 * EPL : 0);
+    using Caps = ListCaps<EPL, true>;
+    const size_t smem = intra_smem_bytes(a, channels, Caps::heap, Caps::r, Caps::c);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    const int threads = 32 * channels;
+    // warps per channel: a batch smaller than the SMs gets up to 16 warps per
+    // query (latency), a larger one a warp per channel (throughput)
+    int wpc = 1;
+    if (a.nq <= num_sms) wpc = kIntraMaxWarps / channels;
+    if (wpc < 1) wpc = 1;
+    const int threads = 32 * channels * wpc;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
@@ -1750,7 +1989,9 @@ template <int ELEM, int EPL, int VROWS>
 static cudaError_t serve_config_t(const ServeLaunch &sv, int num_sms, int *grid, size_t *smem)
 {
     const int heap_cap = (EPL > 8) ? 32 * EPL : 0;
-    *smem = serve_warp_smem_bytes(sv.bloom_bits_max, sv.mc_max, sv.mg_max, heap_cap, sv.ef_max) * 4;
+    using Caps = ListCaps<EPL>;
+    (void)heap_cap;
+    *smem = serve_warp_smem_bytes(sv.bloom_bits_max, sv.mc_max, sv.mg_max, Caps::heap, Caps::r, Caps::c, sv.ef_max) * 4;
     cudaError_t e = cudaFuncSetAttribute(serve_kernel<ELEM, EPL, VROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)*smem);
     int per_sm = 0;

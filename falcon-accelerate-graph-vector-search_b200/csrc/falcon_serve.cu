@@ -5,24 +5,36 @@
 // copied on a copy stream) and each ring entry to the claim queue of its
 // class (traversal precision x register rows, falcon_internal.h), then
 // publishes the queues' tail counters.  A persistent serve_kernel
-// (falcon_kernels.cu) specialised for one class, its launch captured once in
-// a CUDA graph, pulls that class's requests one at a time, so a request
-// admitted while others are on the GPU starts as soon as a warp frees up and
-// its work overlaps theirs.  Each request carries its own index, precision,
-// k, ef, mc, mg (mixed freely).  One class kernel runs at a time; while
-// another class has requests waiting, the running kernel is asked to yield
-// (its warps leave between requests) once its class has nothing uncollected
-// or it has run for kClassSliceUs, and the next class with work (round
-// robin) is launched.  Requests to an index with HNSW upper layers get their
-// entry from the descent kernel, launched at submit on the copy stream over
-// the new queries and writing into the ring descriptors before the tails
-// are published; the class kernels leave block slots free for it.
-// Results go to host-mapped memory and complete with a per-entry done word,
-// so the host collects them without any CUDA call.  The ring's size is
-// chosen from the free device memory at creation (admission by memory): a
+// (falcon_kernels.cu) specialised for one class pulls that class's requests
+// one at a time, so a request admitted while others are on the GPU starts as
+// soon as a warp frees up and its work overlaps theirs.  Each request carries
+// its own index, precision, k, ef, mc, mg (mixed freely).
+//
+// The kernels of all classes with work run at the same time, each on its own
+// stream: with P classes wanting the GPU, each launch gets 1/P of the blocks
+// and its own range of per-warp scratch slots (Bloom filters, rerank
+// candidates).  Each (class, P, range) launch is captured in a CUDA graph the
+// first time it is needed and replayed afterwards.  When another class gets
+// work, a running launch whose share is now too large is asked to yield (its
+// warps leave between requests) and is relaunched with the smaller share; a
+// launch with a smaller share than the current one keeps running until its
+// class idles out, so a load that comes and goes does not relaunch kernels.
+// A class kernel leaves after `idle_exit_us` without a claim or completion of
+// its class and is relaunched by the next submit or poll, so an idle server
+// holds no SMs.
+//
+// Requests to an index with HNSW upper layers get their entry from the
+// descent kernel, launched at submit on the copy stream over the new queries
+// and writing into the ring descriptors before the tails are published; the
+// class kernels leave block slots free for it.  Results go to host-mapped
+// memory and complete with a per-entry done word, so the host collects them
+// without any CUDA call.
+//
+// Admission by memory: the ring is sized from the free device memory at
+// creation, and each submit admits requests only while the requests in
+// flight stay within memory_fraction of the device memory that is free
+// (re-read at most every kMemCheckUs) plus what the server already holds; a
 // request is refused (not queued) while its ring entry is still in use.
-// The kernel leaves after `idle_exit_us` without work and is relaunched by the
-// next submit or poll, so an idle server holds no SMs.
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -56,15 +68,21 @@ struct falcon_server {
     int cap = 0;                          // ring entries
     int qstride = 0;                      // floats per query slot
     std::mutex mu;
-    cudaStream_t kstream = nullptr, cstream = nullptr;
-    cudaGraphExec_t graph[kServeClasses] = {};
-    cudaEvent_t kernel_done = nullptr;
-    bool launched = false;
+    cudaStream_t cstream = nullptr;
+    cudaStream_t ystream = nullptr;       // yield requests: never queued behind a submit's descent
+    cudaStream_t kstream[kServeClasses] = {};
+    cudaEvent_t kernel_done[kServeClasses] = {};
+    // graph[c][P-1][r]: class c's launch over 1/P of the blocks, scratch range r
+    cudaGraphExec_t graph[kServeClasses][4][4] = {};
+    bool launched[kServeClasses] = {};
+    int run_parts[kServeClasses] = {};    // share of the running launch (1/P)
+    int run_range[kServeClasses] = {};    // its scratch range (0 .. P-1)
+    uint32_t epoch[kServeClasses] = {};   // launches of the class so far; the running launch's epoch
+    bool yield_sent[kServeClasses] = {};
     int64_t launches = 0;
-    int run_cls = kServeClasses - 1;      // class of the current (or last) launch
-    uint32_t epoch = 0;                   // launches so far; the current launch's epoch
-    bool yield_sent = false;
-    std::chrono::steady_clock::time_point run_t0;
+    int64_t concurrent_max = 0;           // most class kernels running at once
+    int64_t mem_cap = 0;                  // requests in flight admitted by memory
+    std::chrono::steady_clock::time_point mem_t;   // last free-memory reading
     // device
     GraphView *d_views = nullptr;
     ServeDesc *d_ring = nullptr;
@@ -79,9 +97,12 @@ struct falcon_server {
     ServeDesc *h_desc = nullptr;
     float *h_qstage = nullptr;
     int32_t *h_class_slots = nullptr;
+    int32_t *h_desc_rows = nullptr;             // pinned staging of the ring entries a descent covers
+    int32_t *d_desc_rows = nullptr;
+    int64_t desc_rows_used = 0;
     unsigned long long *h_tail = nullptr;       // kServeClasses pinned values per ring entry (async copy source)
-    uint32_t *h_run_epoch = nullptr;            // host-mapped: read by each launch at start
-    uint32_t *h_yield = nullptr;                // pinned sources of yield copies, one per launch mod 16
+    uint32_t *h_run_epoch = nullptr;            // host-mapped, per class: read by each launch at start
+    uint32_t *h_yield = nullptr;                // pinned sources of yield copies: per class, one per launch mod 16
     int32_t *h_out_ids = nullptr;
     float *h_out_d = nullptr;
     int32_t *h_hops = nullptr, *h_vis = nullptr;
@@ -115,11 +136,15 @@ int cuda_fail(cudaError_t e, const char *what)
 
 void free_server(falcon_server *sv)
 {
-    for (int c = 0; c < kServeClasses; c++)
-        if (sv->graph[c]) cudaGraphExecDestroy(sv->graph[c]);
-    if (sv->kernel_done) cudaEventDestroy(sv->kernel_done);
-    if (sv->kstream) cudaStreamDestroy(sv->kstream);
+    for (int c = 0; c < kServeClasses; c++) {
+        for (int p = 0; p < 4; p++)
+            for (int r = 0; r < 4; r++)
+                if (sv->graph[c][p][r]) cudaGraphExecDestroy(sv->graph[c][p][r]);
+        if (sv->kernel_done[c]) cudaEventDestroy(sv->kernel_done[c]);
+        if (sv->kstream[c]) cudaStreamDestroy(sv->kstream[c]);
+    }
     if (sv->cstream) cudaStreamDestroy(sv->cstream);
+    if (sv->ystream) cudaStreamDestroy(sv->ystream);
     cudaFree(sv->d_views);
     cudaFree(sv->d_ring);
     cudaFree(sv->d_class_slots);
@@ -133,6 +158,8 @@ void free_server(falcon_server *sv)
     cudaFreeHost(sv->h_qstage);
     cudaFreeHost(sv->h_tail);
     cudaFreeHost(sv->h_class_slots);
+    cudaFreeHost(sv->h_desc_rows);
+    cudaFree(sv->d_desc_rows);
     cudaFreeHost(sv->h_run_epoch);
     cudaFreeHost(sv->h_yield);
     cudaFreeHost(sv->h_out_ids);
@@ -143,12 +170,12 @@ void free_server(falcon_server *sv)
     delete sv;
 }
 
-// A class kernel that has run this long yields to another class with
-// requests waiting.
-constexpr double kClassSliceUs = 20000.0;
-
 // Block slots the serve kernels leave free for the submit-time descent.
-constexpr int kDescendSlots = 2;
+constexpr int kDescendSlots = 8;
+// Most classes sharing the SMs at once (more wait for a share to free up).
+constexpr int kMaxParts = 4;
+// Free device memory is re-read at most this often by submit.
+constexpr double kMemCheckUs = 1000.0;
 
 // Whether class c has a request that is neither collected nor done: with no
 // kernel running, exactly the requests still to be claimed.  Walks the
@@ -168,50 +195,127 @@ bool class_pending(const falcon_server *sv, int c)
     return false;
 }
 
-// Keep a class kernel running while any class has requests to claim:
-// relaunch after an idle exit, switch classes round robin, and ask the
-// running kernel to yield when another class waits (see the file comment).
-// Caller holds mu.
+// Per-warp scratch slots [lo, hi) of a launch over 1/parts of the blocks in range r.
+void scratch_range(const falcon_server *sv, int parts, int r, int *lo, int *hi)
+{
+    const int w = sv->max_grid * 4 / parts;
+    *lo = r * w;
+    *hi = *lo + w;
+}
+
+// The graph of class c's launch over 1/parts of its blocks in scratch range
+// r, captured on first use.  Caller holds mu.
+cudaError_t class_graph(falcon_server *sv, int c, int parts, int r, cudaGraphExec_t *out)
+{
+    cudaGraphExec_t &ge = sv->graph[c][parts - 1][r];
+    if (!ge) {
+        ServeLaunch L = sv->launch;
+        int lo, hi;
+        scratch_range(sv, parts, r, &lo, &hi);
+        L.warp_base = lo;
+        int grid = sv->grid[c] / parts;
+        if (grid < 1) grid = 1;
+        if (grid * 4 > hi - lo) grid = (hi - lo) / 4;
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(sv->kstream[c], cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return e;
+        e = launch_serve(L, sv->epl, c, grid, sv->smem[c], sv->kstream[c]);
+        const cudaError_t e2 = cudaStreamEndCapture(sv->kstream[c], &g);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&ge, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            ge = nullptr;
+            return e;
+        }
+    }
+    *out = ge;
+    return cudaSuccess;
+}
+
+// Keep a kernel running for every class with requests to claim, the classes
+// sharing the SMs (see the file comment).  Caller holds mu.
 int ensure_running(falcon_server *sv)
 {
-    if (sv->launched) {
-        const cudaError_t q = cudaEventQuery(sv->kernel_done);
-        if (q == cudaErrorNotReady) {
-            if (!sv->yield_sent) {
-                bool other = false;
-                for (int c = 0; c < kServeClasses; c++) other |= (c != sv->run_cls && sv->unfinished[c] > 0);
-                const double ran = std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() -
-                                                                             sv->run_t0).count();
-                if (other && (sv->unfinished[sv->run_cls] == 0 || ran >= kClassSliceUs)) {
-                    uint32_t *src = sv->h_yield + (sv->epoch % 16);
-                    *src = sv->epoch;
-                    const cudaError_t e = cudaMemcpyAsync(&sv->d_ctl->yield_epoch, src, sizeof(uint32_t),
-                                                          cudaMemcpyHostToDevice, sv->cstream);
-                    if (e != cudaSuccess) return cuda_fail(e, "serve yield");
-                    sv->yield_sent = true;
-                }
-            }
-            return FALCON_OK;
+    bool want[kServeClasses];
+    int nwant = 0;
+    for (int c = 0; c < kServeClasses; c++) {
+        if (sv->launched[c]) {
+            const cudaError_t q = cudaEventQuery(sv->kernel_done[c]);
+            if (q == cudaSuccess) sv->launched[c] = false;
+            else if (q != cudaErrorNotReady) return cuda_fail(q, "serve kernel");
         }
-        if (q != cudaSuccess) return cuda_fail(q, "serve kernel");
-        sv->launched = false;
+        want[c] = sv->launched[c] || (sv->unfinished[c] > 0 && class_pending(sv, c));
+        nwant += want[c] ? 1 : 0;
     }
-    int cls = -1;
-    for (int i = 1; i <= kServeClasses && cls < 0; i++) {
-        const int c = (sv->run_cls + i) % kServeClasses;
-        if (sv->unfinished[c] > 0 && class_pending(sv, c)) cls = c;
+    if (nwant == 0) return FALCON_OK;
+    const int parts = nwant < kMaxParts ? nwant : kMaxParts;
+    // a running launch with a larger share than `parts` makes room
+    for (int c = 0; c < kServeClasses; c++) {
+        if (!sv->launched[c] || sv->yield_sent[c] || sv->run_parts[c] >= parts) continue;
+        uint32_t *src = sv->h_yield + c * 16 + (sv->epoch[c] % 16);
+        *src = sv->epoch[c];
+        const cudaError_t e = cudaMemcpyAsync(&sv->d_ctl->yield_epoch[c], src, sizeof(uint32_t),
+                                              cudaMemcpyHostToDevice, sv->ystream);
+        if (e != cudaSuccess) return cuda_fail(e, "serve yield");
+        sv->yield_sent[c] = true;
     }
-    if (cls < 0) return FALCON_OK;
-    *sv->h_run_epoch = ++sv->epoch;
-    cudaError_t e = cudaGraphLaunch(sv->graph[cls], sv->kstream);
-    if (e == cudaSuccess) e = cudaEventRecord(sv->kernel_done, sv->kstream);
-    if (e != cudaSuccess) return cuda_fail(e, "serve kernel launch");
-    sv->launched = true;
-    sv->launches++;
-    sv->run_cls = cls;
-    sv->yield_sent = false;
-    sv->run_t0 = std::chrono::steady_clock::now();
+    // launch the classes that want the GPU into a free scratch range
+    for (int c = 0; c < kServeClasses; c++) {
+        if (!want[c] || sv->launched[c]) continue;
+        int range = -1;
+        for (int r = 0; r < parts && range < 0; r++) {
+            int lo, hi;
+            scratch_range(sv, parts, r, &lo, &hi);
+            bool free_r = true;
+            for (int o = 0; o < kServeClasses && free_r; o++) {
+                if (!sv->launched[o]) continue;
+                int olo, ohi;
+                scratch_range(sv, sv->run_parts[o], sv->run_range[o], &olo, &ohi);
+                free_r = ohi <= lo || hi <= olo;
+            }
+            if (free_r) range = r;
+        }
+        if (range < 0) continue;   // a yielding launch still holds the range: next pass
+        cudaGraphExec_t ge;
+        cudaError_t e = class_graph(sv, c, parts, range, &ge);
+        if (e != cudaSuccess) return cuda_fail(e, "serve graph");
+        sv->h_run_epoch[c] = ++sv->epoch[c];
+        e = cudaGraphLaunch(ge, sv->kstream[c]);
+        if (e == cudaSuccess) e = cudaEventRecord(sv->kernel_done[c], sv->kstream[c]);
+        if (e != cudaSuccess) return cuda_fail(e, "serve kernel launch");
+        sv->launched[c] = true;
+        sv->run_parts[c] = parts;
+        sv->run_range[c] = range;
+        sv->yield_sent[c] = false;
+        sv->launches++;
+    }
+    int64_t running = 0;
+    for (int c = 0; c < kServeClasses; c++) running += sv->launched[c] ? 1 : 0;
+    if (running > sv->concurrent_max) sv->concurrent_max = running;
     return FALCON_OK;
+}
+
+// Requests in flight the free device memory allows (re-read at most every
+// kMemCheckUs): memory_fraction of (free memory + the server's own), at
+// most the ring.  Caller holds mu.
+int64_t memory_admission_cap(falcon_server *sv)
+{
+    const auto now = std::chrono::steady_clock::now();
+    if (sv->mem_cap == 0 ||
+        std::chrono::duration<double, std::micro>(now - sv->mem_t).count() >= kMemCheckUs) {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+            const double per = (double)(sizeof(float) * sv->qstride + sizeof(ServeDesc));
+            const double budget = sv->cfg.memory_fraction * ((double)free_b + (double)sv->device_bytes);
+            int64_t cap = (int64_t)(budget / per);
+            sv->mem_cap = cap < sv->cap ? (cap < 1 ? 1 : cap) : sv->cap;
+        } else if (sv->mem_cap == 0) {
+            sv->mem_cap = sv->cap;
+        }
+        sv->mem_t = now;
+    }
+    return sv->mem_cap;
 }
 
 }  // namespace
@@ -302,9 +406,12 @@ int falcon_server_create(const falcon_server_config *c, falcon_server **out)
         free_server(sv);                          \
         return cuda_fail(e, what);                \
     }
-    SV_ALLOC(cudaStreamCreateWithFlags(&sv->kstream, cudaStreamNonBlocking), "stream");
+    for (int c = 0; c < kServeClasses; c++) {
+        SV_ALLOC(cudaStreamCreateWithFlags(&sv->kstream[c], cudaStreamNonBlocking), "stream");
+        SV_ALLOC(cudaEventCreateWithFlags(&sv->kernel_done[c], cudaEventDisableTiming), "event");
+    }
     SV_ALLOC(cudaStreamCreateWithFlags(&sv->cstream, cudaStreamNonBlocking), "stream");
-    SV_ALLOC(cudaEventCreateWithFlags(&sv->kernel_done, cudaEventDisableTiming), "event");
+    SV_ALLOC(cudaStreamCreateWithFlags(&sv->ystream, cudaStreamNonBlocking), "stream");
     SV_ALLOC(cudaMalloc(&sv->d_views, sizeof(GraphView) * 48), "views");
     SV_ALLOC(cudaMalloc(&sv->d_ring, sizeof(ServeDesc) * sv->cap), "ring");
     SV_ALLOC(cudaMalloc(&sv->d_class_slots, sizeof(int32_t) * kServeClasses * (size_t)sv->cap), "class queues");
@@ -323,9 +430,14 @@ int falcon_server_create(const falcon_server_config *c, falcon_server **out)
              "pinned");
     SV_ALLOC(cudaHostAlloc(&sv->h_class_slots, sizeof(int32_t) * kServeClasses * (size_t)sv->cap, cudaHostAllocDefault),
              "pinned");
-    SV_ALLOC(cudaHostAlloc(&sv->h_run_epoch, sizeof(uint32_t), cudaHostAllocMapped), "mapped");
-    SV_ALLOC(cudaHostAlloc(&sv->h_yield, sizeof(uint32_t) * 16, cudaHostAllocDefault), "pinned");
-    *sv->h_run_epoch = 0;
+    // descent row lists: twice the ring, so a list copied on the copy stream is
+    // not overwritten before that stream has read it (a submit admits at most
+    // the ring's free entries)
+    SV_ALLOC(cudaHostAlloc(&sv->h_desc_rows, sizeof(int32_t) * 2 * (size_t)sv->cap, cudaHostAllocDefault), "pinned");
+    SV_ALLOC(cudaMalloc(&sv->d_desc_rows, sizeof(int32_t) * 2 * (size_t)sv->cap), "descent rows");
+    SV_ALLOC(cudaHostAlloc(&sv->h_run_epoch, sizeof(uint32_t) * kServeClasses, cudaHostAllocMapped), "mapped");
+    SV_ALLOC(cudaHostAlloc(&sv->h_yield, sizeof(uint32_t) * 16 * kServeClasses, cudaHostAllocDefault), "pinned");
+    memset(sv->h_run_epoch, 0, sizeof(uint32_t) * kServeClasses);
     SV_ALLOC(cudaHostAlloc(&sv->h_out_ids, sizeof(int32_t) * (size_t)c->max_k * sv->cap, cudaHostAllocMapped), "mapped");
     SV_ALLOC(cudaHostAlloc(&sv->h_out_d, sizeof(float) * (size_t)c->max_k * sv->cap, cudaHostAllocMapped), "mapped");
     SV_ALLOC(cudaHostAlloc(&sv->h_hops, sizeof(int32_t) * sv->cap, cudaHostAllocMapped), "mapped");
@@ -358,18 +470,8 @@ int falcon_server_create(const falcon_server_config *c, falcon_server **out)
     L.bloom_global = sv->d_bloom;
     L.cand_ids = sv->d_cand_ids;
     L.cand_d = sv->d_cand_d;
-    // capture each class's persistent launch once; every (re)start replays its graph
-    for (int c = 0; c < kServeClasses; c++) {
-        if (!sv->class_ok[c]) continue;
-        cudaGraph_t g = nullptr;
-        SV_ALLOC(cudaStreamBeginCapture(sv->kstream, cudaStreamCaptureModeThreadLocal), "capture");
-        e = launch_serve(L, sv->epl, c, sv->grid[c], sv->smem[c], sv->kstream);
-        cudaError_t e2 = cudaStreamEndCapture(sv->kstream, &g);
-        if (e == cudaSuccess) e = e2;
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&sv->graph[c], g, 0);
-        if (g) cudaGraphDestroy(g);
-        if (e != cudaSuccess) { free_server(sv); return cuda_fail(e, "serve graph"); }
-    }
+    L.warp_base = 0;
+    // each (class, share, scratch range) launch is captured on first use (class_graph)
 #undef SV_ALLOC
     sv->entry_seq.assign(sv->cap, ~0ull);
     sv->entry_k.assign(sv->cap, 0);
@@ -389,6 +491,10 @@ int falcon_server_add_index(falcon_server *sv, falcon_index *ix, int32_t *index_
     int rc = index_graph_view(ix, FALCON_PREC_F32, &v, &dim, &entry);
     if (rc != FALCON_OK) return rc;
     if (dim > sv->cfg.dim_max) return set_error_code(FALCON_ERR_ARG, "index dimension above the server's dim_max");
+    DescendLaunch dl;
+    bool has_f32 = false;
+    const bool upper = index_descend_launch(ix, &dl, &has_f32);
+    if (upper && !has_f32) return set_error_code(FALCON_ERR_UNSUPPORTED, "the upper-layer descent needs FP32 storage");
     const int id = (int)sv->indexes.size();
     // one device view per precision the index holds: slot id*3 + precision
     GraphView views[3];
@@ -398,13 +504,10 @@ int falcon_server_add_index(falcon_server *sv, falcon_index *ix, int32_t *index_
     }
     cudaError_t e = cudaMemcpy(sv->d_views + 3 * id, views, sizeof(views), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(e, "register index");
+    // nothing below can fail: the index is registered in one step
     sv->indexes.push_back(ix);
     index_server_ref(ix, +1);
     sv->index_dim.push_back(dim);
-    DescendLaunch dl;
-    bool has_f32 = false;
-    const bool upper = index_descend_launch(ix, &dl, &has_f32);
-    if (upper && !has_f32) return set_error_code(FALCON_ERR_UNSUPPORTED, "the upper-layer descent needs FP32 storage");
     sv->index_entry.push_back(upper ? -1 : entry);
     sv->index_upper.push_back(upper ? 1 : 0);
     sv->index_dl.push_back(dl);
@@ -439,12 +542,16 @@ int falcon_server_submit(falcon_server *sv, int32_t n, const int32_t *index_ids,
         if (cls < 0 || cls >= kServeClasses || !sv->class_ok[cls])
             return set_error_code(FALCON_ERR_ARG, "request class not built for this server's dim_max");
     }
-    // then admit in order while ring entries are free
+    // then admit in order while ring entries are free and the free device
+    // memory allows more requests in flight
     int admitted = 0;
     const unsigned long long first = sv->next_seq;
     unsigned long long ctail0[kServeClasses];
+    int64_t unfinished0[kServeClasses];
     memcpy(ctail0, sv->ctail, sizeof(ctail0));
-    for (int i = 0; i < n; i++) {
+    memcpy(unfinished0, sv->unfinished, sizeof(unfinished0));
+    const int64_t room = memory_admission_cap(sv) - sv->in_flight;
+    for (int i = 0; i < n && i < room; i++) {
         const int idx = index_ids[i];
         const falcon_search_params &p = params[per_request_params ? i : 0];
         const int ef = p.ef < p.k ? p.k : p.ef;
@@ -499,24 +606,28 @@ int falcon_server_submit(falcon_server *sv, int32_t n, const int32_t *index_ids,
     }
     // entries of requests to indexes with upper layers: the greedy descent of
     // their queries, written into the ring descriptors before the tails are
-    // published (same stream), one launch per run of consecutive entries of one
-    // index (a run ends at the ring's wrap)
-    for (int i = 0; i < admitted && err == cudaSuccess;) {
-        const int idx = index_ids[i];
-        const int es = (int)((first + (unsigned long long)i) % (unsigned long long)sv->cap);
-        int j = i + 1;
-        while (j < admitted && index_ids[j] == idx && es + (j - i) < sv->cap) j++;
-        if (sv->index_upper[idx]) {
-            DescendLaunch dl = sv->index_dl[idx];
-            dl.queries = sv->d_qpool + (size_t)es * sv->qstride;
-            dl.qstride = sv->qstride;
-            dl.nq = j - i;
-            dl.out_entry = &sv->d_ring[es].entry;
-            dl.out_entry_stride = (int64_t)(sizeof(ServeDesc) / sizeof(int32_t));
-            dl.out_hops = nullptr;
-            err = launch_descend(dl, sv->num_sms, sv->cstream);
-        }
-        i = j;
+    // published (same stream); one launch per such index over the list of its
+    // new ring entries, wherever they lie in the ring
+    for (int idx = 0; idx < (int)sv->indexes.size() && err == cudaSuccess; idx++) {
+        if (!sv->index_upper[idx]) continue;
+        int cnt = 0;
+        int32_t *lst = sv->h_desc_rows + (size_t)sv->desc_rows_used;
+        for (int i = 0; i < admitted; i++)
+            if (index_ids[i] == idx) lst[cnt++] = (int32_t)((first + (unsigned long long)i) % (unsigned long long)sv->cap);
+        if (cnt == 0) continue;
+        int32_t *dlst = sv->d_desc_rows + (size_t)sv->desc_rows_used;
+        sv->desc_rows_used = (sv->desc_rows_used + cnt) % sv->cap;   // the staging area is reused round robin
+        err = cudaMemcpyAsync(dlst, lst, sizeof(int32_t) * cnt, cudaMemcpyHostToDevice, sv->cstream);
+        if (err != cudaSuccess) break;
+        DescendLaunch dl = sv->index_dl[idx];
+        dl.queries = sv->d_qpool;
+        dl.qstride = sv->qstride;
+        dl.nq = cnt;
+        dl.rows = dlst;
+        dl.out_entry = &sv->d_ring[0].entry;
+        dl.out_entry_stride = (int64_t)(sizeof(ServeDesc) / sizeof(int32_t));
+        dl.out_hops = nullptr;
+        err = launch_descend(dl, sv->num_sms, sv->cstream);
     }
     // each class queue's new slots (at most two contiguous ranges), then all tails in one copy
     for (int c = 0; c < kServeClasses && err == cudaSuccess; c++) {
@@ -537,7 +648,14 @@ int falcon_server_submit(falcon_server *sv, int32_t n, const int32_t *index_ids,
     if (err == cudaSuccess)
         err = cudaMemcpyAsync(sv->d_ctl->tail, tails, sizeof(unsigned long long) * kServeClasses,
                               cudaMemcpyHostToDevice, sv->cstream);
-    if (err != cudaSuccess) return cuda_fail(err, "publish requests");
+    if (err != cudaSuccess) {
+        // nothing was published (the tails go last): take the admissions back,
+        // so the next submit reuses the same entries and sequence numbers
+        for (int i = 0; i < admitted; i++) sv->entry_seq[(first + (unsigned long long)i) % (unsigned long long)sv->cap] = ~0ull;
+        memcpy(sv->ctail, ctail0, sizeof(ctail0));
+        memcpy(sv->unfinished, unfinished0, sizeof(unfinished0));
+        return cuda_fail(err, "publish requests");
+    }
     sv->next_seq = tail;
     sv->in_flight += admitted;
     const int rc = ensure_running(sv);
@@ -689,6 +807,7 @@ int falcon_server_info_get(falcon_server *sv, falcon_server_info *info)
     info->kernel_launches = sv->launches;
     info->warps = sv->max_grid * 4;
     info->device_bytes = sv->device_bytes;
+    info->concurrent_classes_max = sv->concurrent_max;
     return FALCON_OK;
 }
 
@@ -702,7 +821,8 @@ int falcon_server_free(falcon_server *sv)
         cudaMemcpy(&sv->d_ctl->stop, &stop, sizeof(stop), cudaMemcpyHostToDevice);
     }
     cudaStreamSynchronize(sv->cstream);
-    cudaStreamSynchronize(sv->kstream);
+    cudaStreamSynchronize(sv->ystream);
+    for (int c = 0; c < kServeClasses; c++) cudaStreamSynchronize(sv->kstream[c]);
     for (const falcon_index *ix : sv->indexes) index_server_ref(const_cast<falcon_index *>(ix), -1);
     free_server(sv);
     return FALCON_OK;

@@ -109,7 +109,8 @@ class ServerConfig(ctypes.Structure):
 
 class ServerInfo(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in
-                ("ring_entries", "in_flight", "submitted", "kernel_launches", "warps", "device_bytes")]
+                ("ring_entries", "in_flight", "submitted", "kernel_launches", "warps", "device_bytes",
+                 "concurrent_classes_max")]
 
 
 # Every symbol include/falcon.h declares, with its ctypes signature.

@@ -36,7 +36,26 @@ class FalconServer:
             setattr(c, k, v)
         h = ctypes.c_void_p()
         _lib.check(lib.falcon_server_create(ctypes.byref(c), ctypes.byref(h)))
-        self._h, self.cfg, self._indexes = h, c, []
+        self._h, self.cfg, self._indexes, self._profile = h, c, [], None
+
+    def set_profile(self, profile):
+        """An autotuner profile (falcon_b200.autotune) that auto_params reads."""
+        self._profile = profile
+
+    def auto_params(self, index_id, k, ef, **overrides):
+        """Request parameters for an index from the autotuner's profile: the
+        candidate queue, (mc, mg) and Bloom size of the throughput entry for
+        the index's (dimension, max degree) at or above `ef` (autotune.pick;
+        the server runs inter-query requests), with the requested k and ef and
+        `overrides` applied."""
+        from .autotune import pick
+        if self._profile is None:
+            raise ValueError("no autotuner profile: call set_profile first")
+        inf = self._indexes[index_id].info()
+        p = pick(self._profile, inf.dim, inf.max_degree, ef, "throughput")
+        p.update(k=k, ef=max(ef, k), mode="inter")
+        p.update(overrides)
+        return make_params(**p)
 
     def add_index(self, index):
         iid = ctypes.c_int32()

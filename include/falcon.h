@@ -337,6 +337,7 @@ typedef struct falcon_server_config {
 
 typedef struct falcon_server_info {
     int64_t ring_entries, in_flight, submitted, kernel_launches, warps, device_bytes;
+    int64_t concurrent_classes_max; /* most request classes whose kernels ran at the same time */
 } falcon_server_info;
 
 void falcon_server_default_config(falcon_server_config *c);

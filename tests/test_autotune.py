@@ -60,6 +60,20 @@ def test_tune_small_index():
             assert t["recall"] >= 0.9
         assert e["latency"]["mode"] in ("inter", "intra")
     assert prof["D96_R64_ef128"]["throughput"]["recall"] >= prof["D96_R64_ef32"]["throughput"]["recall"]
+    # the server takes a request's parameters from the profile
+    from falcon_b200.serving import FalconServer
+    sv = FalconServer(ring_capacity=256, max_k=10, ef_max=128, cand_queue_max=64, dim_max=96, idle_exit_us=2000)
+    iid = sv.add_index(ix)
+    sv.set_profile(prof)
+    p = sv.auto_params(iid, k=10, ef=100)
+    want = prof["D96_R64_ef128"]["throughput"]["params"]     # the entry at or above the requested ef
+    assert (p.ef, p.mc, p.mg, p.cand_queue_size, p.bloom_bits) == (100, want["mc"], want["mg"],
+                                                                    want["cand_queue_size"], want["bloom_bits"])
+    rid = sv.submit([iid], q[:1], p)
+    ids, d, hops, vis = sv.wait(rid[0], 10)
+    r = ix.search(q[:1], k=10, ef=p.ef, mc=p.mc, mg=p.mg, cand_queue_size=p.cand_queue_size, bloom_bits=p.bloom_bits)
+    assert np.array_equal(ids, r.ids[0]) and hops == r.hops[0]
+    sv.close()
 
 
 def test_channel_bloom_bits():

@@ -34,12 +34,35 @@ def test_build_info_and_defaults(lib):
     assert (p.k, p.ef, p.mc, p.mg, p.cand_queue_size, p.bloom_bits, p.hash_seed) == (10, 64, 1, 1, 32, 16, 1)
 
 
-def test_struct_layouts_match_header():
+def test_struct_layouts_match_header(tmp_path):
+    """Every struct the ctypes binding mirrors has the header's size and field
+    offsets (compiled with the system C compiler)."""
     import ctypes
+    import subprocess
     from falcon_b200 import _lib
     assert ctypes.sizeof(_lib.IndexDesc) == 72
     assert ctypes.sizeof(_lib.SearchParams) == 48
     assert ctypes.sizeof(_lib.IndexInfo) == 40
+    pairs = [("falcon_index_desc", _lib.IndexDesc), ("falcon_index_info", _lib.IndexInfo),
+             ("falcon_search_params", _lib.SearchParams), ("falcon_upper_layers_desc", _lib.UpperLayersDesc),
+             ("falcon_server_config", _lib.ServerConfig), ("falcon_server_info", _lib.ServerInfo)]
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "falcon.h"', "int main(void) {"]
+    for cname, cls in pairs:
+        lines.append('printf("%%zu\\n", sizeof(%s));' % cname)
+        for f, _ in cls._fields_:
+            lines.append('printf("%%zu\\n", offsetof(%s, %s));' % (cname, f))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", inc, str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    want = []
+    for _, cls in pairs:
+        want.append(ctypes.sizeof(cls))
+        want += [getattr(cls, f).offset for f, _ in cls._fields_]
+    assert got == want
 
 
 def test_null_arguments_return_errors_without_gpu(lib):

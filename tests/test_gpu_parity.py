@@ -300,6 +300,24 @@ INTRA_CASES = [
 ]
 
 
+def test_gpu_intra_matches_reference_v15_fixture():
+    """Intra-query mode against the reference's own v1.5 kernel pipeline
+    (fixture made by tests/golden/make_golden.py): ids, distance bits, hops."""
+    from falcon_b200.formats import Graph
+    from falcon_b200.synthetic import unit_normal
+    from helpers import fixture
+    f = fixture("intra_v15_d96_md64.npz")
+    x = unit_normal(int(f["n"]), int(f["dim"]), seed=int(f["data_seed"]))
+    q = unit_normal(int(f["n_queries"]), int(f["dim"]), seed=int(f["query_seed"]))
+    g = Graph.from_adjacency(x, f["adjacency"].astype(np.int32), int(f["entry"]))
+    ix = _index(g)
+    for i, (ch, ef, mc, mg, bits) in enumerate(f["params"]):
+        r = ix.search(q, k=int(ef), ef=int(ef), mc=int(mc), mg=int(mg), bloom_bits=int(bits), mode="intra",
+                      channels=int(ch))
+        assert _same(r.ids, r.dists, f["ids_%d" % i], f["dists_%d" % i])
+        assert np.array_equal(r.hops, f["hops_%d" % i])
+
+
 @pytest.mark.parametrize("kind,dim,md,ef,mc,mg,ch,bits,prec", INTRA_CASES)
 def test_gpu_intra_matches_oracle(oracle_mod, kind, dim, md, ef, mc, mg, ch, bits, prec):
     g, q = small_graph(kind, 4000, dim, md, 64, seed=13)

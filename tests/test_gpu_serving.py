@@ -70,6 +70,8 @@ def test_server_results_equal_alone(two_indexes):
         assert _same(got, ref), (w, p)
     info = sv.info()
     assert info.in_flight == 0 and info.submitted == len(reqs)
+    # the classes of the mix (FP32 at D=128 and D=384, BF16, FP8) share the GPU
+    assert info.concurrent_classes_max >= 2
     sv.close()
 
 

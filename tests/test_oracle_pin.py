@@ -161,3 +161,125 @@ def test_intra_channels_change_visits_not_quality(oracle_mod):
             ef=64, mc=2, mg=4, mode="intra", channels=ch, bloom_bits=14))
         recs.append(recall_at_k(ids, gt, 10))
     assert max(recs) - min(recs) < 0.1
+
+
+def _insert_one_at_a_time(R, C, cq, stream):
+    """The sorted-list model of results collection (DRAM_utils.hpp:421-438 +
+    scheduler.hpp:102-110): x kept iff below the result maximum, forwarded iff
+    also below the candidate maximum; lists of (distance, age, id) ascending,
+    the newest of the maximal entries evicted."""
+    R, C = list(R), list(C)
+    for d, age, i in stream:
+        if d < R[-1][0]:
+            R.append((d, age, i))
+            R.sort(key=lambda e: (e[0], e[1]))
+            R.pop()
+            if d < C[cq - 1][0]:
+                C = C[:cq] + [(d, age, i)]
+                C.sort(key=lambda e: (e[0], e[1]))
+                C = C[:cq]
+    return R, C
+
+
+def _merge_window(R, C, cq, stream):
+    """The kernels' window merge (merge_window in the traversal kernels):
+    kept iff fewer than ef of {old results, earlier slots} are <= d; forwarded
+    iff kept and fewer than cq of {old candidates, earlier kept slots} are
+    <= d; every entry placed at its merged position."""
+    ef = len(R)
+    rd = [e[0] for e in R]
+    cdl = [e[0] for e in C[:cq]]
+    ds = [x[0] for x in stream]
+    kept = [sum(v <= d for v in rd) + sum(ds[i] <= d for i in range(j)) < ef for j, d in enumerate(ds)]
+    fwd = [kept[j] and sum(v <= d for v in cdl) + sum(ds[i] <= d for i in range(j) if kept[i]) < cq
+           for j, d in enumerate(ds)]
+
+    def merged(old, n, flags):
+        new = [x for x, f in zip(stream, flags) if f]
+        out = [None] * (len(old) + len(new))
+        for p, e in enumerate(old):
+            out[p + sum(x[0] < e[0] for x in new)] = e
+        for j, x in enumerate(new):
+            pos = sum(v[0] <= x[0] for v in old) + sum(y[0] < x[0] or (y[0] == x[0] and k < j)
+                                                       for k, y in enumerate(new))
+            out[pos] = x
+        return out[:n]
+
+    return merged(R, ef, kept), merged(C[:cq], cq, fwd) + C[cq:]
+
+
+def test_window_merge_equals_one_at_a_time_insertion():
+    """The closed form the kernels merge with (a window of up to 32 stream
+    slots at once) leaves both queues exactly as inserting one at a time
+    does, ties included, over random tie-heavy streams and list sizes."""
+    rng = np.random.default_rng(77)
+    for trial in range(400):
+        ef = int(rng.integers(1, 80))
+        cq = int(rng.integers(1, 40))
+        hi = int(rng.choice([3, 8, 1000]))
+        age = 0
+        R, C = [], []
+        for p in range(ef):
+            R.append((1e20, age, -1))
+            age += 1
+        for p in range(cq):
+            C.append((1e20, age, -1))
+            age += 1
+        # a few windows in sequence; pops of the candidate head between them
+        for w in range(int(rng.integers(1, 5))):
+            m = int(rng.integers(0, 33))
+            stream = []
+            for _ in range(m):
+                stream.append((float(rng.integers(0, hi)), age, age))
+                age += 1
+            R1, C1 = _insert_one_at_a_time(R, C, cq, stream)
+            R2, C2 = _merge_window(R, C, cq, stream)
+            assert [(e[0], e[2]) for e in R1] == [(e[0], e[2]) for e in R2], trial
+            assert [(e[0], e[2]) for e in C1[:cq]] == [(e[0], e[2]) for e in C2[:cq]], trial
+            R, C = R1, C1
+            if rng.integers(0, 2):
+                C = C[1:cq] + [(1e20, age, -1)]
+                age += 1
+
+
+@pytest.mark.parametrize("channels,ef,mc,mg,bits", [(2, 64, 1, 1, 15), (4, 64, 2, 6, 14), (4, 128, 4, 3, 15),
+                                                    (2, 32, 2, 2, 16)])
+def test_intra_live_against_reference_v15_pipeline(oracle_mod, channels, ef, mc, mg, bits):
+    """The oracle's intra-query restatement (channel-order merge) against the
+    reference's own v1.5 kernel headers compiled as C++ (readiness-order merge
+    across channel threads): on data without repeated distances the merge
+    order cannot change a group's outcome, so ids, distance bits and hops
+    agree exactly."""
+    if not oracle_mod.ref_intra_available(96, channels):
+        pytest.skip("reference v1.5 harness not built on this host")
+    g, q = small_graph("unit", 3000, 96, 64, 24, seed=8)
+    og = oracle_graph(oracle_mod, g)
+    ids, d, hops, _, _ = oracle_mod.search(og, q, g.entry_point, oracle_mod.make_params(
+        k=ef, ef=ef, mc=mc, mg=mg, bloom_bits=bits, mode="intra", channels=channels))
+    rid, rd, rh = oracle_mod.ref_intra_search(g.vectors, g.links, 64, q, g.entry_point, channels, ef=ef, mc=mc,
+                                              mg=mg, bloom_bits=bits)
+    assert np.array_equal(ids, rid)
+    assert np.array_equal(d.view(np.uint32), rd.view(np.uint32))
+    assert np.array_equal(hops, rh)
+
+
+def _intra_fixture():
+    from falcon_b200.formats import Graph
+    from falcon_b200.synthetic import unit_normal
+    f = fixture("intra_v15_d96_md64.npz")
+    x = unit_normal(int(f["n"]), int(f["dim"]), seed=int(f["data_seed"]))
+    q = unit_normal(int(f["n_queries"]), int(f["dim"]), seed=int(f["query_seed"]))
+    return f, Graph.from_adjacency(x, f["adjacency"].astype(np.int32), int(f["entry"])), q
+
+
+def test_intra_oracle_matches_v15_fixture(oracle_mod):
+    """The committed fixture from the reference's v1.5 pipeline (runs without
+    the reference checkout)."""
+    f, g, q = _intra_fixture()
+    og = oracle_graph(oracle_mod, g)
+    for i, (ch, ef, mc, mg, bits) in enumerate(f["params"]):
+        ids, d, hops, _, _ = oracle_mod.search(og, q, g.entry_point, oracle_mod.make_params(
+            k=int(ef), ef=int(ef), mc=int(mc), mg=int(mg), bloom_bits=int(bits), mode="intra", channels=int(ch)))
+        assert np.array_equal(ids, f["ids_%d" % i])
+        assert np.array_equal(d.view(np.uint32), f["dists_%d" % i].view(np.uint32))
+        assert np.array_equal(hops, f["hops_%d" % i])
