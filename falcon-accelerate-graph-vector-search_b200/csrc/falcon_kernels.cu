@@ -1735,7 +1735,11 @@ __global__ void __launch_bounds__(128, 3) serve_kernel(const ServeLaunch S)
     float *cand_d = S.cand_d + gw * S.ef_max;
     const int32_t *slots = S.class_slots + (size_t)CLS * S.ring_cap;
     uint32_t epoch = 0;
-    if (lane == 0) epoch = reinterpret_cast<const volatile uint32_t *>(S.run_epoch)[CLS];
+    long long t_start = 0;   // a launch counts its own start as activity of its class
+    if (lane == 0) {
+        epoch = reinterpret_cast<const volatile uint32_t *>(S.run_epoch)[CLS];
+        t_start = global_ns();
+    }
 
     for (;;) {
         unsigned long long h = ~0ull;
@@ -1758,7 +1762,8 @@ __global__ void __launch_bounds__(128, 3) serve_kernel(const ServeLaunch S)
             int leave = 0;
             if (lane == 0) {
                 const int stop = *reinterpret_cast<volatile int *>(&S.ctl->stop);
-                const long long last = *reinterpret_cast<volatile long long *>(&S.ctl->last_active_ns[CLS]);
+                long long last = *reinterpret_cast<volatile long long *>(&S.ctl->last_active_ns[CLS]);
+                if (last < t_start) last = t_start;
                 leave = stop || (global_ns() - last > S.idle_ns);
             }
             if (__shfl_sync(kFull, leave, 0)) break;

@@ -13,15 +13,16 @@
 // The kernels of all classes with work run at the same time, each on its own
 // stream: with P classes wanting the GPU, each launch gets 1/P of the blocks
 // and its own range of per-warp scratch slots (Bloom filters, rerank
-// candidates).  Each (class, P, range) launch is captured in a CUDA graph the
-// first time it is needed and replayed afterwards.  When another class gets
+// candidates).  Each (class, P, range) launch is captured in a CUDA graph when
+// an index of the class is registered (or on first use) and replayed; a launch
+// waits for the tails of the submit that caused it.  When another class gets
 // work, a running launch whose share is now too large is asked to yield (its
 // warps leave between requests) and is relaunched with the smaller share; a
 // launch with a smaller share than the current one keeps running until its
 // class idles out, so a load that comes and goes does not relaunch kernels.
 // A class kernel leaves after `idle_exit_us` without a claim or completion of
-// its class and is relaunched by the next submit or poll, so an idle server
-// holds no SMs.
+// its class (its own start counts as one) and is relaunched by the next submit
+// or poll, so an idle server holds no SMs.
 //
 // Requests to an index with HNSW upper layers get their entry from the
 // descent kernel, launched at submit on the copy stream over the new queries
@@ -32,13 +33,20 @@
 //
 // Admission by memory: the ring is sized from the free device memory at
 // creation, and each submit admits requests only while the requests in
-// flight stay within memory_fraction of the device memory that is free
-// (re-read at most every kMemCheckUs) plus what the server already holds; a
-// request is refused (not queued) while its ring entry is still in use.
+// flight stay within memory_fraction of the device memory that is free plus
+// what the server already holds; a request is refused (not queued) while its
+// ring entry is still in use.  The free memory is read by a monitor thread
+// every kMemPollMs, never on the submit path: cudaMemGetInfo has been
+// measured at up to tens of milliseconds while the class kernels run, so the
+// monitor reads the device's memory through NVML (loaded at run time from
+// the driver's libnvidia-ml) and falls back to cudaMemGetInfo without it.
 #include <cuda_runtime.h>
+
+#include <dlfcn.h>
 
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -72,6 +80,8 @@ struct falcon_server {
     cudaStream_t ystream = nullptr;       // yield requests: never queued behind a submit's descent
     cudaStream_t kstream[kServeClasses] = {};
     cudaEvent_t kernel_done[kServeClasses] = {};
+    cudaEvent_t published = nullptr;      // the last submit's tail copy (copy stream)
+    bool published_rec = false;
     // graph[c][P-1][r]: class c's launch over 1/P of the blocks, scratch range r
     cudaGraphExec_t graph[kServeClasses][4][4] = {};
     bool launched[kServeClasses] = {};
@@ -81,8 +91,11 @@ struct falcon_server {
     bool yield_sent[kServeClasses] = {};
     int64_t launches = 0;
     int64_t concurrent_max = 0;           // most class kernels running at once
-    int64_t mem_cap = 0;                  // requests in flight admitted by memory
-    std::chrono::steady_clock::time_point mem_t;   // last free-memory reading
+    std::atomic<int64_t> mem_cap{0};      // requests in flight admitted by memory (monitor thread)
+    std::thread mem_monitor;
+    std::mutex mem_mu;
+    std::condition_variable mem_cv;
+    bool mem_stop = false;
     // device
     GraphView *d_views = nullptr;
     ServeDesc *d_ring = nullptr;
@@ -136,6 +149,14 @@ int cuda_fail(cudaError_t e, const char *what)
 
 void free_server(falcon_server *sv)
 {
+    if (sv->mem_monitor.joinable()) {
+        {
+            std::lock_guard<std::mutex> l(sv->mem_mu);
+            sv->mem_stop = true;
+        }
+        sv->mem_cv.notify_all();
+        sv->mem_monitor.join();
+    }
     for (int c = 0; c < kServeClasses; c++) {
         for (int p = 0; p < 4; p++)
             for (int r = 0; r < 4; r++)
@@ -143,6 +164,7 @@ void free_server(falcon_server *sv)
         if (sv->kernel_done[c]) cudaEventDestroy(sv->kernel_done[c]);
         if (sv->kstream[c]) cudaStreamDestroy(sv->kstream[c]);
     }
+    if (sv->published) cudaEventDestroy(sv->published);
     if (sv->cstream) cudaStreamDestroy(sv->cstream);
     if (sv->ystream) cudaStreamDestroy(sv->ystream);
     cudaFree(sv->d_views);
@@ -174,8 +196,8 @@ void free_server(falcon_server *sv)
 constexpr int kDescendSlots = 8;
 // Most classes sharing the SMs at once (more wait for a share to free up).
 constexpr int kMaxParts = 4;
-// Free device memory is re-read at most this often by submit.
-constexpr double kMemCheckUs = 1000.0;
+// Period of the free-memory monitor.
+constexpr int kMemPollMs = 5;
 
 // Whether class c has a request that is neither collected nor done: with no
 // kernel running, exactly the requests still to be claimed.  Walks the
@@ -281,7 +303,9 @@ int ensure_running(falcon_server *sv)
         cudaError_t e = class_graph(sv, c, parts, range, &ge);
         if (e != cudaSuccess) return cuda_fail(e, "serve graph");
         sv->h_run_epoch[c] = ++sv->epoch[c];
-        e = cudaGraphLaunch(ge, sv->kstream[c]);
+        // the launch starts after the tails it is launched for have landed
+        if (sv->published_rec) e = cudaStreamWaitEvent(sv->kstream[c], sv->published, 0);
+        if (e == cudaSuccess) e = cudaGraphLaunch(ge, sv->kstream[c]);
         if (e == cudaSuccess) e = cudaEventRecord(sv->kernel_done[c], sv->kstream[c]);
         if (e != cudaSuccess) return cuda_fail(e, "serve kernel launch");
         sv->launched[c] = true;
@@ -296,26 +320,86 @@ int ensure_running(falcon_server *sv)
     return FALCON_OK;
 }
 
-// Requests in flight the free device memory allows (re-read at most every
-// kMemCheckUs): memory_fraction of (free memory + the server's own), at
-// most the ring.  Caller holds mu.
-int64_t memory_admission_cap(falcon_server *sv)
-{
-    const auto now = std::chrono::steady_clock::now();
-    if (sv->mem_cap == 0 ||
-        std::chrono::duration<double, std::micro>(now - sv->mem_t).count() >= kMemCheckUs) {
-        size_t free_b = 0, total_b = 0;
-        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
-            const double per = (double)(sizeof(float) * sv->qstride + sizeof(ServeDesc));
-            const double budget = sv->cfg.memory_fraction * ((double)free_b + (double)sv->device_bytes);
-            int64_t cap = (int64_t)(budget / per);
-            sv->mem_cap = cap < sv->cap ? (cap < 1 ? 1 : cap) : sv->cap;
-        } else if (sv->mem_cap == 0) {
-            sv->mem_cap = sv->cap;
+// NVML's memory query, resolved from the driver's library at run time.
+struct NvmlMemory {
+    unsigned long long total, free, used;
+};
+struct NvmlMem {
+    void *lib = nullptr;
+    void *dev = nullptr;
+    int (*shutdown)() = nullptr;
+    int (*mem)(void *, NvmlMemory *) = nullptr;
+
+    bool open(int device)
+    {
+        char bus[32];
+        if (cudaDeviceGetPCIBusId(bus, (int)sizeof(bus), device) != cudaSuccess) return false;
+        lib = dlopen("libnvidia-ml.so.1", RTLD_NOW | RTLD_LOCAL);
+        if (!lib) return false;
+        auto init = reinterpret_cast<int (*)()>(dlsym(lib, "nvmlInit_v2"));
+        auto by_bus = reinterpret_cast<int (*)(const char *, void **)>(dlsym(lib, "nvmlDeviceGetHandleByPciBusId_v2"));
+        shutdown = reinterpret_cast<int (*)()>(dlsym(lib, "nvmlShutdown"));
+        mem = reinterpret_cast<int (*)(void *, NvmlMemory *)>(dlsym(lib, "nvmlDeviceGetMemoryInfo"));
+        if (!init || !by_bus || !shutdown || !mem || init() != 0) {
+            dlclose(lib);
+            lib = nullptr;
+            return false;
         }
-        sv->mem_t = now;
+        if (by_bus(bus, &dev) != 0) {
+            close();
+            return false;
+        }
+        return true;
     }
-    return sv->mem_cap;
+    bool free_bytes(size_t *out)
+    {
+        NvmlMemory m;
+        if (!lib || mem(dev, &m) != 0) return false;
+        *out = (size_t)m.free;
+        return true;
+    }
+    void close()
+    {
+        if (lib) {
+            shutdown();
+            dlclose(lib);
+            lib = nullptr;
+        }
+    }
+};
+
+// Requests in flight that free_bytes of free device memory allows:
+// memory_fraction of (free memory + the server's own), at most the ring.
+int64_t memory_cap_for(const falcon_server *sv, size_t free_b)
+{
+    const double per = (double)(sizeof(float) * sv->qstride + sizeof(ServeDesc));
+    const double budget = sv->cfg.memory_fraction * ((double)free_b + (double)sv->device_bytes);
+    const int64_t cap = (int64_t)(budget / per);
+    return cap < sv->cap ? (cap < 1 ? 1 : cap) : sv->cap;
+}
+
+// The monitor thread: publishes the admission cap every kMemPollMs.
+void memory_monitor(falcon_server *sv)
+{
+    NvmlMem nv;
+    const bool have_nvml = nv.open(sv->device);
+    if (!have_nvml) cudaSetDevice(sv->device);
+    std::unique_lock<std::mutex> l(sv->mem_mu);
+    while (!sv->mem_stop) {
+        l.unlock();
+        size_t free_b = 0, total_b = 0;
+        bool ok = have_nvml ? nv.free_bytes(&free_b) : (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess);
+        if (ok) sv->mem_cap.store(memory_cap_for(sv, free_b), std::memory_order_relaxed);
+        l.lock();
+        sv->mem_cv.wait_for(l, std::chrono::milliseconds(kMemPollMs), [sv] { return sv->mem_stop; });
+    }
+    l.unlock();
+    nv.close();
+}
+
+int64_t memory_admission_cap(const falcon_server *sv)
+{
+    return sv->mem_cap.load(std::memory_order_relaxed);
 }
 
 }  // namespace
@@ -412,6 +496,7 @@ int falcon_server_create(const falcon_server_config *c, falcon_server **out)
     }
     SV_ALLOC(cudaStreamCreateWithFlags(&sv->cstream, cudaStreamNonBlocking), "stream");
     SV_ALLOC(cudaStreamCreateWithFlags(&sv->ystream, cudaStreamNonBlocking), "stream");
+    SV_ALLOC(cudaEventCreateWithFlags(&sv->published, cudaEventDisableTiming), "event");
     SV_ALLOC(cudaMalloc(&sv->d_views, sizeof(GraphView) * 48), "views");
     SV_ALLOC(cudaMalloc(&sv->d_ring, sizeof(ServeDesc) * sv->cap), "ring");
     SV_ALLOC(cudaMalloc(&sv->d_class_slots, sizeof(int32_t) * kServeClasses * (size_t)sv->cap), "class queues");
@@ -476,6 +561,14 @@ int falcon_server_create(const falcon_server_config *c, falcon_server **out)
     sv->entry_seq.assign(sv->cap, ~0ull);
     sv->entry_k.assign(sv->cap, 0);
     sv->entry_cls.assign(sv->cap, 0);
+    // the first admission cap from the reading above, then the monitor's
+    sv->mem_cap.store(memory_cap_for(sv, free_b), std::memory_order_relaxed);
+    try {
+        sv->mem_monitor = std::thread(memory_monitor, sv);
+    } catch (...) {
+        free_server(sv);
+        return set_error_code(FALCON_ERR_OOM, "falcon_server_create: cannot start the memory monitor");
+    }
     *out = sv;
     return FALCON_OK;
 }
@@ -514,6 +607,21 @@ int falcon_server_add_index(falcon_server *sv, falcon_index *ix, int32_t *index_
     if (upper) sv->any_upper = true;
     for (int pr = 0; pr < 3; pr++) sv->index_vrows.push_back(serve_vrows(views[pr].dpad, pr));
     *index_id = id;
+    // capture the launches of the index's classes now, so that the first
+    // requests of a share do not wait for a graph instantiation (a failure
+    // here only leaves the capture to first use)
+    for (int pr = 0; pr < 3; pr++) {
+        int d2 = 0, e2 = 0;
+        GraphView pv;
+        if (index_graph_view(ix, pr, &pv, &d2, &e2) != FALCON_OK) continue;
+        const int cls = serve_class(pr, serve_vrows(pv.dpad, pr));
+        if (cls < 0 || cls >= kServeClasses || !sv->class_ok[cls] || sv->launched[cls]) continue;
+        for (int parts = 1; parts <= kMaxParts; parts++)
+            for (int r = 0; r < parts; r++) {
+                cudaGraphExec_t ge;
+                if (class_graph(sv, cls, parts, r, &ge) != cudaSuccess) cudaGetLastError();
+            }
+    }
     return FALCON_OK;
 }
 
@@ -658,6 +766,9 @@ int falcon_server_submit(falcon_server *sv, int32_t n, const int32_t *index_ids,
     }
     sv->next_seq = tail;
     sv->in_flight += admitted;
+    // class kernels launched from now on wait for these tails (without the
+    // event a launch could start first; it then idles until they land)
+    if (cudaEventRecord(sv->published, sv->cstream) == cudaSuccess) sv->published_rec = true;
     const int rc = ensure_running(sv);
     return rc != FALCON_OK ? rc : admitted;
 }
