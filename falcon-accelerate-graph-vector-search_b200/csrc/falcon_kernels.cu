@@ -1157,33 +1157,41 @@ __global__ void __launch_bounds__(128, (InterBlocks<ELEM, EPL, VROWS>::value)) i
 
 // ---------------------------------------------------------------------------
 // Intra-query mode (reference intra-query v1.5): one thread block per query,
-// `channels` channels of W warps each (W only spreads the work; results do
-// not depend on it).  Per retired group the block
-//   1. routes the group's neighbour ids to channel id & (channels-1) keeping
-//      stream order (utils.hpp:396-495, split_tasks_to_channels), and the
-//      channel's first warp runs the channel's Bloom filter over them
+// `channels` channels of W fetch warps each (W only spreads the work; results
+// do not depend on it) and one merge warp.  Per group
+//   1. the channel's first warp routes the group's neighbour ids to channel
+//      id & (channels-1) keeping stream order (utils.hpp:396-495,
+//      split_tasks_to_channels) and runs the channel's Bloom filter over them
 //      (the reference's per-channel bloom PE), keeping the new ids in order;
 //   2. the channel's W warps gather the new vectors and form their distances
 //      (the per-channel fetch/compute PEs), batches dealt round robin;
-//   3. warp 0 merges the channels in channel order into the queues
+//   3. the merge warp merges the channels in channel order into the queues
 //      (gather_distances_from_channels, utils.hpp:497-569, merges in
 //      readiness order; channel order is one of its schedules; a whole
 //      group is merged before the scheduler acts, so on distinct distances
 //      the order cannot change the outcome), then the scheduler refills the
 //      group FIFO (v1.5 scheduler.hpp:94-146) and prefetches the rows of the
 //      candidates it popped.
+// Steps 1-2 of a group run while step 3 of the group before it runs (DST:
+// with mg >= 2 groups in flight the fetch overlaps the merge).
 // The stale-threshold prefilter of v1.5 (utils.hpp:277-347) is omitted: it
 // only drops distances that the result queue would reject anyway.
 // ---------------------------------------------------------------------------
 struct IntraSmem {
     unsigned long long qi;
-    int inflight, head, hops, truncated, done;
-    int chan_valid[kMaxChannels];
+    // the group FIFO's state, published by the merge warp each step into the
+    // slot of the step's parity: head, groups in flight (popped, not merged),
+    // hops, truncated
+    int st[2][4];
+    int chan_valid[2][kMaxChannels];   // per step parity
     int chan_visited[kMaxChannels];
 };
 
-// Most warps an intra-query block uses (channels x warps per channel).
-constexpr int kIntraMaxWarps = 16;
+// Most warps an intra-query block uses: up to 12 fetch warps (channels x
+// warps per channel) and the merge warp.  13 warps put at most 4 on each of
+// the SM's four schedulers, which leaves 128 registers per thread (17 would
+// leave 96 and spill).
+constexpr int kIntraMaxWarps = 13;
 
 template <int ELEM, int EPL, int VROWS>
 __global__ void __launch_bounds__(32 * kIntraMaxWarps) intra_kernel(const SearchLaunch A)
@@ -1194,9 +1202,11 @@ __global__ void __launch_bounds__(32 * kIntraMaxWarps) intra_kernel(const Search
     constexpr bool HEAP = EPL > 8;
     constexpr int HEAP_CAP = HEAP ? 32 * EPL : 0;
     const int C = A.channels;
-    const int W = (blockDim.x >> 5) / C;                  // warps per channel
+    const int MW = (blockDim.x >> 5) - 1;                 // the merge warp; 0 .. MW-1 fetch
+    const int W = MW / C;                                 // fetch warps per channel
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int chan = warp / W, sub = warp - chan * W;
+    const bool merger = warp == MW;
+    const int chan = merger ? 0 : warp / W, sub = merger ? 0 : warp - chan * W;
     const GraphView &g = A.g;
     const int nseg = g.dpad * ET<ELEM>::BYTES / 16;
     unsigned char *base_ptr = reinterpret_cast<unsigned char *>(smem_u4);
@@ -1207,13 +1217,14 @@ __global__ void __launch_bounds__(32 * kIntraMaxWarps) intra_kernel(const Search
     uint32_t *bloom = smem_bloom ? reinterpret_cast<uint32_t *>(base_ptr + off + bloom_bytes * chan)
                                  : A.bloom_global + ((size_t)blockIdx.x * C + chan) * (bloom_bytes / 4);
     if (smem_bloom) off += bloom_bytes * C;
-    // channel c's ids (then its new ids and their distances) of the current
-    // group: lcap slots at c * lcap
+    // channel c's ids (then its new ids and their distances) of a group: lcap
+    // slots at (parity * C + c) * lcap; a step fills one parity while the
+    // merge warp reads the other
     const int lcap = A.mc_max * g.max_degree;
     int *list_id = reinterpret_cast<int *>(base_ptr + off);
-    off += sizeof(int) * (size_t)lcap * C;
+    off += sizeof(int) * (size_t)lcap * C * 2;
     float *list_d = reinterpret_cast<float *>(base_ptr + off);
-    off += sizeof(float) * (size_t)lcap * C;
+    off += sizeof(float) * (size_t)lcap * C * 2;
     int *fifo = reinterpret_cast<int *>(base_ptr + off);
     off += sizeof(int) * (size_t)(A.mc_max * A.mg_max);
     int *fifo_len = reinterpret_cast<int *>(base_ptr + off);
@@ -1223,7 +1234,7 @@ __global__ void __launch_bounds__(32 * kIntraMaxWarps) intra_kernel(const Search
     int *hid = reinterpret_cast<int *>(base_ptr + off + sizeof(uint64_t) * HEAP_CAP);
     off += (sizeof(uint64_t) + sizeof(int)) * HEAP_CAP;
     using Caps = ListCaps<EPL, true>;
-    SmemLists L;   // sorted lists for ef <= 256, used by warp 0
+    SmemLists L;   // sorted lists for ef <= 256, used by the merge warp
     L.rd = reinterpret_cast<float *>(base_ptr + off);
     L.ri = reinterpret_cast<int *>(L.rd + Caps::r);
     L.cd = reinterpret_cast<float *>(L.ri + Caps::r);
@@ -1236,8 +1247,6 @@ __global__ void __launch_bounds__(32 * kIntraMaxWarps) intra_kernel(const Search
     const int gmask = (1 << lg) - 1;
     const bool rep_lane = (lane & gmask) < NB;
     const int my_slot = (lane >> lg) * NB + (lane & gmask);
-    int *my_ids = list_id + (size_t)lcap * chan;
-    float *my_d = list_d + (size_t)lcap * chan;
 
     for (;;) {
         if (threadIdx.x == 0) S->qi = atomicAdd(reinterpret_cast<unsigned long long *>(A.work_counter), 1ull);
@@ -1259,25 +1268,25 @@ __global__ void __launch_bounds__(32 * kIntraMaxWarps) intra_kernel(const Search
                 }
             }
         }
-        if (sub == 0) {
+        if (!merger) {   // the channel's warps clear its filter
             const int nvec = 1 << (P.bloom_bits - 7);
             uint4 *b4 = reinterpret_cast<uint4 *>(bloom);
-            for (int i = lane; i < nvec; i += 32) b4[i] = make_uint4(0, 0, 0, 0);
+            for (int i = sub * 32 + lane; i < nvec; i += 32 * W) b4[i] = make_uint4(0, 0, 0, 0);
         }
         const uint32_t bmask = (1u << P.bloom_bits) - 1u;
         int visited = 0;
-        // queues live in warp 0: the bucketed list + register candidate list
-        // for ef > 256, else the sorted lists L in shared memory
+        // queues live in the merge warp: the bucketed list + register candidate
+        // list for ef > 256, else the sorted lists L in shared memory
         uint32_t age = 0;
         BucketMax BM;
         constexpr int CPL = CandPerLane<EPL>::value;
         float cd[HEAP ? CPL : 1];
         int ci[HEAP ? CPL : 1];
         if constexpr (HEAP) {
-            if (warp == 0) bucket_init<EPL>(BM, hkey, hid, P.ef, lane);
+            if (merger) bucket_init<EPL>(BM, hkey, hid, P.ef, lane);
 #pragma unroll
             for (int e = 0; e < CPL; e++) { cd[e] = kLarge; ci[e] = -1; }
-        } else if (warp == 0) {
+        } else if (merger) {
             for (int p = lane; p < P.ef; p += 32) { L.rd[p] = kLarge; L.ri[p] = -1; }
             for (int p = lane; p < P.cq; p += 32) { L.cd[p] = kLarge; L.ci[p] = -1; }
             __syncwarp();
@@ -1285,89 +1294,155 @@ __global__ void __launch_bounds__(32 * kIntraMaxWarps) intra_kernel(const Search
         float rmax = kLarge, cmax = kLarge;
         if (threadIdx.x == 0) {
             int entry = A.entries ? A.entries[qi] : A.default_entry;
-            S->inflight = 1;
-            S->hops = 1;
+            int n = 1;
             if (entry < 0 || (int64_t)entry >= g.n) {
                 atomicOr(A.status, 2);
                 entry = 0;
-                S->inflight = 0;
-                S->hops = 0;
+                n = 0;
             }
             fifo[0] = entry;
             fifo_len[0] = 1;
-            S->head = 0;
-            S->truncated = 0;
+            S->st[1][0] = 0;   // head
+            S->st[1][1] = n;   // groups in flight
+            S->st[1][2] = n;   // hops
+            S->st[1][3] = 0;   // truncated
         }
         __syncthreads();
-        while (S->inflight > 0) {
-            const int head = S->head;
-            const int glen = fifo_len[head];
-            // 1. the channel's first warp: its ids of the group's rows in stream
-            //    order, then its Bloom filter; the new ids are compacted in place
-            if (sub == 0) {
-                int count = 0;
-                for (int b = 0; b < glen; b++) {
-                    const int32_t *row = g.links + (int64_t)fifo[head * mc + b] * g.lstride;
-                    const int cnt = ld_nc_s32(row);
-                    for (int c0 = 0; c0 < cnt; c0 += 32) {
-                        const int nb = (c0 + lane < cnt) ? ld_nc_s32(row + g.ids_off + c0 + lane) : -1;
-                        const bool mine = nb >= 0 && (nb & (C - 1)) == chan;
-                        const unsigned mm = __ballot_sync(kFull, mine);
-                        if (mine) my_ids[count + __popc(mm & ((1u << lane) - 1u))] = nb;
-                        count += __popc(mm);
-                    }
-                }
-                __syncwarp();
-                int nvalid = 0;
-                for (int c0 = 0; c0 < count; c0 += 32) {
-                    const bool act = c0 + lane < count;
-                    const int nb = act ? my_ids[c0 + lane] : -1;
-                    const bool valid = bloom_chunk(bloom, bmask, P.seed, nb, act, lane);
-                    const unsigned vm = __ballot_sync(kFull, valid);
-                    // written at or below the chunk just read: the in-place compaction is safe
-                    if (valid) {
-                        my_ids[nvalid + __popc(vm & ((1u << lane) - 1u))] = nb;
-                        prefetch_l2(g.vecs + (int64_t)nb * g.vstride_bytes, vbytes);
-                    }
-                    nvalid += __popc(vm);
-                    __syncwarp();
-                }
-                visited += nvalid;
-                if (lane == 0) S->chan_valid[chan] = nvalid;
+        // Step s: the fetch warps take the oldest group not yet fetched (split,
+        // Bloom, gathers, distances) into parity s & 1 while the merge warp
+        // merges the group fetched in step s - 1 and refills the FIFO.  Bloom
+        // filters see the groups in FIFO order and the merges happen in FIFO
+        // order, each followed by its pops, so the outcome equals fetching each
+        // group only after the previous one is merged; with mg >= 2 the fetch
+        // of a group overlaps the merge of the one before it.
+        bool hf = false;   // the head group was fetched in the previous step
+        int fin = 1;       // the state slot the loop ends on
+        for (int step = 0;; step++) {
+            const int *st = S->st[(step + 1) & 1];
+            const int head = st[0], n = st[1];
+            if (n == 0) {
+                fin = (step + 1) & 1;
+                break;
             }
-            __syncthreads();
-            // 2. the channel's warps: gathers and distances, batch b by warp b mod W
-            {
-                const int nvalid = S->chan_valid[chan];
-                const int step = BS * W;
+            const int par = step & 1;
+            int fslot = -1;
+            if (!hf) fslot = head;
+            else if (n >= 2) fslot = (head + 1 == mg) ? 0 : head + 1;
+            if (!merger && fslot >= 0) {
+                const int glen = fifo_len[fslot];
+                int *my_ids = list_id + (size_t)lcap * (par * C + chan);
+                float *my_d = list_d + (size_t)lcap * (par * C + chan);
+                // 1. the channel's first warp: its ids of the group's rows in
+                //    stream order, then its Bloom filter; the new ids are
+                //    compacted in place
+                if (sub == 0) {
+                    int count = 0;
+                    if (g.max_degree <= 64) {
+                        // counts and ids of up to 4 rows in one round trip (a row
+                        // always holds max_degree slots; those past the count are masked)
+                        for (int b0 = 0; b0 < glen; b0 += 4) {
+                            int rc[4], r0[4], r1[4];
+#pragma unroll
+                            for (int u = 0; u < 4; u++) {
+                                rc[u] = 0;
+                                r0[u] = r1[u] = -1;
+                                if (b0 + u < glen) {
+                                    const int32_t *row = g.links + (int64_t)fifo[fslot * mc + b0 + u] * g.lstride;
+                                    rc[u] = ld_nc_s32(row);
+                                    if (lane < g.max_degree) r0[u] = ld_nc_s32(row + g.ids_off + lane);
+                                    if (32 + lane < g.max_degree) r1[u] = ld_nc_s32(row + g.ids_off + 32 + lane);
+                                }
+                            }
+#pragma unroll
+                            for (int u = 0; u < 4; u++) {
+#pragma unroll
+                                for (int hf2 = 0; hf2 < 2; hf2++) {
+                                    const int nb = hf2 ? r1[u] : r0[u];
+                                    const bool mine = 32 * hf2 + lane < rc[u] && nb >= 0 && (nb & (C - 1)) == chan;
+                                    const unsigned mm = __ballot_sync(kFull, mine);
+                                    if (mine) my_ids[count + __popc(mm & ((1u << lane) - 1u))] = nb;
+                                    count += __popc(mm);
+                                }
+                            }
+                        }
+                    } else {
+                        for (int b = 0; b < glen; b++) {
+                            const int32_t *row = g.links + (int64_t)fifo[fslot * mc + b] * g.lstride;
+                            const int cnt = ld_nc_s32(row);
+                            for (int c0 = 0; c0 < cnt; c0 += 32) {
+                                const int nb = (c0 + lane < cnt) ? ld_nc_s32(row + g.ids_off + c0 + lane) : -1;
+                                const bool mine = nb >= 0 && (nb & (C - 1)) == chan;
+                                const unsigned mm = __ballot_sync(kFull, mine);
+                                if (mine) my_ids[count + __popc(mm & ((1u << lane) - 1u))] = nb;
+                                count += __popc(mm);
+                            }
+                        }
+                    }
+                    __syncwarp();
+                    int nvalid = 0;
+                    for (int c0 = 0; c0 < count; c0 += 32) {
+                        const bool act = c0 + lane < count;
+                        const int nb = act ? my_ids[c0 + lane] : -1;
+                        const bool valid = bloom_chunk(bloom, bmask, P.seed, nb, act, lane);
+                        const unsigned vm = __ballot_sync(kFull, valid);
+                        // written at or below the chunk just read: the in-place compaction is safe
+                        if (valid) {
+                            my_ids[nvalid + __popc(vm & ((1u << lane) - 1u))] = nb;
+                            prefetch_l2(g.vecs + (int64_t)nb * g.vstride_bytes, vbytes);
+                        }
+                        nvalid += __popc(vm);
+                        __syncwarp();
+                    }
+                    visited += nvalid;
+                    if (lane == 0) S->chan_valid[par][chan] = nvalid;
+                }
+                // the channel's warps wait for its first warp (named barrier 1 + chan)
+                asm volatile("bar.sync %0, %1;" ::"r"(1 + chan), "r"(32 * W) : "memory");
+                // 2. the channel's warps: gathers and distances, batch b by warp b mod W
+                const int nvalid = S->chan_valid[par][chan];
+                const int stp = BS * W;
                 int b0 = BS * sub;
                 uint4 raw[NB][VROWS];
                 float scale[NB];
                 if (b0 < nvalid) gather_batch<ELEM, VROWS, NB>(g, my_ids, b0, nvalid, nseg, lane, lg, raw, scale);
-                for (; b0 < nvalid; b0 += step) {
+                for (; b0 < nvalid; b0 += stp) {
                     const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane, lg);
-                    if (b0 + step < nvalid)
-                        gather_batch<ELEM, VROWS, NB>(g, my_ids, b0 + step, nvalid, nseg, lane, lg, raw, scale);
+                    if (b0 + stp < nvalid)
+                        gather_batch<ELEM, VROWS, NB>(g, my_ids, b0 + stp, nvalid, nseg, lane, lg, raw, scale);
                     if (rep_lane && b0 + my_slot < nvalid) my_d[b0 + my_slot] = dist;
                 }
             }
-            __syncthreads();
-            // 3. warp 0 merges channels in order and runs the scheduler
-            if (warp == 0) {
-                for (int c = 0; c < C; c++) {
-                    const int o = c * lcap;
-                    const int nv = S->chan_valid[c];
-                    for (int j0 = 0; j0 < nv; j0 += 32) {
-                        const bool v = j0 + lane < nv;
-                        const float dl = v ? list_d[o + j0 + lane] : kLarge;
+            if (merger) {
+                int h = head, inflight = n, hops = st[2];
+                bool truncated = st[3] != 0;
+                if (hf) {
+                    // 3. merge the group fetched in the previous step, channels in
+                    //    order; the windows of 32 run over the channel lists laid
+                    //    end to end, so a window spans channel boundaries
+                    const int mp = par ^ 1;
+                    const int *lid = list_id + (size_t)lcap * mp * C;
+                    const float *ld = list_d + (size_t)lcap * mp * C;
+                    int total = 0;
+                    for (int c = 0; c < C; c++) total += S->chan_valid[mp][c];
+                    for (int j0 = 0; j0 < total; j0 += 32) {
+                        const int p = j0 + lane;
+                        const bool v = p < total;
+                        int src = 0;
+                        if (v) {
+                            int rem = p, c = 0;
+                            while (rem >= S->chan_valid[mp][c]) rem -= S->chan_valid[mp][c++];
+                            src = c * lcap + rem;
+                        }
+                        const float dl = v ? ld[src] : kLarge;
                         if constexpr (HEAP) {
                             unsigned m = __ballot_sync(kFull, v && dl < rmax);
                             while (m) {
                                 const int t = __ffs(m) - 1;
                                 m &= m - 1;
                                 const float dd = __shfl_sync(kFull, dl, t);
+                                const int sr = __shfl_sync(kFull, src, t);
                                 if (dd < rmax) {
-                                    const int id = list_id[o + j0 + t];
+                                    const int id = lid[sr];
                                     rmax = bucket_replace_max<EPL>(BM, hkey, hid, heap_key(dd, ++age), id, lane);
                                     if (dd < cmax) {
                                         cl_insert<CPL>(cd, ci, lane, P.cq, dd, id);
@@ -1376,53 +1451,55 @@ __global__ void __launch_bounds__(32 * kIntraMaxWarps) intra_kernel(const Search
                                 }
                             }
                         } else {
-                            const int idl = v ? list_id[o + j0 + lane] : -1;
+                            const int idl = v ? lid[src] : -1;
                             merge_window<EPL, CPL>(L, P.ef, P.cq, dl, idl, v, lane, rmax, cmax);
                         }
                     }
-                }
-                const float thr = rmax;
-                int h = (head + 1 == mg) ? 0 : head + 1;
-                int inflight = S->inflight - 1;
-                int hops = S->hops;
-                bool truncated = S->truncated != 0;
-                for (int oid = inflight; oid < mg && !truncated; oid++) {
-                    int slot = h + inflight;
-                    if (slot >= mg) slot -= mg;
-                    int n = 0;
-                    for (int bb = 0; bb < mc; bb++) {
-                        float best;
-                        if constexpr (HEAP) best = __shfl_sync(kFull, cd[0], 0);
-                        else best = L.cd[0];
-                        if (!(best <= thr && best < kLarge)) break;
-                        if (P.max_hops > 0 && hops >= P.max_hops) { truncated = true; break; }
-                        int pid;
-                        if constexpr (HEAP) pid = cl_pop<CPL>(cd, ci, lane, P.cq);
-                        else pid = list_pop<CPL>(L.cd, L.ci, P.cq, lane);
-                        // the popped candidate's row is read as soon as its group is the oldest
-                        if (lane == n) prefetch_l2(g.links + (int64_t)pid * g.lstride, rbytes);
-                        if (lane == 0) fifo[slot * mc + n] = pid;
-                        n++;
-                        hops++;
+                    // 4. the scheduler retires the group and refills the free
+                    //    group slots (threshold = worst result)
+                    const float thr = rmax;
+                    h = (h + 1 == mg) ? 0 : h + 1;
+                    inflight--;
+                    for (int oid = inflight; oid < mg && !truncated; oid++) {
+                        int slot = h + inflight;
+                        if (slot >= mg) slot -= mg;
+                        int cnt = 0;
+                        for (int bb = 0; bb < mc; bb++) {
+                            float best;
+                            if constexpr (HEAP) best = __shfl_sync(kFull, cd[0], 0);
+                            else best = L.cd[0];
+                            if (!(best <= thr && best < kLarge)) break;
+                            if (P.max_hops > 0 && hops >= P.max_hops) { truncated = true; break; }
+                            int pid;
+                            if constexpr (HEAP) pid = cl_pop<CPL>(cd, ci, lane, P.cq);
+                            else pid = list_pop<CPL>(L.cd, L.ci, P.cq, lane);
+                            // the popped candidate's row is read when its group is fetched
+                            if (lane == cnt) prefetch_l2(g.links + (int64_t)pid * g.lstride, rbytes);
+                            if (lane == 0) fifo[slot * mc + cnt] = pid;
+                            cnt++;
+                            hops++;
+                        }
+                        if (cnt == 0) break;
+                        if (lane == 0) fifo_len[slot] = cnt;
+                        inflight++;
                     }
-                    if (n == 0) break;
-                    if (lane == 0) fifo_len[slot] = n;
-                    inflight++;
+                    if constexpr (HEAP) cmax = rl_get<CPL>(cd, P.cq - 1);
+                    else cmax = L.cd[P.cq - 1];
                 }
-                if constexpr (HEAP) cmax = rl_get<CPL>(cd, P.cq - 1);
-                else cmax = L.cd[P.cq - 1];
                 if (lane == 0) {
-                    S->head = h;
-                    S->inflight = inflight;
-                    S->hops = hops;
-                    S->truncated = truncated ? 1 : 0;
+                    int *nst = S->st[step & 1];
+                    nst[0] = h;
+                    nst[1] = inflight;
+                    nst[2] = hops;
+                    nst[3] = truncated ? 1 : 0;
                 }
             }
+            hf = fslot >= 0;
             __syncthreads();
         }
-        if (sub == 0 && lane == 0) S->chan_visited[chan] = visited;
+        if (!merger && sub == 0 && lane == 0) S->chan_visited[chan] = visited;
         __syncthreads();
-        if (warp == 0) {
+        if (merger) {
             const int nwrite = A.write_all_ef ? P.ef : P.k;
             int32_t *oid_row = A.out_ids + qi * A.out_stride;
             float *od_row = A.out_d + qi * A.out_stride;
@@ -1451,9 +1528,9 @@ __global__ void __launch_bounds__(32 * kIntraMaxWarps) intra_kernel(const Search
             if (lane == 0) {
                 int vis = 0;
                 for (int c = 0; c < C; c++) vis += S->chan_visited[c];
-                if (A.out_hops) A.out_hops[qi] = S->hops;
+                if (A.out_hops) A.out_hops[qi] = S->st[fin][2];
                 if (A.out_visited) A.out_visited[qi] = vis;
-                if (S->truncated) atomicOr(A.status, 1);
+                if (S->st[fin][3]) atomicOr(A.status, 1);
             }
         }
         __syncthreads();
@@ -1464,7 +1541,7 @@ size_t intra_smem_bytes(const SearchLaunch &a, int channels, int heap_cap, int l
 {
     size_t b = (sizeof(IntraSmem) + 15) & ~(size_t)15;
     if (a.bloom_bits_max <= kMaxSmemBloomBits) b += ((size_t)1 << (a.bloom_bits_max - 3)) * channels;
-    b += 2 * sizeof(int) * (size_t)a.mc_max * a.g.max_degree * channels;
+    b += 2 * 2 * sizeof(int) * (size_t)a.mc_max * a.g.max_degree * channels;
     b += sizeof(int) * (size_t)(a.mc_max * a.mg_max + a.mg_max);
     b = (b + 15) & ~(size_t)15;
     b += (size_t)heap_cap * (sizeof(uint64_t) + sizeof(int));
@@ -1882,9 +1959,9 @@ cudaError_t launch_intra(const SearchLaunch &a, int channels, int num_sms, cudaS
     // warps per channel: a batch smaller than the SMs gets up to 16 warps per
     // query (latency), a larger one a warp per channel (throughput)
     int wpc = 1;
-    if (a.nq <= num_sms) wpc = kIntraMaxWarps / channels;
+    if (a.nq <= num_sms) wpc = (kIntraMaxWarps - 1) / channels;
     if (wpc < 1) wpc = 1;
-    const int threads = 32 * channels * wpc;
+    const int threads = 32 * (channels * wpc + 1);   // fetch warps and the merge warp
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
