@@ -512,8 +512,10 @@ def run_cfg1(args, dev, local, out):
     for ef_l in (64, 128, 256):
         for mc_l in (1, 2, 4):
             row = {"ef": ef_l, "mc": mc_l}
-            for mode, extra in (("inter", {}), ("intra4", dict(mode="intra", channels=4))):
-                pl = dict(k=k, ef=ef_l, mc=mc_l, mg=1, cand_queue_size=32, bloom_bits=16, **extra)
+            for mode, extra in (("inter", {}), ("intra4", dict(mode="intra", channels=4)),
+                                ("intra4_mg4", dict(mode="intra", channels=4, mg=4))):
+                pl = dict(k=k, ef=ef_l, mc=mc_l, mg=1, cand_queue_size=32, bloom_bits=16)
+                pl.update(extra)
                 p50, p99 = batch1_latency(ix, dq, args.latency_samples, **pl)
                 rr = ix.search(dq[:2000], **pl)
                 row[mode] = {"p50_ms": p50, "p99_ms": p99, "recall@10": recall_at_k(rr.ids.cpu().numpy(), gt[:2000], k)}
@@ -527,6 +529,16 @@ def run_cfg1(args, dev, local, out):
         pl.update(extra)
         p50, p99 = batch1_latency(ix, dq, args.latency_samples, **pl)
         lat_sel[mode] = {"p50_ms": p50, "p99_ms": p99}
+    # the autotuner's latency pick at the same ef: mode, channels and the DST
+    # setting (mc, mg) whose recall stays at the target
+    PL = pick(prof, dim, 64, ef, objective="latency")
+    if PL.get("channels") is None:
+        PL.pop("channels", None)
+    p50, p99 = batch1_latency(ix, dq, args.latency_samples, **PL)
+    rl = ix.search(dq, **PL)
+    lat_sel["tuned"] = {"p50_ms": p50, "p99_ms": p99, "recall@10": recall_at_k(rl.ids.cpu().numpy(), gt, k),
+                        "params": {kk: v for kk, v in PL.items() if kk != "k"}}
+    log("cfg1 batch-1 at the operating point: %s" % lat_sel)
     served = None if args.no_serve else serve_cfg1(ix, q, gt, prof, ef, nq / (ms_b / 1e3))
     ix.close()
     out["cfg1"] = {

@@ -15,8 +15,10 @@ measures on the device, for an index and a query sample with ground truth:
   * candidate-queue capacity and mc/mg: a grid, keeping the fastest point whose
     recall@k meets the target;
   * threads per query: inter-query (one warp) for throughput; for batch-1
-    latency, intra-query blocks of 4 or 8 channel warps are timed as well, each
-    channel with a filter sized for the ids it sees (channel_bloom_bits).
+    latency, intra-query blocks of 4 or 8 channels (12 fetch warps and a merge
+    warp) are timed as well, each channel with a filter sized for the ids it
+    sees (channel_bloom_bits), and at several (mc, mg): the intra kernel
+    overlaps a group's fetch with the previous group's merge when mg >= 2.
 
 Profiles are JSON files keyed "D{dim}_R{degree}_ef{ef}".
 """
@@ -80,10 +82,14 @@ def profile_key(dim, degree, ef):
 
 def tune(index, queries, gt, dim, degree, ef_list=(64, 128, 256, 512, 1024), k=10, recall_target=0.95,
          fp_target=0.01, cq_grid=(32, 64, 256), mcmg_grid=((1, 1), (2, 1), (1, 4)), latency_channels=(4, 8),
-         log=None):
+         latency_mcmg=((1, 1), (1, 2), (2, 4)), log=None):
     """Measure and return a profile dict {key: entry}; each entry holds the
     throughput-optimal parameters, their QPS and recall, whether the target was
-    met, and the batch-1 latency per threads-per-query choice."""
+    met, and the batch-1 latency per threads-per-query choice.  For latency the
+    intra-query kernel is also timed at the (mc, mg) of latency_mcmg: with mg >=
+    2 its fetch of a group overlaps the merge of the previous one, so DST
+    lowers latency there; a setting is eligible only if its recall stays within
+    0.002 of the throughput pick's (or at the target, when that is met)."""
     import torch
     from .groundtruth import recall_at_k
     dq = torch.from_numpy(np.ascontiguousarray(queries, dtype=np.float32)).cuda()
@@ -108,18 +114,30 @@ def tune(index, queries, gt, dim, degree, ef_list=(64, 128, 256, 512, 1024), k=1
         ok = [x for x in rows if x["recall"] >= recall_target]
         best = max(ok, key=lambda x: x["qps"]) if ok else max(rows, key=lambda x: (x["recall"], x["qps"]))
         params = {kk: best[kk] for kk in ("k", "ef", "mc", "mg", "cand_queue_size", "bloom_bits")}
+        need = min(recall_target, best["recall"] - 0.002) if ok else best["recall"] - 0.002
         lat = {"inter": _time_single(index, dq, **params)}
+        opts = {"inter": dict(params, mode="inter", channels=None)}
+        lat_recall = {"inter": best["recall"]}
         for ch in latency_channels:
-            pc = dict(params, bloom_bits=channel_bloom_bits(params["bloom_bits"], ch))
-            lat["intra_%d" % ch] = _time_single(index, dq, mode="intra", channels=ch, **pc)
+            for mc, mg in latency_mcmg:
+                pc = dict(params, mc=mc, mg=mg, bloom_bits=channel_bloom_bits(params["bloom_bits"], ch))
+                _, r = _time_batch(index, dq, reps=1, mode="intra", channels=ch, **pc)
+                rec = recall_at_k(r.ids.cpu().numpy(), gt, k)
+                name = "intra_%d_mc%d_mg%d" % (ch, mc, mg)
+                if log:
+                    log("tune latency %s ef=%d: recall %.4f (needs %.4f)" % (name, ef, rec, need))
+                if rec < need:
+                    continue
+                lat[name] = _time_single(index, dq, mode="intra", channels=ch, **pc)
+                opts[name] = dict(pc, mode="intra", channels=ch)
+                lat_recall[name] = rec
         fastest = min(lat, key=lat.get)
+        fp = opts[fastest]
         prof[profile_key(dim, degree, ef)] = {
             "throughput": {"params": dict(params, mode="inter"), "qps": best["qps"], "recall": best["recall"]},
-            "latency": {"threads_per_query": 32 if fastest == "inter" else 32 * int(fastest.split("_")[1]),
-                        "mode": "inter" if fastest == "inter" else "intra",
-                        "channels": None if fastest == "inter" else int(fastest.split("_")[1]),
-                        "bloom_bits": params["bloom_bits"] if fastest == "inter" else
-                        channel_bloom_bits(params["bloom_bits"], int(fastest.split("_")[1])),
+            "latency": {"threads_per_query": 32 if fp["mode"] == "inter" else 32 * (12 // fp["channels"] * fp["channels"] + 1),
+                        "mode": fp["mode"], "channels": fp["channels"], "bloom_bits": fp["bloom_bits"],
+                        "mc": fp["mc"], "mg": fp["mg"], "recall": lat_recall[fastest],
                         "median_ms": lat},
             "visited_p90": vis, "recall_target_met": bool(ok), "grid": rows,
         }
@@ -163,6 +181,7 @@ def pick(profile, dim, degree, ef, objective="throughput"):
     p["mode"] = lat["mode"]
     if lat["channels"]:
         p["channels"] = lat["channels"]
-    if lat.get("bloom_bits"):
-        p["bloom_bits"] = lat["bloom_bits"]
+    for kk in ("bloom_bits", "mc", "mg"):
+        if lat.get(kk):
+            p[kk] = lat[kk]
     return p

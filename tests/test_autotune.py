@@ -30,13 +30,16 @@ def test_profile_roundtrip_and_pick(tmp_path):
                          "latency": {"threads_per_query": 32, "mode": "inter", "channels": None, "median_ms": {}}},
         "D96_R64_ef1024": {"throughput": {"params": {"k": 10, "ef": 1024, "mc": 1, "mg": 1, "cand_queue_size": 256,
                                                      "bloom_bits": 20, "mode": "inter"}, "qps": 7e4, "recall": 0.96},
-                           "latency": {"threads_per_query": 256, "mode": "intra", "channels": 8, "median_ms": {}}},
+                           "latency": {"threads_per_query": 416, "mode": "intra", "channels": 8, "mc": 2, "mg": 4,
+                                       "bloom_bits": 18, "median_ms": {}}},
     }
     path = str(tmp_path / "p.json")
     save_profile(prof, path)
     got = load_profile(path)
     assert pick(got, 96, 64, 500)["ef"] == 1024
-    assert pick(got, 96, 64, 1024, objective="latency")["channels"] == 8
+    lp = pick(got, 96, 64, 1024, objective="latency")
+    assert (lp["channels"], lp["mc"], lp["mg"], lp["bloom_bits"]) == (8, 2, 4, 18)     # DST setting of the latency pick
+    assert pick(got, 96, 64, 1024)["mg"] == 1                                          # throughput keeps its own
     assert best_for_recall(got, 0.95)[0] == "D96_R64_ef1024"
     with pytest.raises(KeyError):
         pick(got, 128, 64, 64)
@@ -58,7 +61,11 @@ def test_tune_small_index():
         assert t["qps"] > 0 and 0 <= t["recall"] <= 1
         if e["recall_target_met"]:
             assert t["recall"] >= 0.9
-        assert e["latency"]["mode"] in ("inter", "intra")
+        lat = e["latency"]
+        assert lat["mode"] in ("inter", "intra") and lat["mc"] >= 1 and lat["mg"] >= 1
+        # a latency setting may not cost recall beyond the tolerance (or below a met target)
+        need = min(0.9, t["recall"] - 0.002) if e["recall_target_met"] else t["recall"] - 0.002
+        assert lat["recall"] >= need - 1e-9
     assert prof["D96_R64_ef128"]["throughput"]["recall"] >= prof["D96_R64_ef32"]["throughput"]["recall"]
     # the server takes a request's parameters from the profile
     from falcon_b200.serving import FalconServer
