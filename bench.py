@@ -737,6 +737,44 @@ def run_cfg4(args, H2, H3, out):
                    "points": pts, "kernel_launches": int(inf.kernel_launches)}
 
 
+def profile_latency(args):
+    """Batch-1 intra-query searches of configs[1] (1M x 96) at the DST latency
+    point (ef 1024, mc 2, mg 4, 4 channels), bracketed by
+    cudaProfilerStart/Stop, for a capture of intra_kernel; prints one line."""
+    import torch
+    from falcon_b200 import FalconIndex
+    from falcon_b200.graph import build_graph, build_upper_layers
+    from falcon_b200.synthetic import unit_normal
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = "cuda:%d" % local
+    x = unit_normal(args.cfg1_n, 96, seed=0)
+    q = unit_normal(64, 96, seed=1)
+    g = build_graph(x, 64, device=dev)
+    upper = build_upper_layers(x, 32, seed=0, device=dev)
+    ix = FalconIndex(g, device=local)
+    ix.set_upper_layers(upper)
+    dq = torch.from_numpy(q).to(dev)
+    P = dict(k=10, ef=1024, mc=2, mg=4, cand_queue_size=256, bloom_bits=18, mode="intra", channels=4)
+    for i in range(args.warmup):
+        ix.search(dq[i:i + 1], **P)
+    torch.cuda.synchronize()
+    lat = []
+    torch.cuda.profiler.start()
+    for i in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        r = ix.search(dq[i:i + 1], **P)
+        b.record()
+        b.synchronize()
+        lat.append(a.elapsed_time(b))
+    torch.cuda.profiler.stop()
+    print(json.dumps({"profiled_searches": args.steps, "search": "cfg1 batch-1 intra DST", "params": P,
+                      "p50_ms": float(np.median(lat)), "hops_last": int(r.hops[0]), "visited_last": int(r.visited[0])}))
+    ix.close()
+    return 0
+
+
 def run_ours(args):
     import torch
     ws, rank, local = dist_env()
@@ -857,6 +895,9 @@ def main():
                          "there (for repeated profiling runs of one workload)")
     ap.add_argument("--profile-region", action="store_true",
                     help="bracket only the timed headline steps with cudaProfilerStart/Stop and exit after them")
+    ap.add_argument("--profile-latency", action="store_true",
+                    help="only configs[1] batch-1 intra-query searches at the DST latency point, bracketed by "
+                         "cudaProfilerStart/Stop (--steps searches after --warmup)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -870,6 +911,8 @@ def main():
     fb.build()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_latency:
+        return profile_latency(args)
     return run_ours(args)
 
 
