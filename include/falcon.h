@@ -6,7 +6,8 @@
  * an HNSW base layer or an NSG graph with delayed-synchronization traversal
  * (mc candidates per group, mg groups in flight), in inter-query mode (one
  * warp per query) and intra-query mode (one thread block per query, the
- * neighbour list split over channel warps).  Results, hop counts and visited
+ * neighbour list split over channel warps, a merge warp merging one group
+ * while the channel warps fetch the next).  Results, hop counts and visited
  * counts are bit-identical to the reference kernel's when distances are FP32.
  *
  * Conventions: every function returns an int status (FALCON_OK == 0, negative
@@ -315,8 +316,12 @@ int falcon_graph_prune(const float *vectors, int64_t num_vectors, int32_t dim, i
  * appending, so requests that arrive while others run start as soon as a warp
  * is free; each request has its own index, precision, k, ef, mc, mg.  The ring
  * is sized from free device memory (memory_fraction); falcon_server_submit
- * admits requests in order while ring entries are free and returns how many it
- * admitted (the caller keeps the rest and retries after collecting results).
+ * admits requests in order while ring entries are free and the requests in
+ * flight stay within memory_fraction of the free device memory (read every
+ * few milliseconds by the server's monitor thread) plus the server's own, and
+ * returns how many it admitted (the caller keeps the rest and retries after
+ * collecting results).  Requests of different classes (traversal precision x
+ * vector width) run in concurrent persistent kernels that share the SMs.
  * Results are collected with falcon_server_poll / falcon_server_wait.
  * Only inter-query mode is served.
  */

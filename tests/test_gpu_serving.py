@@ -93,6 +93,40 @@ def test_server_admission_by_ring_entries(two_indexes):
     sv.close()
 
 
+def test_server_admission_follows_free_memory(two_indexes):
+    """Submits admit requests by the device memory that is free now: memory
+    taken by someone else after the server was created lowers the admission
+    cap below the ring, and giving it back raises it again."""
+    import torch
+    from falcon_b200.serving import FalconServer
+    (ix1, q1), _ = two_indexes
+    free0, _ = torch.cuda.mem_get_info()
+    frac = 2000 * 600.0 / free0                         # a ring of about 2000 entries
+    sv = FalconServer(ring_capacity=65536, max_k=10, ef_max=64, dim_max=128, idle_exit_us=2000,
+                      memory_fraction=frac)
+    i0 = sv.add_index(ix1)
+    ring = sv.info().ring_entries
+    assert 1000 < ring < 4000
+    p = dict(k=10, ef=64)
+    qs = np.ascontiguousarray(q1[np.arange(ring) % len(q1)])
+    hog = torch.empty(int(free0 * 0.6), dtype=torch.uint8, device="cuda")
+    time.sleep(0.1)                                     # the server re-reads free memory every few ms
+    r = sv.submit(np.full(ring, i0), qs, p)
+    assert 0 < len(r) < 0.6 * ring                      # ~40 % of the memory is free: ~40 % of the ring
+    for x in r:
+        sv.wait(x, 10)
+    del hog
+    torch.cuda.empty_cache()
+    time.sleep(0.1)
+    r2 = sv.submit(np.full(ring, i0), qs, p)
+    assert len(r2) > 0.9 * ring
+    for j, x in enumerate(r2):
+        got = sv.wait(x, 10)
+        if j < 8:
+            assert _same(got, _alone(ix1, qs[j], p))
+    sv.close()
+
+
 def test_server_idle_exit_and_relaunch(two_indexes):
     from falcon_b200.serving import FalconServer
     (ix1, q1), _ = two_indexes
