@@ -338,6 +338,21 @@ def test_gpu_intra_matches_oracle(oracle_mod, kind, dim, md, ef, mc, mg, ch, bit
     assert np.array_equal(r.hops, hops) and np.array_equal(r.visited, vis)
 
 
+@pytest.mark.parametrize("ch,mc,mg", [(4, 2, 4), (2, 1, 1), (8, 1, 3)])
+def test_gpu_intra_batch_layout_matches_oracle(oracle_mod, ch, mc, mg):
+    """More queries than SMs: blocks of one fetch warp per channel plus the
+    merge warp (the latency layout, up to 12 fetch warps, is the one the other
+    intra cases run)."""
+    g, q = small_graph("unit", 4000, 96, 64, 300, seed=17)
+    ix = _index(g)
+    r = ix.search(q, k=10, ef=128, mc=mc, mg=mg, mode="intra", channels=ch, bloom_bits=16)
+    og = oracle_graph(oracle_mod, g)
+    ids, d, hops, vis, _ = oracle_mod.search(og, q, g.entry_point, oracle_mod.make_params(
+        k=10, ef=128, mc=mc, mg=mg, mode="intra", channels=ch, bloom_bits=16))
+    assert _same(r.ids, r.dists, ids, d)
+    assert np.array_equal(r.hops, hops) and np.array_equal(r.visited, vis)
+
+
 def test_gpu_intra_mixed_params_and_truncation(oracle_mod):
     g, q = small_graph("unit", 4000, 96, 64, 64, seed=13)
     rng = np.random.default_rng(8)
