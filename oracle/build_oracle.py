@@ -14,6 +14,8 @@ Outputs:
                                     variant (eval_trace_FPGA_inter_query_v1.3)
   oracle/_ref/libhnswlib_ref.so     the reference's vendored hnswlib (graph
                                     builder + CPU search baseline)
+  oracle/_ref/CPU_client_simulator the reference's networked CPU client
+                                    simulator (wire-format interop tests)
   oracle/_ref/murmur_golden,
   oracle/_ref/bloom_golden          drivers around the reference's software
                                     Murmur2 / Bloom, used to regenerate the
@@ -158,6 +160,13 @@ def build_ref(force=False):
             _run(["g++", "-O3"] + isa + ["-std=c++17", "-fPIC", "-shared", "-pthread", "-I", REF_HNSWLIB,
                   src, "-o", out + ".tmp"])
             os.replace(out + ".tmp", out)
+    # the networked client simulator (networked_FPGA/CPU_programs/CPU_client_simulator.cpp, the reference's
+    # own Makefile recipe: g++ -std=c++20 ... -lpthread -fopenmp), for the wire-format interop tests
+    out = os.path.join(REF_OUT, "CPU_client_simulator")
+    src = os.path.join(REF_ROOT, "networked_FPGA", "CPU_programs", "CPU_client_simulator.cpp")
+    if force or _stale(out, [src, os.path.abspath(__file__)]):
+        _run(["g++", "-O2", "-std=c++20", src, "-lpthread", "-fopenmp", "-o", out + ".tmp"])
+        os.replace(out + ".tmp", out)
     out = os.path.join(REF_OUT, "murmur_golden")
     src = os.path.join(HERE, "ref_harness", "murmur_golden.cpp")
     if force or _stale(out, [src]):
