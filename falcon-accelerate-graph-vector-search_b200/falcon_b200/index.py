@@ -205,12 +205,14 @@ class FalconIndex:
 
     def search(self, queries, k=10, ef=64, mc=1, mg=1, cand_queue_size=32, bloom_bits=16, hash_seed=1,
                mode="inter", channels=4, precision="f32", rerank=False, max_hops=0, entry_points=None,
-               per_query=None, out_stride=None, stream=None):
+               per_query=None, out_stride=None, stream=None, out=None):
         """Search host queries [nq, dim] (numpy) or device queries (torch CUDA tensor).
 
         per_query: optional list of dicts or SearchParams, one per query, or
         a params_array (mixed k/ef/mc in one launch; host or device queries).  Returns (ids, dists, hops, visited) with
         ids/dists [nq, out_stride] best-first (out_stride = max k by default).
+        out: for host queries, result arrays (ids, dists, hops, visited) to
+        write into, e.g. pinned_results(nq, out_stride) reused across calls.
         """
         lib = _lib.load()
         if per_query is not None:
@@ -227,10 +229,17 @@ class FalconIndex:
         if q.ndim != 2 or q.shape[1] != self.dim:
             raise ValueError("queries must be [nq, %d]" % self.dim)
         nq = q.shape[0]
-        ids = np.empty((nq, ostride), dtype=np.int32)
-        dists = np.empty((nq, ostride), dtype=np.float32)
-        hops = np.empty(nq, dtype=np.int32)
-        vis = np.empty(nq, dtype=np.int32)
+        if out is not None:
+            ids, dists, hops, vis = out
+            for a, shape, dt in ((ids, (nq, ostride), np.int32), (dists, (nq, ostride), np.float32),
+                                 (hops, (nq,), np.int32), (vis, (nq,), np.int32)):
+                if a.shape != shape or a.dtype != dt or not a.flags.c_contiguous:
+                    raise ValueError("out arrays must be C-contiguous %s %s" % (shape, np.dtype(dt).name))
+        else:
+            ids = np.empty((nq, ostride), dtype=np.int32)
+            dists = np.empty((nq, ostride), dtype=np.float32)
+            hops = np.empty(nq, dtype=np.int32)
+            vis = np.empty(nq, dtype=np.int32)
         ep = None
         if entry_points is not None:
             ep = np.ascontiguousarray(entry_points, dtype=np.int32)
@@ -287,6 +296,18 @@ class FalconIndex:
                                vis.data_ptr(), _lib.MEM_DEVICE, ctypes.c_void_p(s))
         _lib.check(rc)
         return SearchResult(ids, dists, hops, vis, rc)
+
+
+def pinned_results(nq, out_stride):
+    """(ids, dists, hops, visited) arrays in page-locked host memory, for
+    search(..., out=...): the device-to-host copies of a host-memory search
+    then run at full link bandwidth and touch no fresh pages (the reference's
+    host likewise allocates its result buffers once)."""
+    import torch
+    return (torch.empty((nq, out_stride), dtype=torch.int32, pin_memory=True).numpy(),
+            torch.empty((nq, out_stride), dtype=torch.float32, pin_memory=True).numpy(),
+            torch.empty(nq, dtype=torch.int32, pin_memory=True).numpy(),
+            torch.empty(nq, dtype=torch.int32, pin_memory=True).numpy())
 
 
 def _is_torch_cuda(x):
