@@ -1420,10 +1420,47 @@ __global__ void __launch_bounds__(32 * kIntraMaxWarps) intra_kernel(const Search
                     //    order; the windows of 32 run over the channel lists laid
                     //    end to end, so a window spans channel boundaries
                     const int mp = par ^ 1;
-                    const int *lid = list_id + (size_t)lcap * mp * C;
-                    const float *ld = list_d + (size_t)lcap * mp * C;
+                    int *lid = list_id + (size_t)lcap * mp * C;
+                    float *ld = list_d + (size_t)lcap * mp * C;
                     int total = 0;
                     for (int c = 0; c < C; c++) total += S->chan_valid[mp][c];
+                    if constexpr (!HEAP) {
+                        // Only ids below the worst result can be kept (the maximum only
+                        // decreases during the merge): they are packed in sequence order
+                        // to the front of this parity's lists, so that every window but
+                        // the last is full.  A packed slot never lies beyond its source
+                        // (channel c's lists start after all earlier channels' ids).
+                        int np = 0;
+                        for (int j0 = 0; j0 < total; j0 += 32) {
+                            const int p = j0 + lane;
+                            const bool v = p < total;
+                            int src = 0;
+                            if (v) {
+                                int rem = p, c = 0;
+                                while (rem >= S->chan_valid[mp][c]) rem -= S->chan_valid[mp][c++];
+                                src = c * lcap + rem;
+                            }
+                            const float dl = v ? ld[src] : kLarge;
+                            const int il = v ? lid[src] : -1;
+                            const bool keep = v && dl < rmax;
+                            const unsigned km = __ballot_sync(kFull, keep);
+                            __syncwarp();
+                            if (keep) {
+                                const int t = np + __popc(km & ((1u << lane) - 1u));
+                                ld[t] = dl;
+                                lid[t] = il;
+                            }
+                            np += __popc(km);
+                            __syncwarp();
+                        }
+                        for (int j0 = 0; j0 < np; j0 += 32) {
+                            const bool v = j0 + lane < np;
+                            const float dl = v ? ld[j0 + lane] : kLarge;
+                            const int idl = v ? lid[j0 + lane] : -1;
+                            merge_window<EPL, CPL>(L, P.ef, P.cq, dl, idl, v, lane, rmax, cmax);
+                        }
+                        total = 0;
+                    }
                     for (int j0 = 0; j0 < total; j0 += 32) {
                         const int p = j0 + lane;
                         const bool v = p < total;
@@ -1450,9 +1487,6 @@ __global__ void __launch_bounds__(32 * kIntraMaxWarps) intra_kernel(const Search
                                     }
                                 }
                             }
-                        } else {
-                            const int idl = v ? lid[src] : -1;
-                            merge_window<EPL, CPL>(L, P.ef, P.cq, dl, idl, v, lane, rmax, cmax);
                         }
                     }
                     // 4. the scheduler retires the group and refills the free
