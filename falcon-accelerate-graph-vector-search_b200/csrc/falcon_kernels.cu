@@ -77,6 +77,28 @@ __device__ __forceinline__ int ld_nc_s32(const int32_t *p)
     return r;
 }
 
+// Paired FP32 add and multiply (sm_100 f32x2): each half rounded to nearest
+// like __fadd_rn / __fmul_rn.  The explicit .rn keeps the code generator from
+// fusing a multiply into a following add, which would round once instead of
+// twice and change the distance bits.
+__device__ __forceinline__ float2 add2_rn(float2 a, float2 b)
+{
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
+__device__ __forceinline__ float2 mul2_rn(float2 a, float2 b)
+{
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
 template <int ELEM>
 __device__ __forceinline__ void decode_seg(const uint4 raw, float scale, float (&x)[ET<ELEM>::EPS])
 {
@@ -110,15 +132,20 @@ __device__ __forceinline__ void decode_seg(const uint4 raw, float scale, float (
 }
 
 // Pairwise tree over the EPS squared differences of one segment: the lower
-// levels of the reference's 16-leaf adder tree (compute.hpp:17-34).
+// levels of the reference's 16-leaf adder tree (compute.hpp:17-34).  nq is
+// the NEGATED query: x + (-q) is exactly -(q - x), whose square has the same
+// bits as (q - x)^2, so the differences and squares of adjacent leaves run as
+// paired operations.
 template <int EPS>
-__device__ __forceinline__ float seg_tree(const float (&q)[EPS], const float (&x)[EPS])
+__device__ __forceinline__ float seg_tree(const float (&nq)[EPS], const float (&x)[EPS])
 {
     float v[EPS];
 #pragma unroll
-    for (int i = 0; i < EPS; i++) {
-        const float d = __fsub_rn(q[i], x[i]);
-        v[i] = __fmul_rn(d, d);
+    for (int i = 0; i < EPS; i += 2) {
+        const float2 d = add2_rn(make_float2(x[i], x[i + 1]), make_float2(nq[i], nq[i + 1]));
+        const float2 s = mul2_rn(d, d);
+        v[i] = s.x;
+        v[i + 1] = s.y;
     }
 #pragma unroll
     for (int w = EPS; w > 1; w >>= 1) {
@@ -147,7 +174,7 @@ __device__ __forceinline__ float seg_tree(const float (&q)[EPS], const float (&x
 // On return lane l holds the distance of row l%NB of group l>>lg.
 // ---------------------------------------------------------------------------
 template <int ELEM, int VROWS, int NB>
-__device__ __forceinline__ float batch_distances(const float (&q)[VROWS][ET<ELEM>::EPS], const uint4 (&raw)[NB][VROWS],
+__device__ __forceinline__ float batch_distances(const float (&nq)[VROWS][ET<ELEM>::EPS], const uint4 (&raw)[NB][VROWS],
                                                  const float (&scale)[NB], int lane, int lg = 5)
 {
     constexpr int EPS = ET<ELEM>::EPS;
@@ -159,7 +186,7 @@ __device__ __forceinline__ float batch_distances(const float (&q)[VROWS][ET<ELEM
         for (int t = 0; t < NB; t++) {
             float x[EPS];
             decode_seg<ELEM>(raw[t][r], scale[t], x);
-            p[t] = seg_tree<EPS>(q[r], x);
+            p[t] = seg_tree<EPS>(nq[r], x);
         }
         // transposed levels
         int level = 0;
@@ -790,7 +817,7 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
     const bool rep_lane = (lane & gmask) < NB;              // one lane per slot
     const int my_slot = (lane >> lg) * NB + (lane & gmask);  // the slot that lane represents
 
-    float q[VROWS][EPS];
+    float nq[VROWS][EPS];   // negated query (seg_tree)
     {
         const float *Q = io.query;
 #pragma unroll
@@ -799,7 +826,7 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
 #pragma unroll
             for (int e = 0; e < EPS; e++) {
                 const int j = seg * EPS + e;
-                q[r][e] = (seg < nseg && j < g.dim) ? __ldcg(Q + j) : 0.0f;
+                nq[r][e] = (seg < nseg && j < g.dim) ? -__ldcg(Q + j) : 0.0f;
             }
         }
     }
@@ -881,7 +908,7 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                 if (p1 && !v1) sids[ps1] = ~n1;
                 __syncwarp();
                 for (int b0 = 0; b0 < PV; b0 += BS) {
-                    const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane, lg);
+                    const float dist = batch_distances<ELEM, VROWS, NB>(nq, raw, scale, lane, lg);
                     if (b0 + BS < PV) gather_batch<ELEM, VROWS, NB>(g, sids, b0 + BS, PV, nseg, lane, lg, raw, scale);
                     const int nt = min(BS, PV - b0);
                     const bool keep = rep_lane && my_slot < nt && sids[b0 + my_slot] >= 0;
@@ -932,7 +959,7 @@ __device__ void search_one_inter(const GraphView &g, const QParams &P, const Que
                 float scale[NB];
                 if (V > 0) gather_batch<ELEM, VROWS, NB>(g, sids, 0, V, nseg, lane, lg, raw, scale);
                 for (int b0 = 0; b0 < V; b0 += BS) {
-                    const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane, lg);
+                    const float dist = batch_distances<ELEM, VROWS, NB>(nq, raw, scale, lane, lg);
                     if (b0 + BS < V) gather_batch<ELEM, VROWS, NB>(g, sids, b0 + BS, V, nseg, lane, lg, raw, scale);
                     const int nt = min(BS, V - b0);
                     if constexpr (TRACE)
@@ -1255,7 +1282,7 @@ __global__ void __launch_bounds__(32 * kIntraMaxWarps) intra_kernel(const Search
         if (qi >= (unsigned long long)A.nq) break;
         const QParams P = A.params[A.per_query ? qi : 0];
         const int mc = P.mc, mg = P.mg;
-        float q[VROWS][EPS];
+        float nq[VROWS][EPS];   // negated query (seg_tree)
         {
             const float *Q = A.queries + qi * A.qstride;
 #pragma unroll
@@ -1264,7 +1291,7 @@ __global__ void __launch_bounds__(32 * kIntraMaxWarps) intra_kernel(const Search
 #pragma unroll
                 for (int e = 0; e < EPS; e++) {
                     const int j = seg * EPS + e;
-                    q[r][e] = (seg < nseg && j < g.dim) ? Q[j] : 0.0f;
+                    nq[r][e] = (seg < nseg && j < g.dim) ? -Q[j] : 0.0f;
                 }
             }
         }
@@ -1406,7 +1433,7 @@ __global__ void __launch_bounds__(32 * kIntraMaxWarps) intra_kernel(const Search
                 float scale[NB];
                 if (b0 < nvalid) gather_batch<ELEM, VROWS, NB>(g, my_ids, b0, nvalid, nseg, lane, lg, raw, scale);
                 for (; b0 < nvalid; b0 += stp) {
-                    const float dist = batch_distances<ELEM, VROWS, NB>(q, raw, scale, lane, lg);
+                    const float dist = batch_distances<ELEM, VROWS, NB>(nq, raw, scale, lane, lg);
                     if (b0 + stp < nvalid)
                         gather_batch<ELEM, VROWS, NB>(g, my_ids, b0 + stp, nvalid, nseg, lane, lg, raw, scale);
                     if (rep_lane && b0 + my_slot < nvalid) my_d[b0 + my_slot] = dist;
@@ -1613,7 +1640,7 @@ __global__ void __launch_bounds__(128) descend_kernel(const DescendLaunch A)
     const int64_t nwarps = (int64_t)gridDim.x * 4;
     for (int64_t qn = (int64_t)blockIdx.x * 4 + warp; qn < A.nq; qn += nwarps) {
         const int64_t qi = A.rows ? (int64_t)A.rows[qn] : qn;   // the query's row
-        float q[VROWS][4];
+        float nq[VROWS][4];   // negated query (seg_tree)
         const float *Q = A.queries + qi * A.qstride;
 #pragma unroll
         for (int r = 0; r < VROWS; r++) {
@@ -1621,7 +1648,7 @@ __global__ void __launch_bounds__(128) descend_kernel(const DescendLaunch A)
 #pragma unroll
             for (int e = 0; e < 4; e++) {
                 const int j = seg * 4 + e;
-                q[r][e] = (seg < nseg && j < g.dim) ? __ldg(Q + j) : 0.0f;
+                nq[r][e] = (seg < nseg && j < g.dim) ? -__ldg(Q + j) : 0.0f;
             }
         }
         int cur = u.entry, hops = 0;
@@ -1632,7 +1659,7 @@ __global__ void __launch_bounds__(128) descend_kernel(const DescendLaunch A)
             uint4 raw[NB][VROWS];
             float scale[NB];
             gather_batch<kF32, VROWS, NB>(g, sids, 0, 1, nseg, lane, lg, raw, scale);
-            curd = __shfl_sync(kFull, batch_distances<kF32, VROWS, NB>(q, raw, scale, lane, lg), 0);
+            curd = __shfl_sync(kFull, batch_distances<kF32, VROWS, NB>(nq, raw, scale, lane, lg), 0);
             __syncwarp();
         }
         for (int level = u.max_level; level > 0; level--) {
@@ -1652,7 +1679,7 @@ __global__ void __launch_bounds__(128) descend_kernel(const DescendLaunch A)
                 float scale[NB];
                 if (cnt > 0) gather_batch<kF32, VROWS, NB>(g, sids, 0, cnt, nseg, lane, lg, raw, scale);
                 for (int b0 = 0; b0 < cnt; b0 += BS) {
-                    const float dist = batch_distances<kF32, VROWS, NB>(q, raw, scale, lane, lg);
+                    const float dist = batch_distances<kF32, VROWS, NB>(nq, raw, scale, lane, lg);
                     if (b0 + BS < cnt) gather_batch<kF32, VROWS, NB>(g, sids, b0 + BS, cnt, nseg, lane, lg, raw, scale);
                     const bool in = rep_lane && b0 + my_slot < cnt;
                     // distances are >= +0: their bit patterns order like the floats
@@ -1692,14 +1719,14 @@ __device__ void rerank_one(const GraphView &g, const QParams &P, const float *Q,
 {
     constexpr int NB = (VROWS == 1) ? 8 : 4;
     const int nseg = g.dpad * 4 / 16;
-    float q[VROWS][4];
+    float nq[VROWS][4];   // negated query (seg_tree)
 #pragma unroll
     for (int r = 0; r < VROWS; r++) {
         const int seg = lane + 32 * r;
 #pragma unroll
         for (int e = 0; e < 4; e++) {
             const int j = seg * 4 + e;
-            q[r][e] = (seg < nseg && j < g.dim) ? __ldcg(Q + j) : 0.0f;
+            nq[r][e] = (seg < nseg && j < g.dim) ? -__ldcg(Q + j) : 0.0f;
         }
     }
     for (int b0 = 0; b0 < P.ef; b0 += NB) {
@@ -1719,7 +1746,7 @@ __device__ void rerank_one(const GraphView &g, const QParams &P, const float *Q,
                 raw[t][r] = (ids[t] >= 0 && seg < nseg) ? ld_nc_v4(base + 16 * seg) : make_uint4(0, 0, 0, 0);
             }
         }
-        const float dist = batch_distances<kF32, VROWS, NB>(q, raw, scale, lane);
+        const float dist = batch_distances<kF32, VROWS, NB>(nq, raw, scale, lane);
         if (lane < NB && b0 + lane < P.ef) {
             const int id = ids[lane];
             sd[b0 + lane] = (id >= 0) ? dist : kLarge;
