@@ -1704,6 +1704,106 @@ __global__ void __launch_bounds__(128) descend_kernel(const DescendLaunch A)
     }
 }
 
+// The same descent with one block of four warps per query, for small batches
+// (at batch 1 the warp-per-query kernel pays one gather round trip per batch
+// of BS slots, four per 32-id row).  Warp w takes the slots [w*BS, (w+1)*BS)
+// of every 4*BS, so a row of up to 4*BS ids costs one gather round trip; each
+// warp reduces its slots to (smallest distance bits, first slot) and the four
+// pairs are combined in the same lexicographic order, which picks the row's
+// first slot with the smallest distance, as the one-warp scan does.  Every
+// warp reads the node's level and row itself (the same addresses), so a hop
+// takes one block barrier.
+template <int VROWS>
+__global__ void __launch_bounds__(128) descend_block_kernel(const DescendLaunch A)
+{
+    __shared__ int s_ids[4][kMaxDegree];
+    __shared__ unsigned long long s_best[2][4];   // per hop parity: (distance bits << 32) | slot
+    constexpr int NB = (VROWS == 1) ? 8 : 4;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int *sids = s_ids[warp];
+    const GraphView &g = A.g;
+    const UpperView &u = A.u;
+    const int nseg = g.dpad * 4 / 16;
+    const int lg = lane_group_log2<VROWS, NB>(nseg);
+    const int BS = (32 >> lg) * NB;
+    const int gmask = (1 << lg) - 1;
+    const bool rep_lane = (lane & gmask) < NB;
+    const int my_slot = (lane >> lg) * NB + (lane & gmask);
+    for (int64_t qn = blockIdx.x; qn < A.nq; qn += gridDim.x) {
+        const int64_t qi = A.rows ? (int64_t)A.rows[qn] : qn;
+        float nq[VROWS][4];   // negated query (seg_tree)
+        const float *Q = A.queries + qi * A.qstride;
+#pragma unroll
+        for (int r = 0; r < VROWS; r++) {
+            const int seg = (lane & gmask) + 32 * r;
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int j = seg * 4 + e;
+                nq[r][e] = (seg < nseg && j < g.dim) ? -__ldg(Q + j) : 0.0f;
+            }
+        }
+        int cur = u.entry, hops = 0;
+        float curd;
+        {   // distance to the top entry (every warp, the same value)
+            if (lane == 0) sids[0] = cur;
+            __syncwarp();
+            uint4 raw[NB][VROWS];
+            float scale[NB];
+            gather_batch<kF32, VROWS, NB>(g, sids, 0, 1, nseg, lane, lg, raw, scale);
+            curd = __shfl_sync(kFull, batch_distances<kF32, VROWS, NB>(nq, raw, scale, lane, lg), 0);
+            __syncwarp();
+        }
+        int par = 0;
+        for (int level = u.max_level; level > 0; level--) {
+            for (;;) {
+                int cnt = 0;
+                const int32_t *row = nullptr;
+                if (__ldg(u.levels + cur) >= level) {
+                    row = u.rows + (__ldg(u.row_start + cur) + level - 1) * u.stride;
+                    cnt = __ldg(row);
+                }
+                hops++;
+                // this warp's slots: [b*BS, (b+1)*BS) for b = warp, warp + 4, ...
+                uint32_t mbits = 0xffffffffu;
+                int mslot = 0x7fffffff;
+                for (int base = warp * BS; base < cnt; base += 4 * BS) {
+                    const int n = min(BS, cnt - base);
+                    for (int i = lane; i < n; i += 32) sids[i] = __ldg(row + 16 + base + i);
+                    __syncwarp();
+                    uint4 raw[NB][VROWS];
+                    float scale[NB];
+                    gather_batch<kF32, VROWS, NB>(g, sids, 0, n, nseg, lane, lg, raw, scale);
+                    const float dist = batch_distances<kF32, VROWS, NB>(nq, raw, scale, lane, lg);
+                    const bool in = rep_lane && my_slot < n;
+                    // distances are >= +0: their bit patterns order like the floats
+                    const uint32_t mb = __reduce_min_sync(kFull, in ? __float_as_uint(dist) : 0xffffffffu);
+                    const unsigned at = __ballot_sync(kFull, in && __float_as_uint(dist) == mb);
+                    if (at && mb < mbits) {   // earlier batches of this warp hold lower slots
+                        const int t = __ffs(at) - 1;
+                        mbits = mb;
+                        mslot = base + (t >> lg) * NB + (t & gmask);
+                    }
+                    __syncwarp();
+                }
+                if (lane == 0) s_best[par][warp] = ((unsigned long long)mbits << 32) | (unsigned)mslot;
+                __syncthreads();
+                unsigned long long b = s_best[par][0];
+#pragma unroll
+                for (int w = 1; w < 4; w++) b = min(b, s_best[par][w]);
+                par ^= 1;
+                const uint32_t bb = (uint32_t)(b >> 32);
+                if (bb == 0xffffffffu || !(__uint_as_float(bb) < curd)) break;
+                cur = __ldg(row + 16 + (int)(b & 0xffffffffu));
+                curd = __uint_as_float(bb);
+            }
+        }
+        if (threadIdx.x == 0) {
+            A.out_entry[qi * (A.out_entry_stride > 0 ? A.out_entry_stride : 1)] = cur;
+            if (A.out_hops) A.out_hops[qn] = hops;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Exact FP32 rerank of the final ef candidates of a reduced-precision
 // traversal (extension beyond the reference): one warp per query, the same
@@ -2105,6 +2205,17 @@ cudaError_t launch_descend(const DescendLaunch &a, int num_sms, cudaStream_t s)
 {
     if (a.nq <= 0) return cudaSuccess;
     const int vrows = (a.g.dpad * 4 / 16 + 31) / 32;
+    if (a.nq <= (int64_t)num_sms * 4) {   // small batches: a block per query
+        const unsigned nb = (unsigned)a.nq;
+        switch (vrows) {
+            case 1: descend_block_kernel<1><<<nb, 128, 0, s>>>(a); break;
+            case 2: descend_block_kernel<2><<<nb, 128, 0, s>>>(a); break;
+            case 3: descend_block_kernel<3><<<nb, 128, 0, s>>>(a); break;
+            case 4: descend_block_kernel<4><<<nb, 128, 0, s>>>(a); break;
+            default: return cudaErrorInvalidValue;
+        }
+        return cudaGetLastError();
+    }
     int64_t blocks = (a.nq + 3) / 4;
     const int64_t cap = (int64_t)num_sms * 8;
     if (blocks > cap) blocks = cap;

@@ -211,8 +211,10 @@ class FalconIndex:
         per_query: optional list of dicts or SearchParams, one per query, or
         a params_array (mixed k/ef/mc in one launch; host or device queries).  Returns (ids, dists, hops, visited) with
         ids/dists [nq, out_stride] best-first (out_stride = max k by default).
-        out: for host queries, result arrays (ids, dists, hops, visited) to
-        write into, e.g. pinned_results(nq, out_stride) reused across calls.
+        out: result arrays (ids, dists, hops, visited) to write into and
+        return, reused across calls: numpy arrays for host queries (e.g.
+        pinned_results(nq, out_stride)), CUDA tensors on the queries' device
+        for device queries (device_results(nq, out_stride)).
         """
         lib = _lib.load()
         if per_query is not None:
@@ -224,7 +226,7 @@ class FalconIndex:
             kmax = params.k
         ostride = int(out_stride or kmax)
         if _is_torch_cuda(queries):
-            return self._search_device(queries, params, pq, ostride, entry_points, stream)
+            return self._search_device(queries, params, pq, ostride, entry_points, stream, out)
         q = np.ascontiguousarray(queries, dtype=np.float32)
         if q.ndim != 2 or q.shape[1] != self.dim:
             raise ValueError("queries must be [nq, %d]" % self.dim)
@@ -276,16 +278,24 @@ class FalconIndex:
         _lib.check(rc)
         return SearchResult(ids, dists, hops, vis, rc), Trace(cd, cn, td, ti, cnt)
 
-    def _search_device(self, queries, params, pq, ostride, entry_points, stream):
+    def _search_device(self, queries, params, pq, ostride, entry_points, stream, out=None):
         import torch
         lib = _lib.load()
         q = queries.contiguous().float()
         nq = q.shape[0]
         dev = q.device
-        ids = torch.empty((nq, ostride), dtype=torch.int32, device=dev)
-        dists = torch.empty((nq, ostride), dtype=torch.float32, device=dev)
-        hops = torch.empty(nq, dtype=torch.int32, device=dev)
-        vis = torch.empty(nq, dtype=torch.int32, device=dev)
+        if out is not None:
+            ids, dists, hops, vis = out
+            for a, shape, dt in ((ids, (nq, ostride), torch.int32), (dists, (nq, ostride), torch.float32),
+                                 (hops, (nq,), torch.int32), (vis, (nq,), torch.int32)):
+                if (not isinstance(a, torch.Tensor) or a.device != dev or tuple(a.shape) != shape or a.dtype != dt
+                        or not a.is_contiguous()):
+                    raise ValueError("out tensors must be contiguous %s %s on %s" % (shape, dt, dev))
+        else:
+            ids = torch.empty((nq, ostride), dtype=torch.int32, device=dev)
+            dists = torch.empty((nq, ostride), dtype=torch.float32, device=dev)
+            hops = torch.empty(nq, dtype=torch.int32, device=dev)
+            vis = torch.empty(nq, dtype=torch.int32, device=dev)
         ep = None
         if entry_points is not None:
             ep = entry_points.to(device=dev, dtype=torch.int32).contiguous()
@@ -308,6 +318,17 @@ def pinned_results(nq, out_stride):
             torch.empty((nq, out_stride), dtype=torch.float32, pin_memory=True).numpy(),
             torch.empty(nq, dtype=torch.int32, pin_memory=True).numpy(),
             torch.empty(nq, dtype=torch.int32, pin_memory=True).numpy())
+
+
+def device_results(nq, out_stride, device=0):
+    """(ids, dists, hops, visited) CUDA tensors for search(..., out=...) on
+    device queries: a caller that searches small batches in a loop allocates
+    its result buffers once instead of four times per call."""
+    import torch
+    return (torch.empty((nq, out_stride), dtype=torch.int32, device=device),
+            torch.empty((nq, out_stride), dtype=torch.float32, device=device),
+            torch.empty(nq, dtype=torch.int32, device=device),
+            torch.empty(nq, dtype=torch.int32, device=device))
 
 
 def _is_torch_cuda(x):

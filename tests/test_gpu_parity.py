@@ -191,6 +191,17 @@ def test_device_memory_path_matches_host():
     torch.cuda.synchronize()
     assert _same(h.ids, h.dists, d.ids.cpu().numpy(), d.dists.cpu().numpy())
     assert np.array_equal(h.hops, d.hops.cpu().numpy())
+    # result tensors supplied by the caller and reused across calls (one query at a time)
+    from falcon_b200.index import device_results
+    out = device_results(1, 10)
+    for i in (0, 5, 17):
+        r = ix.search(dq[i:i + 1], k=10, ef=64, mc=2, mg=3, out=out)
+        assert r.ids is out[0]
+        torch.cuda.synchronize()
+        assert _same(h.ids[i:i + 1], h.dists[i:i + 1], out[0].cpu().numpy(), out[1].cpu().numpy())
+        assert h.hops[i] == int(out[2][0]) and h.visited[i] == int(out[3][0])
+    with pytest.raises(ValueError):
+        ix.search(dq[:2], k=10, ef=64, out=out)
 
 
 def test_max_hops_truncation_matches_oracle(oracle_mod):

@@ -167,6 +167,13 @@ def test_gpu_descent_matches_oracle(oracle_mod, source, tmp_path):
     import torch
     dent, dhops = ix.descend(torch.from_numpy(q).cuda())
     assert np.array_equal(dent.cpu().numpy(), oent) and np.array_equal(dhops.cpu().numpy(), ohops)
+    # small batches run a block per query, large ones a warp per query: both
+    # kernels (1000 queries here, the 200 above tiled) give the oracle's entries
+    big = np.tile(q, (5, 1))
+    bent, bhops = ix.descend(big)
+    assert np.array_equal(bent, np.tile(oent, 5)) and np.array_equal(bhops, np.tile(ohops, 5))
+    ent1, hops1 = ix.descend(q[:1])
+    assert ent1[0] == oent[0] and hops1[0] == ohops[0]
     ix.close()
 
 
