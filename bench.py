@@ -13,17 +13,20 @@ against FP64 ground truth on the first 10k queries.  Beside it, the same
 graph and queries at uniform k=10 and growing ef, to show where recall@10
 reaches 0.95.
 
-Extra keys (the other workloads, same run):
-  cfg0: 100k x 128 sift-like, HNSW-style M=16 graph, 1000 queries, k=10, ef=64, mc=1
-  cfg1: 1M x 96 unit-normal, HNSW-style M=32, 10k queries: throughput sweep to
-        recall >= 0.95, batch-1 latency grid ef {64,128,256} x mc {1,2,4}
-        (inter and intra), BF16/FP8 traversal + FP32 rerank, served
-  cfg3: 1M x 384 unit-normal, HNSW-style M=32, BF16 and FP8-E4M3 traversal
-        with FP32 rerank, ef {64,128}, mc=2, distance error vs FP64
-  cfg4: cfg2 and cfg3 resident together, Poisson arrivals 10k-500k QPS,
-        each request a random index, k, ef and mc; p50/p99 and sustained QPS
+Extra keys (the other workloads, same run; --workloads selects them):
+  sift100k_hnsw_m16: 100k x 128 sift-like, HNSW-style M=16 graph, 1000 queries,
+        k=10, ef=64, mc=1
+  deep1m_hnsw_m32: 1M x 96 unit-normal, HNSW-style M=32, 10k queries: throughput
+        sweep to recall >= 0.95, batch-1 latency grid ef {64,128,256} x
+        mc {1,2,4} (inter and intra), BF16/FP8 traversal + FP32 rerank, served
+  sbert1m_hnsw_m32: 1M x 384 unit-normal, HNSW-style M=32, BF16 and FP8-E4M3
+        traversal with FP32 rerank, ef {64,128}, mc=2, distance error vs FP64
+  serving_sift10m_sbert1m: the sift10m and sbert1m indexes resident together,
+        Poisson arrivals 10k-500k QPS, each request a random index, k, ef and
+        mc; p50/p99 and sustained QPS
 
-usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--configs 2,0,1,3,4]
+usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                       [--workloads sift100k,deep1m,sbert1m,serving]
        multi-GPU: python -m torch.distributed.run --nproc-per-node N bench.py --gpus N
 """
 import argparse
@@ -41,16 +44,16 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(REPO, "falcon-accelerate-graph-vector-search_b200"))
 
 RECALL_TARGET = 0.95
-# the operating point the autotuner selects at recall@10 >= 0.95
-# on this workload (recorded by the bench); --profile-throughput captures it
-CFG1_THROUGHPUT_POINT = dict(k=10, ef=1024, mc=1, mg=1, cand_queue_size=256, bloom_bits=19)
+# deep1m_hnsw_m32: the operating point the autotuner selects at recall@10 >=
+# 0.95 on this workload (recorded by the bench); --profile-throughput captures it
+DEEP1M_THROUGHPUT_POINT = dict(k=10, ef=1024, mc=1, mg=1, cand_queue_size=256, bloom_bits=19)
 METRIC = "QPS at recall@10>=0.95 (batched search; plain vs batched/served)"
 
-# the headline workload
-CFG2 = dict(n=10_000_000, dim=128, nq=100_000, degree=64, seed_data=0, seed_query=1, seed_graph=1, ngt=10_000,
+# sift10m_nsg_r64: the headline workload
+SIFT10M = dict(n=10_000_000, dim=128, nq=100_000, degree=64, seed_data=0, seed_query=1, seed_graph=1, ngt=10_000,
             efs=(32, 64, 128, 256), ks=(1, 10, 100), mcs=(1, 2, 4), cq=32, bits=16, param_seed=7,
             search_passes=((128, 1.0),))
-WORKLOAD2 = ("sift10m_nsg_r64: 10M x 128 clipped-integer base (seeded SIFT10M stand-in), NSG-style graph max degree 64 "
+WORKLOAD_SIFT10M = ("sift10m_nsg_r64: 10M x 128 clipped-integer base (seeded SIFT10M stand-in), NSG-style graph max degree 64 "
              "from the medoid (GPU-built, seed 1), 100k queries in one launch, per-query ef in {32,64,128,256}, "
              "k in {1,10,100}, mc in {1,2,4}")
 
@@ -192,18 +195,18 @@ def rounded(d):
 
 
 # ---------------------------------------------------------------------------
-# data, graph, ground truth, mixed per-query parameters
+# sift10m_nsg_r64: data, graph, ground truth, mixed per-query parameters
 # ---------------------------------------------------------------------------
-def cfg2_params(nq):
+def sift10m_params(nq):
     """Per-query (ef, k, mc) drawn by a seeded generator; ef is raised to k."""
-    rng = np.random.default_rng(CFG2["param_seed"])
-    efs = rng.choice(CFG2["efs"], nq)
-    ks = rng.choice(CFG2["ks"], nq)
-    mcs = rng.choice(CFG2["mcs"], nq)
+    rng = np.random.default_rng(SIFT10M["param_seed"])
+    efs = rng.choice(SIFT10M["efs"], nq)
+    ks = rng.choice(SIFT10M["ks"], nq)
+    mcs = rng.choice(SIFT10M["mcs"], nq)
     return np.maximum(efs, ks), ks, mcs
 
 
-def cfg2_workload(dev, rank=0, timings=None):
+def sift10m_workload(dev, rank=0, timings=None):
     """Base, queries (seeded by rank for replicas), graph (host formats.Graph),
     FP64 ground truth (top 100) of the first ngt queries."""
     import torch
@@ -212,34 +215,34 @@ def cfg2_workload(dev, rank=0, timings=None):
     from falcon_b200.synthetic import sift_like_blocks
     tm = timings if timings is not None else {}
     t = time.time()
-    x = sift_like_blocks(CFG2["n"], CFG2["dim"], seed=CFG2["seed_data"])
-    q = sift_like_blocks(CFG2["nq"], CFG2["dim"], seed=CFG2["seed_query"] + 1000 * rank)
+    x = sift_like_blocks(SIFT10M["n"], SIFT10M["dim"], seed=SIFT10M["seed_data"])
+    q = sift_like_blocks(SIFT10M["nq"], SIFT10M["dim"], seed=SIFT10M["seed_query"] + 1000 * rank)
     tm["data_s"] = time.time() - t
-    cache = CFG2.get("graph_cache")
+    cache = SIFT10M.get("graph_cache")
     if cache and os.path.exists(cache):
         # a graph and ground truth saved by an earlier run of the same workload (profiling runs)
         from falcon_b200.formats import Graph
         z = np.load(cache)
         st = json.loads(str(z["stats"]))
-        g = Graph(x, z["links"], CFG2["degree"], int(z["entry"]))
+        g = Graph(x, z["links"], SIFT10M["degree"], int(z["entry"]))
         gt = z["gt"]
         tm["graph_cache"] = cache
-        log("cfg2 workload from %s" % cache)
+        log("sift10m workload from %s" % cache)
         return x, q, g, gt, st
     xd = torch.from_numpy(x).to(dev)
     st = {}
     t = time.time()
-    g = build_nsg(x, CFG2["degree"], seed=CFG2["seed_graph"], search_passes=CFG2["search_passes"], device=dev,
+    g = build_nsg(x, SIFT10M["degree"], seed=SIFT10M["seed_graph"], search_passes=SIFT10M["search_passes"], device=dev,
                   vectors_device=xd, stats=st, verbose=True)
     tm["graph_s"] = time.time() - t
     t = time.time()
-    gt, _ = shortlist_f64_tiled(x, q[:CFG2["ngt"]], 100, shortlist=128, base_device=xd, device=dev)
+    gt, _ = shortlist_f64_tiled(x, q[:SIFT10M["ngt"]], 100, shortlist=128, base_device=xd, device=dev)
     tm["ground_truth_s"] = time.time() - t
     if cache:
         np.savez(cache, links=g.links, entry=g.entry_point, gt=gt, stats=json.dumps(st))
     del xd
     torch.cuda.empty_cache()
-    log("cfg2 workload: %s" % rounded(tm))
+    log("sift10m workload: %s" % rounded(tm))
     return x, q, g, gt, st
 
 
@@ -266,19 +269,19 @@ def mixed_recall(ids, gt, ks):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
-def headline_cfg2(args, dev, local, rank, ws, out):
+def headline_sift10m(args, dev, local, rank, ws, out):
     import torch
     from falcon_b200 import FalconIndex, make_params
     from falcon_b200.index import params_array
     tm = {}
-    x, q, g, gt, gstats = cfg2_workload(dev, rank, tm)
+    x, q, g, gt, gstats = sift10m_workload(dev, rank, tm)
     t = time.time()
     ix = FalconIndex(g, device=local)
     tm["index_s"] = time.time() - t
     nq = len(q)
-    efs, ks, mcs = cfg2_params(nq)
-    parr = params_array([make_params(k=int(k), ef=int(e), mc=int(m), mg=1, cand_queue_size=CFG2["cq"],
-                                     bloom_bits=CFG2["bits"]) for e, k, m in zip(efs, ks, mcs)])
+    efs, ks, mcs = sift10m_params(nq)
+    parr = params_array([make_params(k=int(k), ef=int(e), mc=int(m), mg=1, cand_queue_size=SIFT10M["cq"],
+                                     bloom_bits=SIFT10M["bits"]) for e, k, m in zip(efs, ks, mcs)])
     dq = torch.from_numpy(q).to(dev)
     for _ in range(args.warmup):
         r = ix.search(dq, per_query=parr)
@@ -307,13 +310,13 @@ def headline_cfg2(args, dev, local, rank, ws, out):
     ids = r.ids.cpu().numpy()
     hops, vis = r.hops.cpu().numpy(), r.visited.cpu().numpy()
     rec = mixed_recall(ids, gt, ks)
-    log("cfg2 headline: %.2f ms/step, %.0f QPS, %s, hops %.1f visited %.1f" % (
+    log("sift10m headline: %.2f ms/step, %.0f QPS, %s, hops %.1f visited %.1f" % (
         ms_step, nq / ms_step * 1e3, rounded(rec), hops.mean(), vis.mean()))
     if args.profile_region:
-        print(json.dumps({"profiled_steps": args.steps, "search": "cfg2 mixed", "ms_per_step": ms_step,
-                          "n_base": CFG2["n"], "queries_per_step": nq, "hops_mean": float(hops.mean()),
+        print(json.dumps({"profiled_steps": args.steps, "search": "sift10m mixed", "ms_per_step": ms_step,
+                          "n_base": SIFT10M["n"], "queries_per_step": nq, "hops_mean": float(hops.mean()),
                           "visited_mean": float(vis.mean()),
-                          "bytes_per_query": algorithmic_bytes(hops, vis, CFG2["dim"], CFG2["degree"], ks) / nq}))
+                          "bytes_per_query": algorithmic_bytes(hops, vis, SIFT10M["dim"], SIFT10M["degree"], ks) / nq}))
         ix.close()
         return None
 
@@ -338,20 +341,20 @@ def headline_cfg2(args, dev, local, rank, ws, out):
     same = bool(np.array_equal(rh.ids, ids) and np.array_equal(rh.hops, hops))
 
     peak, peak_kind = measured_peak()
-    alg = algorithmic_bytes(hops, vis, CFG2["dim"], CFG2["degree"], ks)
+    alg = algorithmic_bytes(hops, vis, SIFT10M["dim"], SIFT10M["degree"], ks)
     achieved = alg / (ms_step / 1e3) / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": None, "peak_kind": peak_kind, "bytes_per_query": alg / nq,
             "kernel": "inter_kernel<f32, EPL=8, VROWS=1>",
             "achieved_from": "algorithmic bytes of the step / CUDA-event step time (the search kernel is the "
                              "step's only kernel)"}
-    traffic_from_profile(roof, "cfg2_mixed", alg)
+    traffic_from_profile(roof, "sift10m_mixed", alg)
     out.update({
         "metric": METRIC, "value": ws * nq / (ms_step / 1e3), "unit": "queries/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded clipped-integer stand-in for SIFT10M; the reference's datasets are not available)",
-        "config": {"workload": WORKLOAD2, "queries_per_step": nq, "per_query": "ef/k/mc drawn per query (seed 7), "
+        "config": {"workload": WORKLOAD_SIFT10M, "queries_per_step": nq, "per_query": "ef/k/mc drawn per query (seed 7), "
                    "ef raised to k, cand_queue_size 32, bloom_bits 16, mg 1 (the reference defaults)",
                    "mode": "inter", "recall": rec, "recall_target_reached": bool(rec.get("recall@10_k>=10", 0) >=
                                                                              RECALL_TARGET),
@@ -392,7 +395,7 @@ def traffic_from_profile(roof, key, alg_bytes):
     roof["traffic_note"] = e["note"]
 
 
-def recall_curve_cfg2(H, out):
+def recall_curve_sift10m(H, out):
     """Same graph and the ground-truth queries at uniform k=10 and growing ef:
     the smallest ef whose recall@10 reaches the target, or the best reached."""
     import torch
@@ -406,16 +409,16 @@ def recall_curve_cfg2(H, out):
         rec = recall_at_k(r.ids.cpu().numpy(), gt, 10)
         pts.append(dict(ef=ef, cq=cq, bits=bits, mc=mc, mg=mg, recall=rec, qps=n / ms * 1e3,
                         visited=float(r.visited.float().mean()), hops=float(r.hops.float().mean())))
-        log("cfg2 uniform k=10: %s" % rounded(pts[-1]))
+        log("sift10m uniform k=10: %s" % rounded(pts[-1]))
     ok = [p for p in pts if p["recall"] >= RECALL_TARGET]
     best = min(ok, key=lambda p: (p["ef"], -p["qps"])) if ok else max(pts, key=lambda p: p["recall"])
-    out["cfg2_uniform_k10"] = {"queries": n, "points": [rounded(p) for p in pts], "selected": rounded(best),
+    out["sift10m_uniform_k10"] = {"queries": n, "points": [rounded(p) for p in pts], "selected": rounded(best),
                                "recall_target_reached": bool(ok),
                                "note": "i.i.d. coordinates give full intrinsic dimension (128): graph search needs "
                                        "a large ef on this stand-in; the kernel's ef limit is 1024"}
 
 
-def cpu_baselines_cfg2(H, out, threads, budget_s=15.0):
+def cpu_baselines_sift10m(H, out, threads, budget_s=15.0):
     """Reference CPU search (the reference's vendored hnswlib, built from its
     headers) on the same graph from the same medoid with the same per-query ef
     and k, all host threads, bounded sample; then the oracle (the C
@@ -446,12 +449,12 @@ def cpu_baselines_cfg2(H, out, threads, budget_s=15.0):
                                          "(setEf per (ef, k) group), base layer from the same medoid; mc has no "
                                          "hnswlib counterpart" % n,
                                "recall": mixed_recall(lab, gt[:n], ks[:n]), "graph_load_s": load_s}
-        log("cfg2 cpu baseline: %s" % rounded({k: v for k, v in res["cpu_baseline"].items() if k != "recall"}))
+        log("sift10m cpu baseline: %s" % rounded({k: v for k, v in res["cpu_baseline"].items() if k != "recall"}))
     # oracle port + parity sample
     og = oracle.OracleGraph(g.vectors, g.links, g.max_degree, g.ids_offset)
     m = min(len(q), 4 * threads)
-    plist = [oracle.make_params(k=int(k), ef=int(e), mc=int(c), mg=1, cand_queue_size=CFG2["cq"],
-                                bloom_bits=CFG2["bits"]) for e, k, c in zip(efs[:m], ks[:m], mcs[:m])]
+    plist = [oracle.make_params(k=int(k), ef=int(e), mc=int(c), mg=1, cand_queue_size=SIFT10M["cq"],
+                                bloom_bits=SIFT10M["bits"]) for e, k, c in zip(efs[:m], ks[:m], mcs[:m])]
     t = time.time()
     ids, d, hops, vis, _ = oracle.search(og, q[:m], g.entry_point, plist, out_stride=H["ids"].shape[1],
                                          threads=threads)
@@ -465,13 +468,13 @@ def cpu_baselines_cfg2(H, out, threads, budget_s=15.0):
     res["parity_sample"] = {"queries": m, "bit_exact": int(sum(exact)),
                             "compared": "ids, distance bits, hops, visited of the GPU headline rows against the "
                                         "oracle on the same 10M graph"}
-    log("cfg2 parity sample: %d/%d bit-exact; oracle %.1f QPS" % (sum(exact), m, m / dt))
+    log("sift10m parity sample: %d/%d bit-exact; oracle %.1f QPS" % (sum(exact), m, m / dt))
     del og
     return res
 
 
-def run_cfg1(args, dev, local, out):
-    """1M x 96 unit-normal, HNSW-style M=32; throughput at the
+def run_deep1m(args, dev, local, out):
+    """deep1m_hnsw_m32: 1M x 96 unit-normal, HNSW-style M=32; throughput at the
     recall target, batch-1 latency grid, reduced precision + rerank, served."""
     import torch
     from falcon_b200 import FalconIndex
@@ -479,7 +482,7 @@ def run_cfg1(args, dev, local, out):
     from falcon_b200.graph import build_graph, build_upper_layers
     from falcon_b200.groundtruth import recall_at_k, shortlist_f64
     from falcon_b200.synthetic import unit_normal
-    n, dim, nq, k = args.cfg1_n, 96, 10_000, 10
+    n, dim, nq, k = args.deep1m_n, 96, 10_000, 10
     t0 = time.time()
     x = unit_normal(n, dim, seed=0)
     q = unit_normal(nq, dim, seed=1)
@@ -496,7 +499,7 @@ def run_cfg1(args, dev, local, out):
     from falcon_b200.autotune import best_for_recall, pick, tune
     prof = tune(ix, q[:2000], gt[:2000], dim, 64, ef_list=(256, 512, 1024), k=k, recall_target=RECALL_TARGET,
                 cq_grid=(64, 256), mcmg_grid=((1, 1), (2, 4), (1, 4)), latency_channels=(4,),
-                log=lambda m: log("cfg1 " + m))
+                log=lambda m: log("deep1m " + m))
     key, entry = best_for_recall(prof, RECALL_TARGET)
     P = pick(prof, dim, 64, entry["throughput"]["params"]["ef"])
     P.pop("mode", None)
@@ -507,7 +510,7 @@ def run_cfg1(args, dev, local, out):
                profile_key=key)
     ok = sel["recall"] >= RECALL_TARGET
     pts = [rounded({kk: v for kk, v in row.items()}) for e in prof.values() for row in e["grid"]]
-    log("cfg1 selected by the autotuner: %s" % rounded(sel))
+    log("deep1m selected by the autotuner: %s" % rounded(sel))
     ms_b, rb = timed(lambda: ix.search(dq, precision="bf16", rerank=True, **P))
     ms_f, rf = timed(lambda: ix.search(dq, precision="fp8", rerank=True, **P))
     # roofline of the throughput point: algorithmic bytes of each launch over
@@ -520,8 +523,8 @@ def run_cfg1(args, dev, local, out):
                                 np.full(nq, ef), elem_bytes=eb, scale_bytes=sb, rerank=rr)
         gbs = alg / (t_ms / 1e3) / 1e9
         roof1[name] = {"achieved_gbs": gbs, "frac": gbs / peak, "bytes_per_query": alg / nq}
-    if all(P.get(kk) == v for kk, v in CFG1_THROUGHPUT_POINT.items()):
-        traffic_from_profile(roof1["f32"], "cfg1_f32_throughput_point", roof1["f32"]["bytes_per_query"] * nq)
+    if all(P.get(kk) == v for kk, v in DEEP1M_THROUGHPUT_POINT.items()):
+        traffic_from_profile(roof1["f32"], "deep1m_f32_throughput_point", roof1["f32"]["bytes_per_query"] * nq)
     roof1["peak_gbs"] = peak
     roof1["peak_kind"] = peak_kind
     roof1["note"] = ("latency-bound: 3 blocks of 4 warps per SM (registers, and the ef-1024 result list in shared "
@@ -533,7 +536,7 @@ def run_cfg1(args, dev, local, out):
         derr[prec + "_rerank"] = distance_error_f64(x, q, res.ids.cpu().numpy(), res.dists.cpu().numpy())
         derr[prec + "_traversal"] = distance_error_f64(x, q, raw.ids.cpu().numpy(), raw.dists.cpu().numpy())
         derr[prec + "_traversal"]["recall@10"] = recall_at_k(raw.ids.cpu().numpy(), gt, k)
-    # batch-1 latency grid (configs[1]: ef {64,128,256} x mc {1,2,4}), inter and intra (4 channels)
+    # batch-1 latency grid (ef {64,128,256} x mc {1,2,4}), inter and intra (4 channels)
     grid = []
     for ef_l in (64, 128, 256):
         for mc_l in (1, 2, 4):
@@ -546,7 +549,7 @@ def run_cfg1(args, dev, local, out):
                 rr = ix.search(dq[:2000], **pl)
                 row[mode] = {"p50_ms": p50, "p99_ms": p99, "recall@10": recall_at_k(rr.ids.cpu().numpy(), gt[:2000], k)}
             grid.append(row)
-            log("cfg1 batch-1 %s" % row)
+            log("deep1m batch-1 %s" % row)
     # batch-1 at the throughput operating point
     lat_sel = {}
     for mode, extra in (("inter", {}), ("intra4", dict(mode="intra", channels=4,
@@ -564,10 +567,10 @@ def run_cfg1(args, dev, local, out):
     rl = ix.search(dq, **PL)
     lat_sel["tuned"] = {"p50_ms": p50, "p99_ms": p99, "recall@10": recall_at_k(rl.ids.cpu().numpy(), gt, k),
                         "params": {kk: v for kk, v in PL.items() if kk != "k"}}
-    log("cfg1 batch-1 at the operating point: %s" % lat_sel)
-    served = None if args.no_serve else serve_cfg1(ix, q, gt, prof, ef, nq / (ms_b / 1e3))
+    log("deep1m batch-1 at the operating point: %s" % lat_sel)
+    served = None if args.no_serve else serve_deep1m(ix, q, gt, prof, ef, nq / (ms_b / 1e3))
     ix.close()
-    out["cfg1"] = {
+    out["deep1m_hnsw_m32"] = {
         "workload": "deep1m_hnsw_m32: 1M x 96 unit-normal (seeded Deep1M stand-in), HNSW-style M=32 graph (exact "
                     "kNN + hnswlib's neighbour heuristic + reverse edges, upper layers with hnswlib's level "
                     "distribution), 10k queries, k=10; searches descend the upper layers",
@@ -583,7 +586,7 @@ def run_cfg1(args, dev, local, out):
         "served": served}
 
 
-def serve_cfg1(ix, q, gt, prof, ef, batched_bf16_qps):
+def serve_deep1m(ix, q, gt, prof, ef, batched_bf16_qps):
     """Continuous batching of single-query requests (BF16 traversal + exact
     FP32 rerank) with Poisson arrivals at 50 %, 80 % of the batched BF16 rate
     and at saturation; each request's parameters come from the autotuner's
@@ -609,14 +612,14 @@ def serve_cfg1(ix, q, gt, prof, ef, batched_bf16_qps):
               "offered": "saturation" if frac >= 10 else "%.0f%%" % (frac * 100),
               "sustained_qps": n / (el / 1e6), "p50_ms": float(np.percentile(lat, 50)) / 1e3,
               "p99_ms": float(np.percentile(lat, 99)) / 1e3, "recall@10": recall_at_k(ids[:len(q)], gt, k)}
-        log("cfg1 served %s" % rounded(pt))
+        log("deep1m served %s" % rounded(pt))
         out["points"].append(pt)
     sv.close()
     return out
 
 
-def run_cfg0(args, dev, local, out, threads):
-    """100k x 128 sift-like, HNSW-style M=16 (degree 32), 1000
+def run_sift100k(args, dev, local, out, threads):
+    """sift100k_hnsw_m16: 100k x 128 sift-like, HNSW-style M=16 (degree 32), 1000
     queries, k=10, ef=64, mc=1; hnswlib on the same graph beside it."""
     import torch
     from falcon_b200 import FalconIndex
@@ -658,12 +661,12 @@ def run_cfg0(args, dev, local, out, threads):
                                              "the same upper layers"}
             h.free()
     ix.close()
-    log("cfg0: %s" % rounded({k2: v for k2, v in res.items() if not isinstance(v, dict)}))
-    out["cfg0"] = res
+    log("sift100k: %s" % rounded({k2: v for k2, v in res.items() if not isinstance(v, dict)}))
+    out["sift100k_hnsw_m16"] = res
 
 
-def run_cfg3(args, dev, local, out, keep=False):
-    """1M x 384 unit-normal, HNSW-style M=32, BF16 and FP8-E4M3
+def run_sbert1m(args, dev, local, out, keep=False):
+    """sbert1m_hnsw_m32: 1M x 384 unit-normal, HNSW-style M=32, BF16 and FP8-E4M3
     (+ per-vector scale) traversal with FP32 accumulation and an exact FP32
     rerank of the final ef; ef {64,128}, mc=2, 10k queries."""
     import torch
@@ -671,7 +674,7 @@ def run_cfg3(args, dev, local, out, keep=False):
     from falcon_b200.graph import build_graph, build_upper_layers
     from falcon_b200.groundtruth import recall_at_k, shortlist_f64
     from falcon_b200.synthetic import unit_normal_blocks
-    n, dim, nq = args.cfg3_n, 384, 10_000
+    n, dim, nq = args.sbert1m_n, 384, 10_000
     t = time.time()
     x = unit_normal_blocks(n, dim, seed=3)
     q = unit_normal_blocks(nq, dim, seed=4)
@@ -705,8 +708,8 @@ def run_cfg3(args, dev, local, out, keep=False):
                                                                       raw.dists.cpu().numpy()),
                 "roofline_achieved_gbs": alg / (ms / 1e3) / 1e9}
         pts.append(row)
-        log("cfg3 %s" % json.dumps(row)[:600])
-    out["cfg3"] = {"workload": "sbert1m_hnsw_m32: 1M x 384 unit-normal (seeded SBERT1M stand-in), HNSW-style M=32, "
+        log("sbert1m %s" % json.dumps(row)[:600])
+    out["sbert1m_hnsw_m32"] = {"workload": "sbert1m_hnsw_m32: 1M x 384 unit-normal (seeded SBERT1M stand-in), HNSW-style M=32, "
                                "10k queries, k=10, mc=2, cand queue 32, 2^16-bit filter; BF16 / FP8-E4M3 + per-vector "
                                "FP32 scale traversal, FP32 accumulation, exact FP32 rerank of the final ef",
                    "n_base": n, "build_s": build_s, "points": pts}
@@ -716,9 +719,10 @@ def run_cfg3(args, dev, local, out, keep=False):
     return None
 
 
-def run_cfg4(args, H2, H3, out):
-    """the configs[2] (FP32, D=128, NSG) and configs[3] (BF16 +
-    FP32 rerank, D=384, HNSW) indexes resident together; Poisson arrivals,
+def run_serving(args, H2, H3, out):
+    """Online serving: the sift10m_nsg_r64 (FP32, D=128, NSG) and
+    sbert1m_hnsw_m32 (BF16 + FP32 rerank, D=384, HNSW) indexes resident
+    together; Poisson arrivals,
     each request a random index with k from {1,10,100}, ef from {32..256},
     mc from {1,2,4}."""
     from falcon_b200 import make_params
@@ -752,20 +756,20 @@ def run_cfg4(args, H2, H3, out):
         lat, ids, d, hops, vis, el = sv.replay(iids[:m], qmax[:m], params[:m], arr, 100)
         pt = {"offered_qps": rate, "requests": m, "sustained_qps": m / (el / 1e6),
               "p50_ms": float(np.percentile(lat, 50)) / 1e3, "p99_ms": float(np.percentile(lat, 99)) / 1e3,
-              "p50_ms_cfg2": float(np.percentile(lat[which[:m] == 0], 50)) / 1e3,
-              "p50_ms_cfg3": float(np.percentile(lat[which[:m] == 1], 50)) / 1e3}
-        log("cfg4 %s" % rounded(pt))
+              "p50_ms_sift10m": float(np.percentile(lat[which[:m] == 0], 50)) / 1e3,
+              "p50_ms_sbert1m": float(np.percentile(lat[which[:m] == 1], 50)) / 1e3}
+        log("serving %s" % rounded(pt))
         pts.append(pt)
     inf = sv.info()
     sv.close()
-    out["cfg4"] = {"workload": "online serving: sift10m_nsg_r64 (FP32) and sbert1m_hnsw_m32 (BF16 + FP32 rerank) "
+    out["serving_sift10m_sbert1m"] = {"workload": "online serving: sift10m_nsg_r64 (FP32) and sbert1m_hnsw_m32 (BF16 + FP32 rerank) "
                                "resident together, Poisson arrivals, each request a random index, k {1,10,100}, "
                                "ef {32,64,128,256} (raised to k), mc {1,2,4}",
                    "points": pts, "kernel_launches": int(inf.kernel_launches)}
 
 
 def profile_latency(args):
-    """Batch-1 intra-query searches of configs[1] (1M x 96) at the DST latency
+    """Batch-1 intra-query searches of deep1m_hnsw_m32 (1M x 96) at the DST latency
     point (ef 1024, mc 2, mg 4, 4 channels), bracketed by
     cudaProfilerStart/Stop, for a capture of intra_kernel; prints one line."""
     import torch
@@ -775,7 +779,7 @@ def profile_latency(args):
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
     dev = "cuda:%d" % local
-    x = unit_normal(args.cfg1_n, 96, seed=0)
+    x = unit_normal(args.deep1m_n, 96, seed=0)
     q = unit_normal(64, 96, seed=1)
     g = build_graph(x, 64, device=dev)
     upper = build_upper_layers(x, 32, seed=0, device=dev)
@@ -796,14 +800,14 @@ def profile_latency(args):
         b.synchronize()
         lat.append(a.elapsed_time(b))
     torch.cuda.profiler.stop()
-    print(json.dumps({"profiled_searches": args.steps, "search": "cfg1 batch-1 intra DST", "params": P,
+    print(json.dumps({"profiled_searches": args.steps, "search": "deep1m batch-1 intra DST", "params": P,
                       "p50_ms": float(np.median(lat)), "hops_last": int(r.hops[0]), "visited_last": int(r.visited[0])}))
     ix.close()
     return 0
 
 
 def profile_throughput(args):
-    """configs[1] (1M x 96) 10k-query searches at the throughput point the
+    """deep1m_hnsw_m32 (1M x 96) 10k-query searches at the throughput point the
     tuner selects at recall 0.95 (ef 1024, cand queue 256, 2^19-bit filters,
     mc 1, mg 1), bracketed by cudaProfilerStart/Stop, for a DRAM capture of
     the inter kernel; prints one line."""
@@ -815,14 +819,14 @@ def profile_throughput(args):
     torch.cuda.set_device(local)
     dev = "cuda:%d" % local
     nq = 10_000
-    x = unit_normal(args.cfg1_n, 96, seed=0)
+    x = unit_normal(args.deep1m_n, 96, seed=0)
     q = unit_normal(nq, 96, seed=1)
     g = build_graph(x, 64, device=dev)
     upper = build_upper_layers(x, 32, seed=0, device=dev)
     ix = FalconIndex(g, device=local)
     ix.set_upper_layers(upper)
     dq = torch.from_numpy(q).to(dev)
-    P = dict(CFG1_THROUGHPUT_POINT)
+    P = dict(DEEP1M_THROUGHPUT_POINT)
     for _ in range(args.warmup):
         r = ix.search(dq, **P)
     torch.cuda.synchronize()
@@ -836,7 +840,7 @@ def profile_throughput(args):
     torch.cuda.profiler.stop()
     hops, vis = r.hops.cpu().numpy(), r.visited.cpu().numpy()
     alg = algorithmic_bytes(hops, vis, 96, 64, np.full(nq, P["k"]))
-    print(json.dumps({"profiled_steps": args.steps, "search": "cfg1 throughput point", "params": P,
+    print(json.dumps({"profiled_steps": args.steps, "search": "deep1m throughput point", "params": P,
                       "ms_per_step": a.elapsed_time(b) / args.steps, "hops_mean": float(hops.mean()),
                       "visited_mean": float(vis.mean()), "bytes_per_query": alg / nq}))
     ix.close()
@@ -853,38 +857,38 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
     threads = os.cpu_count() or 1
-    cfgs = [int(c) for c in args.configs.split(",") if c.strip().isdigit()]
+    wl = {w.strip() for w in args.workloads.split(",") if w.strip()}
     out = {}
     t0 = time.time()
-    H2 = headline_cfg2(args, dev, local, rank, ws, out)
+    H2 = headline_sift10m(args, dev, local, rank, ws, out)
     if H2 is None:
         return 0
     if ws == 1:
-        recall_curve_cfg2(H2, out)
+        recall_curve_sift10m(H2, out)
         if not args.no_cpu_baseline:
-            res = cpu_baselines_cfg2(H2, out, threads)
+            res = cpu_baselines_sift10m(H2, out, threads)
             out["cpu_baseline"] = res.get("cpu_baseline")
             out["cpu_fpga_semantics_port"] = res.get("cpu_fpga_semantics_port")
             out["config"]["parity_sample"] = res.get("parity_sample")
-        log("cfg2 done at %.0fs" % (time.time() - t0))
+        log("sift10m done at %.0fs" % (time.time() - t0))
         H3 = None
-        if 3 in cfgs or 4 in cfgs:
-            H3 = run_cfg3(args, dev, local, out, keep=4 in cfgs)
-            log("cfg3 done at %.0fs" % (time.time() - t0))
-        if 4 in cfgs and H3 is not None and not args.no_serve:
-            run_cfg4(args, H2, H3, out)
-            log("cfg4 done at %.0fs" % (time.time() - t0))
+        if "sbert1m" in wl or "serving" in wl:
+            H3 = run_sbert1m(args, dev, local, out, keep="serving" in wl)
+            log("sbert1m done at %.0fs" % (time.time() - t0))
+        if "serving" in wl and H3 is not None and not args.no_serve:
+            run_serving(args, H2, H3, out)
+            log("serving done at %.0fs" % (time.time() - t0))
         if H3 is not None:
             H3["ix"].close()
         H2["ix"].close()
         del H2, H3
         torch.cuda.empty_cache()
-        if 1 in cfgs:
-            run_cfg1(args, dev, local, out)
-            log("cfg1 done at %.0fs" % (time.time() - t0))
-        if 0 in cfgs:
-            run_cfg0(args, dev, local, out, threads)
-            log("cfg0 done at %.0fs" % (time.time() - t0))
+        if "deep1m" in wl:
+            run_deep1m(args, dev, local, out)
+            log("deep1m done at %.0fs" % (time.time() - t0))
+        if "sift100k" in wl:
+            run_sift100k(args, dev, local, out, threads)
+            log("sift100k done at %.0fs" % (time.time() - t0))
     else:
         H2["ix"].close()
     if rank == 0:
@@ -909,8 +913,8 @@ def run_reference(args):
     if not oracle.Hnsw.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libhnswlib_ref.so not built"}))
         return 0
-    x, q, g, gt, _ = cfg2_workload("cuda:%d" % local)
-    efs, ks, _ = cfg2_params(len(q))
+    x, q, g, gt, _ = sift10m_workload("cuda:%d" % local)
+    efs, ks, _ = sift10m_params(len(q))
     h = oracle.Hnsw.from_graph(g.vectors, g.adjacency(), g.entry_point)
     n = args.ref_queries
     times = []
@@ -929,7 +933,7 @@ def run_reference(args):
             "warmup": args.warmup, "ms_per_step": dt / len(times) * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded clipped-integer stand-in for SIFT10M)", "impl": "reference",
-            "config": {"workload": WORKLOAD2, "queries_per_step": n, "recall": rec,
+            "config": {"workload": WORKLOAD_SIFT10M, "queries_per_step": n, "recall": rec,
                        "step": "%d-query slice of the 100k mixed-parameter batch (the slice moves each step); "
                                "hnswlib searchKnn with each query's ef and k from the same medoid on the same "
                                "graph; mc has no hnswlib counterpart" % n,
@@ -949,35 +953,36 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--configs", default="0,1,3,4", help="extra workloads after the configs[2] headline")
+    ap.add_argument("--workloads", default="sift100k,deep1m,sbert1m,serving",
+                    help="extra workloads after the sift10m headline (comma-separated; 'none' for the headline only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the continuous-batching measurements")
-    ap.add_argument("--n-base", type=int, default=None, help="configs[2] base size (scaled-down runs: checks only)")
+    ap.add_argument("--n-base", type=int, default=None, help="sift10m base size (scaled-down runs: checks only)")
     ap.add_argument("--n-queries", type=int, default=None)
-    ap.add_argument("--cfg1-n", type=int, default=1_000_000)
-    ap.add_argument("--cfg3-n", type=int, default=1_000_000)
+    ap.add_argument("--deep1m-n", type=int, default=1_000_000)
+    ap.add_argument("--sbert1m-n", type=int, default=1_000_000)
     ap.add_argument("--latency-samples", type=int, default=200)
     ap.add_argument("--ref-queries", type=int, default=4000, help="reference arm: queries per step")
     ap.add_argument("--graph-cache", default=None,
-                    help="configs[2]: load the graph and ground truth from this .npz if it exists, else save them "
+                    help="sift10m: load the graph and ground truth from this .npz if it exists, else save them "
                          "there (for repeated profiling runs of one workload)")
     ap.add_argument("--profile-region", action="store_true",
                     help="bracket only the timed headline steps with cudaProfilerStart/Stop and exit after them")
     ap.add_argument("--profile-throughput", action="store_true",
-                    help="only configs[1] 10k-query searches at the recall-0.95 throughput point, bracketed by "
+                    help="only deep1m 10k-query searches at the recall-0.95 throughput point, bracketed by "
                          "cudaProfilerStart/Stop (--steps searches after --warmup)")
     ap.add_argument("--profile-latency", action="store_true",
-                    help="only configs[1] batch-1 intra-query searches at the DST latency point, bracketed by "
+                    help="only deep1m batch-1 intra-query searches at the DST latency point, bracketed by "
                          "cudaProfilerStart/Stop (--steps searches after --warmup)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.n_base:
-        CFG2["n"] = args.n_base
-    CFG2["graph_cache"] = args.graph_cache
+        SIFT10M["n"] = args.n_base
+    SIFT10M["graph_cache"] = args.graph_cache
     if args.n_queries:
-        CFG2["nq"] = args.n_queries
-        CFG2["ngt"] = min(CFG2["ngt"], args.n_queries)
+        SIFT10M["nq"] = args.n_queries
+        SIFT10M["ngt"] = min(SIFT10M["ngt"], args.n_queries)
     from falcon_b200 import build as fb
     fb.build()
     if args.impl == "reference":

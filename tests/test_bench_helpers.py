@@ -41,10 +41,10 @@ def test_mixed_recall_groups():
     assert abs(r["recall@10_k>=10"] - (10 + 10 + 5) / 30.0) < 1e-12
 
 
-def test_cfg2_params_seeded():
+def test_sift10m_params_seeded():
     import bench
-    e1, k1, m1 = bench.cfg2_params(1000)
-    e2, k2, m2 = bench.cfg2_params(1000)
+    e1, k1, m1 = bench.sift10m_params(1000)
+    e2, k2, m2 = bench.sift10m_params(1000)
     assert np.array_equal(e1, e2) and np.array_equal(k1, k2) and np.array_equal(m1, m2)
     assert set(np.unique(k1)) == {1, 10, 100} and set(np.unique(m1)) == {1, 2, 4}
     assert (e1 >= k1).all() and set(np.unique(e1)) <= {32, 64, 100, 128, 256}

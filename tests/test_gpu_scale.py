@@ -1,6 +1,6 @@
 """GPU parity at the scales and operating points the benchmark runs.
 
-* configs[0] in full: the 100k x 128 base with the HNSW graph the
+* the sift100k_hnsw_m16 workload in full: the 100k x 128 base with the HNSW graph the
   reference's own scripts would build (the vendored hnswlib, M=16,
   ef_construction=128, random_seed 0, points added in order on one thread;
   vector_search_baselines/scripts_hnsw/construct_and_search_hnsw.py:124-153),
@@ -28,7 +28,7 @@ def _same(a_ids, a_d, b_ids, b_d):
 
 
 @pytest.fixture(scope="module")
-def cfg0(oracle_mod):
+def sift100k(oracle_mod):
     if not oracle_mod.Hnsw.available():
         pytest.skip("reference-derived hnswlib library not built on this host")
     from falcon_b200.formats import Graph, UpperLayers
@@ -44,9 +44,9 @@ def cfg0(oracle_mod):
     return h, g, upper, x, q
 
 
-def test_cfg0_hnswlib_graph_bit_exact(cfg0, oracle_mod):
+def test_sift100k_hnswlib_graph_bit_exact(sift100k, oracle_mod):
     from falcon_b200 import FalconIndex
-    h, g, upper, x, q = cfg0
+    h, g, upper, x, q = sift100k
     assert g.max_degree == 32
     ix = FalconIndex(g)
     # the reference's multi-DDR host starts every query at the global entry (host.cpp:711-713)
@@ -59,10 +59,10 @@ def test_cfg0_hnswlib_graph_bit_exact(cfg0, oracle_mod):
     ix.close()
 
 
-def test_cfg0_recall_within_hnswlib_tolerance(cfg0):
+def test_sift100k_recall_within_hnswlib_tolerance(sift100k):
     from falcon_b200 import FalconIndex
     from falcon_b200.groundtruth import brute_force_f64, recall_at_k
-    h, g, upper, x, q = cfg0
+    h, g, upper, x, q = sift100k
     gt, _ = brute_force_f64(x, q, 10)
     ix = FalconIndex(g)
     ix.set_upper_layers(upper)
