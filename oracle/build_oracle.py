@@ -22,7 +22,7 @@ Outputs:
                                     golden fixtures in tests/golden/
 
 The reference builds need the reference checkout at REF_ROOT; when it is
-absent (the GPU box) only the prebuilt files are used.  Reference sources are
+absent (a machine without the checkout) only the prebuilt files are used.  Reference sources are
 compiled where they lie; the only copies are transient ones in a temporary
 directory for the v1.3 kernel headers, which get three build-time edits
 (listed in ref_harness/ref_inter_harness.cpp) before compilation.
@@ -110,7 +110,7 @@ def _patched_v13_copy(dst, dim, src=None, channels=None):
 
 
 def build_ref(force=False):
-    """Build the reference-derived checkers.  Returns False if the reference
+    """Build the reference-derived harnesses.  Returns False if the reference
     checkout is absent (prebuilt files are then used as they are)."""
     if not os.path.isdir(REF_ROOT):
         return False
@@ -188,4 +188,4 @@ def build_all(force=False):
 
 if __name__ == "__main__":
     ok = build_all(force="--force" in sys.argv)
-    print("oracle built; reference checkers %s" % ("built" if ok else "skipped (no reference checkout)"))
+    print("oracle built; reference harnesses %s" % ("built" if ok else "skipped (no reference checkout)"))
