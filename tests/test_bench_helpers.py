@@ -65,3 +65,30 @@ def test_distance_error_f64():
     assert e["max_rel"] == 0.0 and e["mean_rel"] == 0.0
     e = bench.distance_error_f64(x, q, ids, exact * (1 + 1e-3))
     assert abs(e["max_rel"] - 1e-3) < 1e-9
+
+
+def test_traffic_record_follows_the_kernel_source(tmp_path, monkeypatch):
+    """roofline.traffic comes from profiles/traffic.json only while the
+    recorded capture was taken on the current kernel source; the committed
+    record covers both workloads the bench applies it to."""
+    import hashlib
+    import json
+    import bench
+    src = os.path.join(bench.REPO, "falcon-accelerate-graph-vector-search_b200", "csrc", "falcon_kernels.cu")
+    h = hashlib.sha256(open(src, "rb").read()).hexdigest()[:16]
+    rec = json.load(open(os.path.join(bench.REPO, "profiles", "traffic.json")))
+    for key in ("sift10m_mixed", "deep1m_f32_throughput_point"):
+        assert rec[key]["kernel_source_sha16"] == h
+        roof = {}
+        bench.traffic_from_profile(roof, key, 1000.0)
+        assert abs(roof["traffic"] - rec[key]["ratio"] * 1000.0) < 1e-9
+    # a record of another source is not applied
+    fake = tmp_path / "repo"
+    (fake / "profiles").mkdir(parents=True)
+    (fake / "falcon-accelerate-graph-vector-search_b200" / "csrc").mkdir(parents=True)
+    (fake / "falcon-accelerate-graph-vector-search_b200" / "csrc" / "falcon_kernels.cu").write_text("changed")
+    (fake / "profiles" / "traffic.json").write_text(json.dumps(rec))
+    monkeypatch.setattr(bench, "REPO", str(fake))
+    roof = {}
+    bench.traffic_from_profile(roof, "sift10m_mixed", 1000.0)
+    assert "traffic" not in roof and "no ncu capture" in roof["traffic_note"]
