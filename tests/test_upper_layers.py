@@ -95,6 +95,53 @@ def test_oracle_descent_matches_hnswlib(hnswlib_index, oracle_mod):
     assert np.all(hops >= upper.max_level)
 
 
+def _scan_one_warp(d, cur_d, bs):
+    """The one-warp descent's row scan (descend_kernel): batches of bs slots in
+    order; a batch's smallest distance (first slot among equals) replaces the
+    best only if strictly smaller.  Returns the chosen slot or -1."""
+    best, bestd = -1, cur_d
+    for b0 in range(0, len(d), bs):
+        blk = d[b0:b0 + bs]
+        m = blk.min()
+        if m < bestd:
+            bestd, best = m, b0 + int(np.argmax(blk == m))
+    return best
+
+
+def _scan_four_warps(d, cur_d, bs):
+    """descend_block_kernel's row scan: warp w takes batches w, w+4, ...; each
+    warp keeps (smallest distance bits, first slot); the block takes the
+    lexicographic minimum of the four pairs and moves iff it is below cur_d."""
+    bits = d.astype(np.float32).view(np.uint32).astype(np.uint64)
+    keys = []
+    for w in range(4):
+        mb, ms = 0xFFFFFFFF, 0x7FFFFFFF
+        for b0 in range(w * bs, len(d), 4 * bs):
+            blk = bits[b0:b0 + bs]
+            m = int(blk.min())
+            if m < mb:
+                mb, ms = m, b0 + int(np.argmax(blk == m))
+        keys.append((mb << 32) | ms)
+    k = min(keys)
+    mb = k >> 32
+    if mb == 0xFFFFFFFF or not (np.uint32(mb).view(np.float32) < np.float32(cur_d)):
+        return -1
+    return int(k & 0xFFFFFFFF)
+
+
+def test_block_descent_scan_equals_one_warp_scan():
+    """The four-warp split of a row scan picks the same neighbour as the
+    one-warp scan: the first slot holding the row's smallest distance, if
+    that distance is below the current one (tie-heavy rows, any row length)."""
+    rng = np.random.default_rng(5)
+    for trial in range(3000):
+        n = int(rng.integers(0, 130))
+        bs = int(rng.choice([4, 8, 16, 32]))
+        d = rng.integers(0, 12, n).astype(np.float32) / 4.0   # few distinct values: many ties
+        cur = np.float32(rng.integers(0, 14) / 4.0)
+        assert _scan_four_warps(d, cur, bs) == _scan_one_warp(d, cur, bs), (trial, n, bs)
+
+
 def test_synthetic_upper_layers_are_consistent():
     from falcon_b200.graph import build_upper_layers
     from falcon_b200.synthetic import unit_normal
